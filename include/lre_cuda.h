@@ -1,0 +1,234 @@
+/*
+ * lre_cuda.h -- C ABI of the B200 (sm_100a) develop backend for libraw_enhanced.
+ *
+ * This is the drop-in boundary for the reference's GPU accelerator: every
+ * stage entry point below replaces one method of `GPUAccelerator`
+ * (core/gpu_accelerator.h:18-118 in uniuyuni/libraw_enhanced), which
+ * `Accelerator` (core/accelerator.cpp) dispatches to when
+ * `use_gpu_acceleration` is set.  Argument meaning and defaults follow the
+ * reference method each one cites; the C++ adapter `CudaAccelerator`
+ * (libraw_enhanced_b200/csrc/cuda_accelerator.h) restores the exact C++
+ * signatures on top of this ABI.
+ *
+ * Conventions
+ *   - Images use the reference layouts (core/accelerator.h:59-80):
+ *       float RGB : interleaved float[H][W][3], row stride = W pixels
+ *                   (ImageBufferFloat);
+ *       raw uint16: uint16_t[H][W][4] (ImageBuffer);
+ *       dense CFA : float[H][W] holding each site's own sample (the packed
+ *                   form of the reference's sparse raw buffer).
+ *   - `lre_<stage>` functions take HOST pointers and are synchronous: the
+ *     result is in the host buffer on return, exactly like the reference's
+ *     blocking Metal path.  Input and output may alias for every
+ *     post-demosaic stage (the pipeline calls them in place).
+ *   - `lre_dev_<stage>` functions take DEVICE pointers, enqueue on the
+ *     context's stream and return without synchronising.
+ *   - Every function returns an lre_status; on failure `lre_last_error(ctx)`
+ *     holds a message.  There is no CPU fallback: a missing device or a
+ *     failed launch is reported, never silently computed on the host.
+ */
+#ifndef LRE_CUDA_H
+#define LRE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LRE_ABI_VERSION 1
+
+typedef enum lre_status {
+  LRE_OK = 0,
+  LRE_ERR_INVALID_ARGUMENT = 1, /* shape / pointer / parameter rejected     */
+  LRE_ERR_CUDA = 2,             /* a CUDA runtime call or launch failed      */
+  LRE_ERR_OUT_OF_MEMORY = 3,    /* device or pinned allocation failed        */
+  LRE_ERR_NO_DEVICE = 4,        /* no usable sm_100 device                   */
+  LRE_ERR_TIMEOUT = 5,          /* a bounded device-side wait expired        */
+  LRE_ERR_INJECTED = 6,         /* host-side fault injection fired           */
+  LRE_ERR_BUSY = 7              /* admission refused (device budget)         */
+} lre_status;
+
+/* X-Trans `filters` sentinel (core/accelerator.h:179). */
+#define LRE_FILTERS_XTRANS 9u
+
+typedef struct lre_ctx lre_ctx;
+
+/* ---------------------------------------------------------------- context */
+/* Create a context on `device` (GPUAccelerator::initialize,
+ * core/gpu_accelerator.mm:47-105).  One context owns a stream, a growable
+ * device workspace and pinned staging buffers. */
+lre_status lre_create(int device, lre_ctx** out);
+void lre_destroy(lre_ctx* ctx);
+/* Message of the last failure on this context (never NULL). */
+const char* lre_last_error(const lre_ctx* ctx);
+/* GPUAccelerator::get_device_info (core/gpu_accelerator.h:25). */
+lre_status lre_device_info(lre_ctx* ctx, char* buf, size_t buflen);
+/* GPUAccelerator::is_available (core/gpu_accelerator.h:24). */
+int lre_is_available(void);
+int lre_abi_version(void);
+/* Use a caller-owned cudaStream_t for all later work (NULL: own stream). */
+lre_status lre_set_stream(lre_ctx* ctx, void* cuda_stream);
+void* lre_get_stream(lre_ctx* ctx);
+lre_status lre_synchronize(lre_ctx* ctx);
+/* Pre-size the device workspace (bytes); later calls reuse it. */
+lre_status lre_reserve_workspace(lre_ctx* ctx, size_t bytes);
+size_t lre_workspace_bytes(const lre_ctx* ctx);
+/* Number of kernels this context has launched so far. */
+uint64_t lre_launch_count(const lre_ctx* ctx);
+/* Page-locked host memory for fast transfers (PageAlignedAllocator,
+ * core/accelerator.h:24-53, is the reference's analogue). */
+lre_status lre_host_alloc(lre_ctx* ctx, size_t bytes, void** out);
+lre_status lre_host_free(lre_ctx* ctx, void* p);
+/* Host-side fault injection for failure-path tests: the next `countdown`-th
+ * device operation on this context fails with LRE_ERR_INJECTED before any
+ * work is enqueued (0 disables).  Never touches the GPU. */
+void lre_inject_fault(lre_ctx* ctx, int countdown);
+
+/* ------------------------------------------------ stages, host buffers */
+/* GPUAccelerator::demosaic_bayer_amaze (core/gpu_accelerator.h:35-39;
+ * CPU semantics core/cpu_accelerator.cpp:1635-1653, AMaZE then a 4-px
+ * border interpolation).  `raw_rgb` is the reference's sparse (H,W,3) raw
+ * buffer: only each site's own channel is read. */
+lre_status lre_demosaic_bayer_amaze(lre_ctx* ctx, const float* raw_rgb, float* rgb, size_t width,
+                                    size_t height, uint32_t filters, const float cam_mul[4],
+                                    float maximum_value);
+/* GPUAccelerator::demosaic_xtrans_1pass / _3pass (core/gpu_accelerator.h:42-53;
+ * core/cpu_accelerator.cpp:2767-2784).  `color_matrix` is accepted for
+ * signature parity; the reference's YPbPr 3-pass does not use it. */
+lre_status lre_demosaic_xtrans_1pass(lre_ctx* ctx, const float* raw_rgb, float* rgb, size_t width,
+                                     size_t height, const char xtrans[36],
+                                     const float color_matrix[12], float maximum_value);
+lre_status lre_demosaic_xtrans_3pass(lre_ctx* ctx, const float* raw_rgb, float* rgb, size_t width,
+                                     size_t height, const char xtrans[36],
+                                     const float color_matrix[12], float maximum_value);
+/* GPUAccelerator::apply_white_balance (core/gpu_accelerator.h:62-66;
+ * core/cpu_accelerator.cpp:2789-2869).  Writes only each site's own
+ * channel of `rgb` (G2 into channel 1); other channels are left as they are. */
+lre_status lre_apply_white_balance(lre_ctx* ctx, const uint16_t* raw4, float* rgb, size_t width,
+                                   size_t height, const float wb[4], uint32_t filters,
+                                   const char xtrans[36]);
+/* GPUAccelerator::tone_mapping (core/gpu_accelerator.h:78-80;
+ * core/cpu_accelerator.cpp:3034-3068): ACES per channel times after_scale. */
+lre_status lre_tone_mapping(lre_ctx* ctx, const float* in, float* out, size_t width, size_t height,
+                            float after_scale);
+/* GPUAccelerator::apply_detail_preserving_tonemap (core/gpu_accelerator.h:94-95;
+ * CPU semantics core/libraw_wrapper.cpp:1389-1471). */
+lre_status lre_detail_tonemap(lre_ctx* ctx, const float* in, float* out, size_t width,
+                              size_t height);
+/* GPUAccelerator::enhance_micro_contrast (core/gpu_accelerator.h:85-90;
+ * core/cpu_accelerator.cpp:3130-3319).  `mask` (W*H floats) may be NULL. */
+lre_status lre_enhance_micro_contrast(lre_ctx* ctx, const float* in, float* out, size_t width,
+                                      size_t height, float threshold, float strength,
+                                      float target_contrast, const float* mask);
+/* GPUAccelerator::ca_register_lateral (core/gpu_accelerator.h:98-104;
+ * core/cpu_accelerator.cpp:3496-3673). */
+lre_status lre_ca_register_lateral(lre_ctx* ctx, const float* in, float* out, size_t width,
+                                   size_t height, int cell_size, int max_iterations,
+                                   float max_shift, float min_confidence, int pyramid_levels);
+/* GPUAccelerator::ca_axial_cleanup (core/gpu_accelerator.h:107-111;
+ * core/cpu_accelerator.cpp:3799-3928). */
+lre_status lre_ca_axial_cleanup(lre_ctx* ctx, const float* in, float* out, size_t width,
+                                size_t height, int radius, float epsilon, float strength);
+/* GPUAccelerator::defringe (core/gpu_accelerator.h:114-121;
+ * core/cpu_accelerator.cpp:3939-5064). */
+lre_status lre_defringe(lre_ctx* ctx, const float* in, float* out, size_t width, size_t height,
+                        float radius, float edge_threshold, float chroma_threshold, float strength,
+                        int defringe_green, float green_strength_scale);
+
+/* Integer pieces around the path (core/libraw_wrapper.cpp, bit-exact). */
+/* apply_black_level_correction (core/libraw_wrapper.cpp:401-491), in place.
+ * `cblack` has LibRaw's layout: [0..3] per channel, [4],[5] the positional
+ * pattern size, [6..] the pattern; `cblack_len` entries are read. */
+lre_status lre_black_level(lre_ctx* ctx, uint16_t* raw4, size_t width, size_t height,
+                           const unsigned* cblack, size_t cblack_len, unsigned black,
+                           unsigned maximum);
+/* adjust_maximum (core/libraw_wrapper.cpp:1010-1087): scans the CFA samples
+ * of a sparse raw buffer when *data_maximum == 0 and returns the adopted
+ * maximum in *maximum. */
+lre_status lre_adjust_maximum(lre_ctx* ctx, const float* raw_rgb, size_t width, size_t height,
+                              uint32_t filters, float threshold, float* data_maximum,
+                              float* maximum);
+/* ProcessedImageData.to_numpy quantisation (core/python_bindings.cpp:235-257):
+ * out = (uint16)(clamp(x,0,1)*65535 + 0.5) over n floats. */
+lre_status lre_quantize_u16(lre_ctx* ctx, const float* in, uint16_t* out, size_t n);
+lre_status lre_quantize_u8(lre_ctx* ctx, const float* in, uint8_t* out, size_t n);
+
+/* ------------------------------------------------ stages, device buffers */
+/* Same arithmetic as the host versions, on device pointers, asynchronous on
+ * the context stream.  `raw` is a DENSE float CFA mosaic (H*W floats). */
+lre_status lre_dev_demosaic_bayer_amaze(lre_ctx* ctx, const float* raw, float* rgb, size_t width,
+                                        size_t height, uint32_t filters, const float cam_mul[4],
+                                        float maximum_value);
+lre_status lre_dev_demosaic_xtrans(lre_ctx* ctx, const float* raw, float* rgb, size_t width,
+                                   size_t height, const char xtrans[36], float maximum_value,
+                                   int passes);
+lre_status lre_dev_tone_mapping(lre_ctx* ctx, const float* in, float* out, size_t width,
+                                size_t height, float after_scale);
+lre_status lre_dev_detail_tonemap(lre_ctx* ctx, const float* in, float* out, size_t width,
+                                  size_t height);
+lre_status lre_dev_enhance_micro_contrast(lre_ctx* ctx, const float* in, float* out, size_t width,
+                                          size_t height, float threshold, float strength,
+                                          float target_contrast, const float* mask);
+lre_status lre_dev_ca_register_lateral(lre_ctx* ctx, const float* in, float* out, size_t width,
+                                       size_t height, int cell_size, int max_iterations,
+                                       float max_shift, float min_confidence, int pyramid_levels);
+lre_status lre_dev_ca_axial_cleanup(lre_ctx* ctx, const float* in, float* out, size_t width,
+                                    size_t height, int radius, float epsilon, float strength);
+lre_status lre_dev_defringe(lre_ctx* ctx, const float* in, float* out, size_t width, size_t height,
+                            float radius, float edge_threshold, float chroma_threshold,
+                            float strength, int defringe_green, float green_strength_scale);
+lre_status lre_dev_quantize_u16(lre_ctx* ctx, const float* in, uint16_t* out, size_t n);
+
+/* ------------------------------------------------ develop pipeline */
+/* Stage switches and parameters of one develop request.  Field names and
+ * defaults follow ProcessingParams (core/accelerator.h:83-177); `cfa` is a
+ * LibRaw filters word or LRE_FILTERS_XTRANS (then `xtrans` is read). */
+typedef struct lre_develop_params {
+  uint32_t filters;
+  char xtrans[36];
+  float cam_mul[4];
+  float maximum_value;
+  int xtrans_passes; /* 1 or 3 */
+  int lateral_ca_correction;
+  int lateral_ca_cell_size;
+  int lateral_ca_max_iterations;
+  float lateral_ca_max_shift;
+  float lateral_ca_min_confidence;
+  int lateral_ca_pyramid_levels;
+  int axial_ca_correction;
+  int axial_ca_radius;
+  float axial_ca_epsilon;
+  float axial_ca_strength;
+  int defringe;
+  float defringe_radius;
+  float defringe_edge_threshold;
+  float defringe_chroma_threshold;
+  float defringe_strength;
+  int defringe_green;
+  float defringe_green_strength;
+  int tone_mapping; /* 0 off, 1 ACES(after_scale), 2 detail-preserving */
+  float tone_after_scale;
+  int output_bits; /* 32: float RGB out; 16: uint16 RGB out */
+  int stage_order; /* 0: reference order (lateral, axial, defringe, tone);
+                      1: demosaic, defringe, axial, tone */
+} lre_develop_params;
+
+/* Fill `p` with the reference defaults (ProcessingParams()). */
+void lre_develop_params_default(lre_develop_params* p);
+
+/* Plain per-image develop: dense float CFA mosaic (host) -> RGB (host, float
+ * or uint16 per output_bits).  One upload, device-resident intermediates,
+ * one download. */
+lre_status lre_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t width, size_t height,
+                       const lre_develop_params* params);
+/* Same on device buffers, asynchronous on the context stream. */
+lre_status lre_dev_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t width,
+                           size_t height, const lre_develop_params* params);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LRE_CUDA_H */

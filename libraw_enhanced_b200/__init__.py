@@ -1,0 +1,374 @@
+"""B200 (sm_100a) CUDA develop backend for libraw_enhanced.
+
+The product is ``liblre_cuda.so`` (C ABI: ``include/lre_cuda.h``).  This
+package is its Python face, mirroring the reference's operator surface for the
+develop hot path:
+
+* :class:`CudaAccelerator` -- the ``GPUAccelerator`` method set
+  (core/gpu_accelerator.h:18-118 of uniuyuni/libraw_enhanced) on numpy arrays
+  in the reference layouts (float32 ``(H, W, 3)``, uint16 ``(H, W, 4)``), and
+  ``dev_*`` variants on CUDA tensors (device pointers, asynchronous on the
+  accelerator's stream).
+* :func:`tone_mapping`, :func:`enhance_micro_contrast`, :func:`defringe` --
+  the standalone ``RawImage`` / ``LibRawWrapper`` numpy methods
+  (libraw_enhanced/high_level_api.py:465-546, core/libraw_wrapper.cpp:3098-3214)
+  with their argument names, defaults and shape errors.
+* :func:`develop` -- the plain per-image develop of a CFA mosaic
+  (core/libraw_wrapper.cpp:1477-1853 stage order) through ``lre_develop``.
+
+Everything runs on the GPU; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import FILTERS_XTRANS, DevelopParams, LibRawError
+
+__all__ = [
+    "CudaAccelerator",
+    "LibRawError",
+    "FILTERS_XTRANS",
+    "FILTERS",
+    "DevelopParams",
+    "develop",
+    "defringe",
+    "tone_mapping",
+    "enhance_micro_contrast",
+    "default_accelerator",
+]
+
+# LibRaw `filters` words of the four Bayer layouts.
+FILTERS = {"RGGB": 0x94949494, "BGGR": 0x16161616, "GRBG": 0x61616161, "GBRG": 0x49494949}
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def _rgb(image, name: str) -> np.ndarray:
+    a = np.asarray(image)
+    if a.ndim != 3 or a.shape[2] != 3:
+        raise ValueError(f"{name}: image must be shape (H, W, 3) float32")
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _xtrans_bytes(xtrans) -> C.Array:
+    buf = (C.c_char * 36)()
+    if xtrans is not None:
+        x = np.asarray(xtrans, dtype=np.int8).reshape(36)
+        C.memmove(buf, x.ctypes.data, 36)
+    return buf
+
+
+def _dptr(t) -> C.c_void_p:
+    """Device pointer of a CUDA tensor (torch) or an integer address."""
+    if isinstance(t, int):
+        return C.c_void_p(t)
+    if hasattr(t, "data_ptr"):
+        if not t.is_cuda or not t.is_contiguous():
+            raise ValueError("device buffers must be contiguous CUDA tensors")
+        return C.c_void_p(t.data_ptr())
+    raise TypeError("expected a CUDA tensor or a device address")
+
+
+class CudaAccelerator:
+    """The GPUAccelerator method set on one CUDA device.
+
+    Host methods take numpy arrays and are synchronous (result on return);
+    ``dev_*`` methods take CUDA tensors and enqueue on :attr:`stream`.
+    """
+
+    def __init__(self, device: int = 0):
+        self._lib = _lib.load()
+        h = C.c_void_p()
+        st = self._lib.lre_create(int(device), C.byref(h))
+        if st != _lib.LRE_OK:
+            raise LibRawError(st, f"lre_create(device={device}) failed (no usable sm_100 device?)")
+        self._h = h
+        self.device = int(device)
+
+    # ------------------------------------------------------------ plumbing
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.lre_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int) -> None:
+        if st != _lib.LRE_OK:
+            msg = self._lib.lre_last_error(self._h)
+            raise LibRawError(st, msg.decode() if msg else "")
+
+    def is_available(self) -> bool:
+        return bool(self._lib.lre_is_available())
+
+    def get_device_info(self) -> str:
+        buf = C.create_string_buffer(256)
+        self._check(self._lib.lre_device_info(self._h, buf, 256))
+        return buf.value.decode()
+
+    @property
+    def stream(self) -> int:
+        return int(self._lib.lre_get_stream(self._h) or 0)
+
+    def set_stream(self, cuda_stream: Optional[int]) -> None:
+        """Run later work on a caller-owned cudaStream_t (None: own stream)."""
+        self._check(self._lib.lre_set_stream(self._h, C.c_void_p(cuda_stream or 0)))
+
+    def synchronize(self) -> None:
+        self._check(self._lib.lre_synchronize(self._h))
+
+    def reserve_workspace(self, nbytes: int) -> None:
+        self._check(self._lib.lre_reserve_workspace(self._h, int(nbytes)))
+
+    @property
+    def launch_count(self) -> int:
+        return int(self._lib.lre_launch_count(self._h))
+
+    def inject_fault(self, countdown: int) -> None:
+        """Host-side fault injection: the countdown-th next call fails."""
+        self._lib.lre_inject_fault(self._h, int(countdown))
+
+    # ------------------------------------------------------------ stages (host)
+    def demosaic_bayer_amaze(self, raw_rgb, filters: int, cam_mul=(1.0, 1.0, 1.0, 1.0), maximum_value: float = 1.0):
+        """AMaZE + 4-px border fill of the reference's sparse (H, W, 3) raw buffer."""
+        raw = _rgb(raw_rgb, "demosaic_bayer_amaze")
+        out = np.empty_like(raw)
+        cm = np.asarray(cam_mul, dtype=np.float32)
+        self._check(
+            self._lib.lre_demosaic_bayer_amaze(
+                self._h, _ptr(raw), _ptr(out), raw.shape[1], raw.shape[0], int(filters), _ptr(cm), float(maximum_value)
+            )
+        )
+        return out
+
+    def demosaic_xtrans_1pass(self, raw_rgb, xtrans, color_matrix=None, maximum_value: float = 1.0):
+        return self._xtrans(raw_rgb, xtrans, color_matrix, maximum_value, 1)
+
+    def demosaic_xtrans_3pass(self, raw_rgb, xtrans, color_matrix=None, maximum_value: float = 1.0):
+        return self._xtrans(raw_rgb, xtrans, color_matrix, maximum_value, 3)
+
+    def _xtrans(self, raw_rgb, xtrans, color_matrix, maximum_value, passes):
+        raw = _rgb(raw_rgb, "demosaic_xtrans")
+        out = np.empty_like(raw)
+        cm = np.zeros(12, np.float32) if color_matrix is None else np.asarray(color_matrix, np.float32).reshape(12)
+        xt = _xtrans_bytes(xtrans)
+        fn = self._lib.lre_demosaic_xtrans_1pass if passes == 1 else self._lib.lre_demosaic_xtrans_3pass
+        self._check(fn(self._h, _ptr(raw), _ptr(out), raw.shape[1], raw.shape[0], xt, _ptr(cm), float(maximum_value)))
+        return out
+
+    def apply_white_balance(self, raw4, wb, filters: int, xtrans=None, out=None):
+        r = np.asarray(raw4)
+        if r.ndim != 3 or r.shape[2] != 4:
+            raise ValueError("apply_white_balance: raw buffer must be shape (H, W, 4) uint16")
+        r = np.ascontiguousarray(r, dtype=np.uint16)
+        h, w, _ = r.shape
+        o = np.zeros((h, w, 3), np.float32) if out is None else np.ascontiguousarray(out, np.float32)
+        wbv = np.asarray(wb, dtype=np.float32)
+        xt = _xtrans_bytes(xtrans)
+        self._check(self._lib.lre_apply_white_balance(self._h, _ptr(r), _ptr(o), w, h, _ptr(wbv), int(filters), xt))
+        return o
+
+    def tone_mapping(self, image, after_scale: float = 1.0):
+        a = _rgb(image, "tone_mapping")
+        out = np.empty_like(a)
+        self._check(self._lib.lre_tone_mapping(self._h, _ptr(a), _ptr(out), a.shape[1], a.shape[0], float(after_scale)))
+        return out
+
+    def apply_detail_preserving_tonemap(self, image):
+        a = _rgb(image, "apply_detail_preserving_tonemap")
+        out = np.empty_like(a)
+        self._check(self._lib.lre_detail_tonemap(self._h, _ptr(a), _ptr(out), a.shape[1], a.shape[0]))
+        return out
+
+    def enhance_micro_contrast(self, image, threshold: float, strength: float = 8.0, target_contrast: float = 0.06, mask=None):
+        a = _rgb(image, "enhance_micro_contrast")
+        out = np.empty_like(a)
+        mp = None
+        if mask is not None:
+            mask = np.ascontiguousarray(mask, dtype=np.float32)
+            if mask.size != a.shape[0] * a.shape[1]:
+                raise ValueError("enhance_micro_contrast: mask must hold H*W floats")
+            mp = _ptr(mask)
+        self._check(
+            self._lib.lre_enhance_micro_contrast(
+                self._h, _ptr(a), _ptr(out), a.shape[1], a.shape[0], float(threshold), float(strength), float(target_contrast), mp
+            )
+        )
+        return out
+
+    def ca_register_lateral(self, image, cell_size=96, max_iterations=3, max_shift=6.0, min_confidence=0.02, pyramid_levels=3):
+        a = _rgb(image, "ca_register_lateral")
+        out = np.empty_like(a)
+        self._check(
+            self._lib.lre_ca_register_lateral(
+                self._h, _ptr(a), _ptr(out), a.shape[1], a.shape[0], int(cell_size), int(max_iterations),
+                float(max_shift), float(min_confidence), int(pyramid_levels),
+            )
+        )
+        return out
+
+    def ca_axial_cleanup(self, image, radius=6, epsilon=1e-4, strength=0.3):
+        a = _rgb(image, "ca_axial_cleanup")
+        out = np.empty_like(a)
+        self._check(
+            self._lib.lre_ca_axial_cleanup(self._h, _ptr(a), _ptr(out), a.shape[1], a.shape[0], int(radius), float(epsilon), float(strength))
+        )
+        return out
+
+    def defringe(self, image, radius=10.0, edge_threshold=0.1, chroma_threshold=0.15, strength=10.0,
+                 defringe_green=False, green_strength_scale=0.3):
+        a = _rgb(image, "defringe")
+        out = np.empty_like(a)
+        self._check(
+            self._lib.lre_defringe(
+                self._h, _ptr(a), _ptr(out), a.shape[1], a.shape[0], float(radius), float(edge_threshold),
+                float(chroma_threshold), float(strength), int(bool(defringe_green)), float(green_strength_scale),
+            )
+        )
+        return out
+
+    def black_level(self, raw4, cblack, black: int, maximum: int):
+        r = np.ascontiguousarray(raw4, dtype=np.uint16).copy()
+        cb = np.asarray(list(cblack) + [0] * max(0, 6 - len(cblack)), dtype=np.uint32)
+        self._check(self._lib.lre_black_level(self._h, _ptr(r), r.shape[1], r.shape[0], _ptr(cb), cb.size, int(black), int(maximum)))
+        return r
+
+    def adjust_maximum(self, raw_rgb, filters: int, threshold: float, data_maximum: float, maximum: float):
+        a = _rgb(raw_rgb, "adjust_maximum")
+        dm = C.c_float(float(data_maximum))
+        mx = C.c_float(float(maximum))
+        self._check(self._lib.lre_adjust_maximum(self._h, _ptr(a), a.shape[1], a.shape[0], int(filters), float(threshold), C.byref(dm), C.byref(mx)))
+        return float(mx.value), float(dm.value)
+
+    def quantize(self, image, bits: int = 16):
+        a = np.ascontiguousarray(image, dtype=np.float32)
+        if bits == 16:
+            out = np.empty(a.shape, np.uint16)
+            self._check(self._lib.lre_quantize_u16(self._h, _ptr(a), _ptr(out), a.size))
+        elif bits == 8:
+            out = np.empty(a.shape, np.uint8)
+            self._check(self._lib.lre_quantize_u8(self._h, _ptr(a), _ptr(out), a.size))
+        else:
+            raise ValueError("bits must be 8 or 16")
+        return out
+
+    # ------------------------------------------------------------ develop
+    def develop(self, mosaic, params: DevelopParams, out=None):
+        m = np.ascontiguousarray(mosaic, dtype=np.float32)
+        if m.ndim != 2:
+            raise ValueError("develop: mosaic must be a dense (H, W) float32 CFA image")
+        h, w = m.shape
+        if out is None:
+            out = np.empty((h, w, 3), np.float32 if params.output_bits == 32 else np.uint16)
+        self._check(self._lib.lre_develop(self._h, _ptr(m), _ptr(out), w, h, C.byref(params)))
+        return out
+
+    # ------------------------------------------------------------ device variants
+    def dev_demosaic_bayer_amaze(self, raw, rgb, width, height, filters, cam_mul, maximum_value=1.0):
+        cm = np.asarray(cam_mul, dtype=np.float32)
+        self._check(self._lib.lre_dev_demosaic_bayer_amaze(self._h, _dptr(raw), _dptr(rgb), int(width), int(height), int(filters), _ptr(cm), float(maximum_value)))
+
+    def dev_demosaic_xtrans(self, raw, rgb, width, height, xtrans, maximum_value=1.0, passes=3):
+        self._check(self._lib.lre_dev_demosaic_xtrans(self._h, _dptr(raw), _dptr(rgb), int(width), int(height), _xtrans_bytes(xtrans), float(maximum_value), int(passes)))
+
+    def dev_tone_mapping(self, inp, out, width, height, after_scale=1.0):
+        self._check(self._lib.lre_dev_tone_mapping(self._h, _dptr(inp), _dptr(out), int(width), int(height), float(after_scale)))
+
+    def dev_detail_tonemap(self, inp, out, width, height):
+        self._check(self._lib.lre_dev_detail_tonemap(self._h, _dptr(inp), _dptr(out), int(width), int(height)))
+
+    def dev_enhance_micro_contrast(self, inp, out, width, height, threshold, strength=8.0, target_contrast=0.06, mask=None):
+        mp = None if mask is None else _dptr(mask)
+        self._check(self._lib.lre_dev_enhance_micro_contrast(self._h, _dptr(inp), _dptr(out), int(width), int(height), float(threshold), float(strength), float(target_contrast), mp))
+
+    def dev_ca_register_lateral(self, inp, out, width, height, cell_size=96, max_iterations=3, max_shift=6.0, min_confidence=0.02, pyramid_levels=3):
+        self._check(self._lib.lre_dev_ca_register_lateral(self._h, _dptr(inp), _dptr(out), int(width), int(height), int(cell_size), int(max_iterations), float(max_shift), float(min_confidence), int(pyramid_levels)))
+
+    def dev_ca_axial_cleanup(self, inp, out, width, height, radius=6, epsilon=1e-4, strength=0.3):
+        self._check(self._lib.lre_dev_ca_axial_cleanup(self._h, _dptr(inp), _dptr(out), int(width), int(height), int(radius), float(epsilon), float(strength)))
+
+    def dev_defringe(self, inp, out, width, height, radius=10.0, edge_threshold=0.1, chroma_threshold=0.15, strength=10.0, defringe_green=False, green_strength_scale=0.3):
+        self._check(self._lib.lre_dev_defringe(self._h, _dptr(inp), _dptr(out), int(width), int(height), float(radius), float(edge_threshold), float(chroma_threshold), float(strength), int(bool(defringe_green)), float(green_strength_scale)))
+
+    def dev_develop(self, mosaic, out, width, height, params: DevelopParams):
+        self._check(self._lib.lre_dev_develop(self._h, _dptr(mosaic), _dptr(out), int(width), int(height), C.byref(params)))
+
+
+def develop_params(**kw) -> DevelopParams:
+    """ProcessingParams-style develop settings (reference defaults), overridden by kw.
+
+    ``cfa`` may be a Bayer layout name, a LibRaw filters word, or a 6x6 X-Trans
+    pattern; ``tone_mapping`` is 0 (off), 1 (ACES) or 2 (detail-preserving).
+    """
+    lib = _lib.load()
+    p = DevelopParams()
+    lib.lre_develop_params_default(C.byref(p))
+    cfa = kw.pop("cfa", None)
+    if cfa is not None:
+        if isinstance(cfa, str):
+            p.filters = FILTERS[cfa]
+        elif np.ndim(cfa) == 2:
+            p.filters = FILTERS_XTRANS
+            x = np.asarray(cfa, dtype=np.int8).reshape(36)
+            C.memmove(p.xtrans, x.ctypes.data, 36)
+        else:
+            p.filters = int(cfa)
+    if "cam_mul" in kw:
+        for i, v in enumerate(kw.pop("cam_mul")):
+            p.cam_mul[i] = float(v)
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise TypeError(f"unknown develop parameter {k!r}")
+        setattr(p, k, v)
+    return p
+
+
+_default = None
+
+
+def default_accelerator() -> CudaAccelerator:
+    global _default
+    if _default is None:
+        _default = CudaAccelerator(0)
+    return _default
+
+
+def develop(mosaic, **kw):
+    """Plain per-image develop of a dense float32 CFA mosaic (see develop_params)."""
+    return default_accelerator().develop(mosaic, develop_params(**kw))
+
+
+# ---------------------------------------------------------------- standalone
+# RawImage.tone_mapping / enhance_micro_contrast / defringe
+# (libraw_enhanced/high_level_api.py:465-546 -> core/libraw_wrapper.cpp:3098-3214)
+def tone_mapping(image, after_scale: float = 1.0) -> np.ndarray:
+    return default_accelerator().tone_mapping(image, after_scale)
+
+
+def enhance_micro_contrast(image, threshold: float = -1.0, strength: float = 8.0, target_contrast: float = 0.06) -> np.ndarray:
+    """``threshold < 0`` means maximum/data_maximum in the reference; without a
+    loaded RAW the ratio is 1.0 (core/libraw_wrapper.cpp:3140-3142)."""
+    if threshold < 0.0:
+        threshold = 1.0
+    return default_accelerator().enhance_micro_contrast(image, threshold, strength, target_contrast)
+
+
+def defringe(image, radius: float = 10.0, strength: float = 10.0, defringe_green: bool = False) -> np.ndarray:
+    """Edge / chroma thresholds fixed at 0.1 / 0.15 as in defringe_numpy."""
+    return default_accelerator().defringe(image, radius, 0.1, 0.15, strength, defringe_green)

@@ -1,0 +1,141 @@
+"""ctypes binding of liblre_cuda.so (the C ABI in include/lre_cuda.h).
+
+The library is built in-tree by ``python -m libraw_enhanced_b200.build`` (or
+``__graft_entry__.build()``).  There is no CPU fallback: if the library is
+missing, or no sm_100 device is present, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblre_cuda.so")
+
+LRE_OK = 0
+STATUS_NAMES = {
+    0: "LRE_OK",
+    1: "LRE_ERR_INVALID_ARGUMENT",
+    2: "LRE_ERR_CUDA",
+    3: "LRE_ERR_OUT_OF_MEMORY",
+    4: "LRE_ERR_NO_DEVICE",
+    5: "LRE_ERR_TIMEOUT",
+    6: "LRE_ERR_INJECTED",
+    7: "LRE_ERR_BUSY",
+}
+FILTERS_XTRANS = 9
+
+
+class LibRawError(RuntimeError):
+    """Failure reported by the CUDA develop backend (mirrors libraw_enhanced's
+    LibRawError, core/python_bindings.cpp:503-505)."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+
+
+class DevelopParams(C.Structure):
+    _fields_ = [
+        ("filters", C.c_uint32),
+        ("xtrans", C.c_char * 36),
+        ("cam_mul", C.c_float * 4),
+        ("maximum_value", C.c_float),
+        ("xtrans_passes", C.c_int),
+        ("lateral_ca_correction", C.c_int),
+        ("lateral_ca_cell_size", C.c_int),
+        ("lateral_ca_max_iterations", C.c_int),
+        ("lateral_ca_max_shift", C.c_float),
+        ("lateral_ca_min_confidence", C.c_float),
+        ("lateral_ca_pyramid_levels", C.c_int),
+        ("axial_ca_correction", C.c_int),
+        ("axial_ca_radius", C.c_int),
+        ("axial_ca_epsilon", C.c_float),
+        ("axial_ca_strength", C.c_float),
+        ("defringe", C.c_int),
+        ("defringe_radius", C.c_float),
+        ("defringe_edge_threshold", C.c_float),
+        ("defringe_chroma_threshold", C.c_float),
+        ("defringe_strength", C.c_float),
+        ("defringe_green", C.c_int),
+        ("defringe_green_strength", C.c_float),
+        ("tone_mapping", C.c_int),
+        ("tone_after_scale", C.c_float),
+        ("output_bits", C.c_int),
+        ("stage_order", C.c_int),
+    ]
+
+
+_p = C.c_void_p
+_sz = C.c_size_t
+_f = C.c_float
+_i = C.c_int
+_st = C.c_int
+
+# name -> (restype, argtypes); every symbol include/lre_cuda.h declares.
+SIGNATURES = {
+    "lre_create": (_st, [_i, C.POINTER(_p)]),
+    "lre_destroy": (None, [_p]),
+    "lre_last_error": (C.c_char_p, [_p]),
+    "lre_device_info": (_st, [_p, C.c_char_p, _sz]),
+    "lre_is_available": (_i, []),
+    "lre_abi_version": (_i, []),
+    "lre_set_stream": (_st, [_p, _p]),
+    "lre_get_stream": (_p, [_p]),
+    "lre_synchronize": (_st, [_p]),
+    "lre_reserve_workspace": (_st, [_p, _sz]),
+    "lre_workspace_bytes": (_sz, [_p]),
+    "lre_launch_count": (C.c_uint64, [_p]),
+    "lre_host_alloc": (_st, [_p, _sz, C.POINTER(_p)]),
+    "lre_host_free": (_st, [_p, _p]),
+    "lre_inject_fault": (None, [_p, _i]),
+    "lre_demosaic_bayer_amaze": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _p, _f]),
+    "lre_demosaic_xtrans_1pass": (_st, [_p, _p, _p, _sz, _sz, _p, _p, _f]),
+    "lre_demosaic_xtrans_3pass": (_st, [_p, _p, _p, _sz, _sz, _p, _p, _f]),
+    "lre_apply_white_balance": (_st, [_p, _p, _p, _sz, _sz, _p, C.c_uint32, _p]),
+    "lre_tone_mapping": (_st, [_p, _p, _p, _sz, _sz, _f]),
+    "lre_detail_tonemap": (_st, [_p, _p, _p, _sz, _sz]),
+    "lre_enhance_micro_contrast": (_st, [_p, _p, _p, _sz, _sz, _f, _f, _f, _p]),
+    "lre_ca_register_lateral": (_st, [_p, _p, _p, _sz, _sz, _i, _i, _f, _f, _i]),
+    "lre_ca_axial_cleanup": (_st, [_p, _p, _p, _sz, _sz, _i, _f, _f]),
+    "lre_defringe": (_st, [_p, _p, _p, _sz, _sz, _f, _f, _f, _f, _i, _f]),
+    "lre_black_level": (_st, [_p, _p, _sz, _sz, _p, _sz, C.c_uint, C.c_uint]),
+    "lre_adjust_maximum": (_st, [_p, _p, _sz, _sz, C.c_uint32, _f, C.POINTER(_f), C.POINTER(_f)]),
+    "lre_quantize_u16": (_st, [_p, _p, _p, _sz]),
+    "lre_quantize_u8": (_st, [_p, _p, _p, _sz]),
+    "lre_dev_demosaic_bayer_amaze": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _p, _f]),
+    "lre_dev_demosaic_xtrans": (_st, [_p, _p, _p, _sz, _sz, _p, _f, _i]),
+    "lre_dev_tone_mapping": (_st, [_p, _p, _p, _sz, _sz, _f]),
+    "lre_dev_detail_tonemap": (_st, [_p, _p, _p, _sz, _sz]),
+    "lre_dev_enhance_micro_contrast": (_st, [_p, _p, _p, _sz, _sz, _f, _f, _f, _p]),
+    "lre_dev_ca_register_lateral": (_st, [_p, _p, _p, _sz, _sz, _i, _i, _f, _f, _i]),
+    "lre_dev_ca_axial_cleanup": (_st, [_p, _p, _p, _sz, _sz, _i, _f, _f]),
+    "lre_dev_defringe": (_st, [_p, _p, _p, _sz, _sz, _f, _f, _f, _f, _i, _f]),
+    "lre_dev_quantize_u16": (_st, [_p, _p, _p, _sz]),
+    "lre_develop_params_default": (None, [C.POINTER(DevelopParams)]),
+    "lre_develop": (_st, [_p, _p, _p, _sz, _sz, C.POINTER(DevelopParams)]),
+    "lre_dev_develop": (_st, [_p, _p, _p, _sz, _sz, C.POINTER(DevelopParams)]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load() -> C.CDLL:
+    """Load liblre_cuda.so (raises if it was not built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    f"{LIB_PATH} is missing: build it with `python -m libraw_enhanced_b200.build` "
+                    "(there is no CPU fallback for the develop backend)"
+                )
+            lib = C.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib

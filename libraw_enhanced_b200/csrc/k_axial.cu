@@ -1,0 +1,345 @@
+// k_axial.cu -- axial chromatic-aberration cleanup: cross-channel guided
+// filter of R and B with G as the guide, edge-gated blend.
+//
+// Semantics follow core/cpu_accelerator.cpp:3799-3928
+// (CPUAccelerator::ca_axial_cleanup) with guided_filter_with_shared_guide
+// (:3725-3777) and box_mean (:3703-3716):
+//   * R, G, B are normalised by norm = max(1e-6, max G) (float multiply by
+//     1/norm, exactly as the reference);
+//   * box means use an edge-truncated (2r+1)^2 window; the reference builds
+//     double summed-area tables, here every window sum is accumulated in
+//     double directly (sliding sums), which equals the SAT difference up to
+//     double rounding;
+//   * a = cov(G,X) / (var(G) + eps), b = mean(X) - a mean(G) in double, stored
+//     as float; q = mean(a) * G + mean(b) in double, stored as float;
+//   * edge weight w = smoothstep(0.01, 0.06, boxmean_r(|central grad G|));
+//   * out = (X (1 - s w) + q s w) * norm, G passes through.
+//
+// B200 design: ONE fused kernel per image.  A CTA owns a T x T output tile,
+// stages the normalised (T+4r)^2 input region in shared memory once, and runs
+// both box-filter levels, the a/b solve, the edge gate and the blend out of
+// shared memory, so HBM sees 12 B/px in + 12 B/px out (the algorithmic
+// minimum) plus halo re-reads that hit L2.  The only other pass is the global
+// max(G) reduction that the normalisation needs before any tile can start.
+#include "common.cuh"
+#include "lre_internal.h"
+
+namespace lre {
+
+namespace {
+
+constexpr int AX_THREADS = 512;
+
+struct AxGeom {
+  int T, r, IN, AB;
+  size_t off_g, off_r, off_b, off_h0, off_h1, off_mi, off_vi, off_ar, off_br, off_ab, off_bb, off_er, bytes;
+};
+
+__host__ __device__ inline AxGeom ax_geom(int T, int r) {
+  AxGeom g;
+  g.T = T;
+  g.r = r;
+  g.IN = T + 4 * r;
+  g.AB = T + 2 * r;
+  size_t o = 0;
+  auto take = [&](size_t b) {
+    size_t cur = o;
+    o += (b + 15) & ~size_t(15);
+    return cur;
+  };
+  size_t in2 = (size_t)g.IN * g.IN, hb = (size_t)g.IN * g.AB, ab2 = (size_t)g.AB * g.AB;
+  g.off_h0 = take(hb * 8);
+  g.off_h1 = take(hb * 8);
+  g.off_mi = take(ab2 * 8);
+  g.off_vi = take(ab2 * 8);
+  g.off_g = take(in2 * 4);
+  g.off_r = take(in2 * 4);
+  g.off_b = take(in2 * 4);
+  g.off_ar = take(ab2 * 4);
+  g.off_br = take(ab2 * 4);
+  g.off_ab = take(ab2 * 4);
+  g.off_bb = take(ab2 * 4);
+  g.off_er = take(ab2 * 4);
+  g.bytes = o;
+  return g;
+}
+
+// Sliding horizontal window sums: dst[j][k] = sum_{t=0..2r} val(j, k + t)
+// for j < rows, k < cols_out.  Rows are split into segments so every thread
+// has work; inside a segment the sum slides with one add and one subtract.
+template <typename F>
+__device__ void hsum(double* dst, int rows, int cols_out, int r, F val) {
+  const int seg = 8;
+  const int nseg = (cols_out + seg - 1) / seg;
+  for (int item = threadIdx.x; item < rows * nseg; item += blockDim.x) {
+    int j = item / nseg, s = item % nseg;
+    int k0 = s * seg, k1 = min(cols_out, k0 + seg);
+    double acc = 0.0;
+    for (int t = 0; t <= 2 * r; t++) acc += val(j, k0 + t);
+    dst[j * cols_out + k0] = acc;
+    for (int k = k0 + 1; k < k1; k++) {
+      acc += val(j, k + 2 * r);
+      acc -= val(j, k - 1);
+      dst[j * cols_out + k] = acc;
+    }
+  }
+}
+
+// Sliding vertical sums over a row-major [rows_in][cols] double buffer:
+// out(j, k) = sum_{t=0..2r} src[(j+t)*cols + k], handed to `emit(j, k, sum)`.
+template <typename E>
+__device__ void vsum(const double* src, int rows_out, int cols, int r, E emit) {
+  const int seg = 8;
+  const int nseg = (rows_out + seg - 1) / seg;
+  for (int item = threadIdx.x; item < cols * nseg; item += blockDim.x) {
+    int k = item % cols, s = item / cols;
+    int j0 = s * seg, j1 = min(rows_out, j0 + seg);
+    double acc = 0.0;
+    for (int t = 0; t <= 2 * r; t++) acc += src[(j0 + t) * cols + k];
+    emit(j0, k, acc);
+    for (int j = j0 + 1; j < j1; j++) {
+      acc += src[(j + 2 * r) * cols + k];
+      acc -= src[(j - 1) * cols + k];
+      emit(j, k, acc);
+    }
+  }
+}
+
+__device__ __forceinline__ int win_count(int p, int r, int n) {
+  int lo = p - r < 0 ? 0 : p - r;
+  int hi = p + r > n - 1 ? n - 1 : p + r;
+  return hi - lo + 1;
+}
+
+template <int T>
+__global__ void __launch_bounds__(AX_THREADS, 1)
+    k_axial_fused(const float* __restrict__ src, float* __restrict__ dst, int W, int H, int r, float eps,
+                  float strength, const float* __restrict__ d_maxg) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const AxGeom g = ax_geom(T, r);
+  double* h0 = reinterpret_cast<double*>(smem + g.off_h0);
+  double* h1 = reinterpret_cast<double*>(smem + g.off_h1);
+  double* mI = reinterpret_cast<double*>(smem + g.off_mi);
+  double* vI = reinterpret_cast<double*>(smem + g.off_vi);
+  float* sG = reinterpret_cast<float*>(smem + g.off_g);
+  float* sR = reinterpret_cast<float*>(smem + g.off_r);
+  float* sB = reinterpret_cast<float*>(smem + g.off_b);
+  float* aR = reinterpret_cast<float*>(smem + g.off_ar);
+  float* bR = reinterpret_cast<float*>(smem + g.off_br);
+  float* aB = reinterpret_cast<float*>(smem + g.off_ab);
+  float* bB = reinterpret_cast<float*>(smem + g.off_bb);
+  float* er = reinterpret_cast<float*>(smem + g.off_er);
+
+  const int IN = g.IN, AB = g.AB;
+  const int x0 = blockIdx.x * T, y0 = blockIdx.y * T;
+  const int ix0 = x0 - 2 * r, iy0 = y0 - 2 * r;  // global coords of input region origin
+  const int ax0 = x0 - r, ay0 = y0 - r;          // global coords of a/b region origin
+
+  const float norm_ref = fmaxf(*d_maxg, 1e-6f);
+  const float inv_norm = 1.f / norm_ref;
+
+  // 1. stage normalised R, G, B (zeros outside the image).
+  for (int i = threadIdx.x; i < IN * IN; i += blockDim.x) {
+    int gy = iy0 + i / IN, gx = ix0 + i % IN;
+    float r_ = 0.f, g_ = 0.f, b_ = 0.f;
+    if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
+      const float* p = src + ((size_t)gy * W + gx) * 3;
+      r_ = p[0] * inv_norm;
+      g_ = p[1] * inv_norm;
+      b_ = p[2] * inv_norm;
+    }
+    sR[i] = r_;
+    sG[i] = g_;
+    sB[i] = b_;
+  }
+  __syncthreads();
+
+  // 2. guide statistics mean(G), var(G) over the a/b region.
+  hsum(h0, IN, AB, r, [&](int j, int k) { return (double)sG[j * IN + k]; });
+  hsum(h1, IN, AB, r, [&](int j, int k) {
+    float v = sG[j * IN + k];
+    return (double)(v * v);
+  });
+  __syncthreads();
+  vsum(h0, AB, AB, r, [&](int j, int k, double s) {
+    int gy = ay0 + j, gx = ax0 + k;
+    double m = 0.0;
+    if (gx >= 0 && gx < W && gy >= 0 && gy < H) m = s / (double)(win_count(gx, r, W) * win_count(gy, r, H));
+    mI[j * AB + k] = m;
+  });
+  __syncthreads();
+  vsum(h1, AB, AB, r, [&](int j, int k, double s) {
+    int gy = ay0 + j, gx = ax0 + k;
+    double v = 0.0;
+    if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
+      double mII = s / (double)(win_count(gx, r, W) * win_count(gy, r, H));
+      double m = mI[j * AB + k];
+      v = mII - m * m;
+    }
+    vI[j * AB + k] = v;
+  });
+  __syncthreads();
+
+  // 3. per-channel a, b (R then B), sharing the guide statistics.
+  for (int ch = 0; ch < 2; ch++) {
+    const float* sX = ch == 0 ? sR : sB;
+    float* aX = ch == 0 ? aR : aB;
+    float* bX = ch == 0 ? bR : bB;
+    hsum(h0, IN, AB, r, [&](int j, int k) { return (double)sX[j * IN + k]; });
+    hsum(h1, IN, AB, r, [&](int j, int k) { return (double)(sG[j * IN + k] * sX[j * IN + k]); });
+    __syncthreads();
+    // mean(X) into aX temporarily as double is not possible (float); keep the
+    // double mean in vI's sibling: reuse h0's first AB*AB doubles after the
+    // vertical pass would clobber its input, so compute both sums per pixel
+    // in one vertical sweep over the two buffers.
+    {
+      const int seg = 8;
+      const int nseg = (AB + seg - 1) / seg;
+      for (int item = threadIdx.x; item < AB * nseg; item += blockDim.x) {
+        int k = item % AB, s = item / AB;
+        int j0 = s * seg, j1 = min(AB, j0 + seg);
+        double sp = 0.0, sip = 0.0;
+        for (int t = 0; t <= 2 * r; t++) {
+          sp += h0[(j0 + t) * AB + k];
+          sip += h1[(j0 + t) * AB + k];
+        }
+        for (int j = j0; j < j1; j++) {
+          if (j > j0) {
+            sp += h0[(j + 2 * r) * AB + k];
+            sp -= h0[(j - 1) * AB + k];
+            sip += h1[(j + 2 * r) * AB + k];
+            sip -= h1[(j - 1) * AB + k];
+          }
+          int gy = ay0 + j, gx = ax0 + k;
+          float a_f = 0.f, b_f = 0.f;
+          if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
+            double area = (double)(win_count(gx, r, W) * win_count(gy, r, H));
+            double mp = sp / area, mIp = sip / area;
+            double mi = mI[j * AB + k];
+            double cov = mIp - mi * mp;
+            double a = cov / (vI[j * AB + k] + (double)eps);
+            double b = mp - a * mi;
+            a_f = (float)a;
+            b_f = (float)b;
+          }
+          aX[j * AB + k] = a_f;
+          bX[j * AB + k] = b_f;
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // 4. edge magnitude |(G[x+1]-G[x-1], G[y+1]-G[y-1])| on the interior.
+  for (int i = threadIdx.x; i < AB * AB; i += blockDim.x) {
+    int j = i / AB, k = i % AB;
+    int gy = ay0 + j, gx = ax0 + k;
+    float e = 0.f;
+    if (gx >= 1 && gx < W - 1 && gy >= 1 && gy < H - 1) {
+      int c = (j + r) * IN + (k + r);
+      float gxv = sG[c + 1] - sG[c - 1];
+      float gyv = sG[c + IN] - sG[c - IN];
+      e = sqrtf(gxv * gxv + gyv * gyv);
+    }
+    er[i] = e;
+  }
+  __syncthreads();
+
+  // 5. second box level and blend.  Each thread owns a fixed set of output
+  // pixels; the three sweeps (R, B, edge) keep their results in registers.
+  constexpr int PER = (T * T + AX_THREADS - 1) / AX_THREADS;
+  float qR[PER], qB[PER], ew[PER];
+  for (int pass = 0; pass < 3; pass++) {
+    if (pass < 2) {
+      const float* aX = pass == 0 ? aR : aB;
+      const float* bX = pass == 0 ? bR : bB;
+      hsum(h0, AB, T, r, [&](int j, int k) { return (double)aX[j * AB + k]; });
+      hsum(h1, AB, T, r, [&](int j, int k) { return (double)bX[j * AB + k]; });
+    } else {
+      hsum(h0, AB, T, r, [&](int j, int k) { return (double)er[j * AB + k]; });
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+      int i = threadIdx.x + q * AX_THREADS;
+      if (i >= T * T) break;
+      int j = i / T, k = i % T;
+      int gy = y0 + j, gx = x0 + k;
+      if (gx >= W || gy >= H) continue;
+      double area = (double)(win_count(gx, r, W) * win_count(gy, r, H));
+      double s0 = 0.0, s1 = 0.0;
+      for (int t = 0; t <= 2 * r; t++) {
+        s0 += h0[(j + t) * T + k];
+        if (pass < 2) s1 += h1[(j + t) * T + k];
+      }
+      if (pass < 2) {
+        double ma = s0 / area, mb = s1 / area;
+        float I = sG[(j + 2 * r) * IN + (k + 2 * r)];
+        float qv = (float)(ma * (double)I + mb);
+        if (pass == 0) qR[q] = qv; else qB[q] = qv;
+      } else {
+        double m = s0 / area;
+        float t = clampf(((float)m - 0.01f) / 0.05f, 0.f, 1.f);
+        ew[q] = t * t * (3.f - 2.f * t);
+      }
+    }
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    int i = threadIdx.x + q * AX_THREADS;
+    if (i >= T * T) break;
+    int j = i / T, k = i % T;
+    int gy = y0 + j, gx = x0 + k;
+    if (gx >= W || gy >= H) continue;
+    int c = (j + 2 * r) * IN + (k + 2 * r);
+    float w = strength * ew[q];
+    float r_out = sR[c] * (1.f - w) + qR[q] * w;
+    float b_out = sB[c] * (1.f - w) + qB[q] * w;
+    size_t o = ((size_t)gy * W + gx) * 3;
+    float gsrc = src[o + 1];
+    dst[o + 0] = r_out * norm_ref;
+    dst[o + 1] = gsrc;
+    dst[o + 2] = b_out * norm_ref;
+  }
+}
+
+int pick_tile(int r) { return r <= 8 ? 32 : 16; }
+
+}  // namespace
+
+size_t ws_bytes_axial(size_t w, size_t h, int radius) {
+  (void)radius;
+  // out-of-place copy when the caller runs in place (tiles read halos of
+  // their neighbours' inputs).
+  return w * h * 3 * sizeof(float);
+}
+
+lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, size_t h, int radius, float eps,
+                           float strength, const float* d_max_g) {
+  if (radius < 1) radius = 1;
+  if (radius > 16) return fail(c, LRE_ERR_INVALID_ARGUMENT, "ca_axial_cleanup: radius > 16 is not supported");
+  strength = fminf(fmaxf(strength, 0.f), 1.f);
+  int T = pick_tile(radius);
+  AxGeom g = ax_geom(T, radius);
+  const float* src = in;
+  if (in == out) {
+    float* tmp = reinterpret_cast<float*>(c->ws.take(w * h * 3 * sizeof(float)));
+    if (!tmp) return fail(c, LRE_ERR_OUT_OF_MEMORY, "ca_axial_cleanup: workspace too small");
+    LRE_CUDA_TRY(c, cudaMemcpyAsync(tmp, in, w * h * 3 * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+    src = tmp;
+  }
+  dim3 grid((unsigned)((w + T - 1) / T), (unsigned)((h + T - 1) / T));
+  if (T == 32) {
+    LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_axial_fused<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.bytes));
+    k_axial_fused<32><<<grid, AX_THREADS, g.bytes, c->stream>>>(src, out, (int)w, (int)h, radius, eps, strength, d_max_g);
+  } else {
+    LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_axial_fused<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.bytes));
+    k_axial_fused<16><<<grid, AX_THREADS, g.bytes, c->stream>>>(src, out, (int)w, (int)h, radius, eps, strength, d_max_g);
+  }
+  count_launch(c);
+  return check_launch(c, "ca_axial_cleanup");
+}
+
+}  // namespace lre

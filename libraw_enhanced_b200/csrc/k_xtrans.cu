@@ -1,0 +1,662 @@
+// k_xtrans.cu -- X-Trans demosaic: fast 1-pass interpolation and the 3-pass
+// Markesteijn interpolation (RawTherapee's algorithm as ported in
+// libraw_enhanced, YPbPr derivative variant), plus the X-Trans border fill.
+//
+// Semantics: core/cpu_accelerator.cpp:1664-2762 (XTrans_Processor):
+//   xtrans_border_interpolate (:1806-1861), run_3pass (:1870-2676),
+//   run_1pass (:2679-2762).
+//
+// 3-pass device design: the reference's 114 x 114 tiles (step 98, origin 3)
+// are kept -- its homogeneity maps read outside the rows a tile computes at
+// the first/last tile rows and columns, so the tiling is part of the result.
+// One CTA runs one tile; the row scans whose column walk is data-pattern
+// driven (green min/max, green interpolation, green recalculation, R/B
+// fills) run one row per thread in the reference's column order; the
+// derivative, homogeneity and averaging steps run one pixel per thread.
+// Tile planes (8 directions x 114^2 RGB, derivatives, homogeneity maps) live
+// in a per-CTA global scratch slab; positions a tile reads without computing
+// read zeros (a freshly allocated reference buffer).
+#include <cfloat>
+#include <cstring>
+
+#include "common.cuh"
+#include "lre_internal.h"
+
+namespace lre {
+
+namespace {
+
+constexpr int XTS = 114;
+constexpr int NDIR = 8;
+constexpr int XT_THREADS = 256;
+
+struct XtParams {
+  char xt[6][6];
+  short allhex0[3][3][8];
+  short allhex1[3][3][8];
+  int sgrow, sgcol;
+  int right_shift[3];
+};
+
+struct XtArgs {
+  const float* raw;
+  int cstride;
+  float* rgb_out;
+  int W, H;
+  float maximum;
+  int n_top, n_left;
+  unsigned char* scratch;
+  int* tile_counter;
+  XtParams P;
+};
+
+struct XtSlab {
+  float* rgb;           // [NDIR][XTS][XTS][3]
+  float2* gmm;          // [XTS][XTS/2] (min, max)
+  float* drv;           // [NDIR][XTS-10][XTS-10]
+  unsigned char* homo;  // [NDIR][XTS][XTS]
+  unsigned char* homosum;
+  unsigned char* homosummax;  // [XTS][XTS]
+};
+
+constexpr size_t kRgbBytes = (size_t)NDIR * XTS * XTS * 3 * 4;
+constexpr size_t kGmmBytes = (size_t)XTS * (XTS / 2) * 8;
+constexpr size_t kDrvBytes = (size_t)NDIR * (XTS - 10) * (XTS - 10) * 4;
+constexpr size_t kHomoBytes = (size_t)NDIR * XTS * XTS;
+constexpr size_t kHmaxBytes = (size_t)XTS * XTS;
+constexpr size_t kXtSlabBytes = ((kRgbBytes + kGmmBytes + kDrvBytes + 2 * kHomoBytes + kHmaxBytes + 255) / 256) * 256;
+
+__device__ XtSlab make_xt_slab(unsigned char* base) {
+  XtSlab s;
+  s.rgb = reinterpret_cast<float*>(base);
+  base += kRgbBytes;
+  s.gmm = reinterpret_cast<float2*>(base);
+  base += kGmmBytes;
+  s.drv = reinterpret_cast<float*>(base);
+  base += kDrvBytes;
+  s.homo = base;
+  base += kHomoBytes;
+  s.homosum = base;
+  base += kHomoBytes;
+  s.homosummax = base;
+  return s;
+}
+
+__device__ __forceinline__ int xfc(const XtParams& P, int row, int col) { return P.xt[(row + 6) % 6][(col + 6) % 6]; }
+__device__ __forceinline__ int xisgreen(const XtParams& P, int row, int col) { return P.xt[row % 3][col % 3] & 1; }
+
+__device__ __forceinline__ float xraw(const XtArgs& A, int row, int col) {
+  const size_t i = (size_t)row * A.W + col;
+  const float v = A.cstride == 1 ? A.raw[i] : A.raw[i * 3 + xfc(A.P, row, col)];
+  return v / A.maximum;
+}
+// raw_buffer_hex (:1691-1695): linear offset from (row, col), colour of the
+// landing site.
+__device__ __forceinline__ float xraw_hex(const XtArgs& A, int row, int col, int hex) {
+  const long long pos = (long long)row * A.W + col + hex;
+  const int r = (int)(pos / A.W), c = (int)(pos % A.W);
+  const float v = A.cstride == 1 ? A.raw[pos] : A.raw[pos * 3 + xfc(A.P, r, c)];
+  return v / A.maximum;
+}
+
+// std::max(low, std::min(val, high)) -- LIM of core/metal/shader_common.h.
+__device__ __forceinline__ float LIMf(float val, float low, float high) {
+  float m = (high < val) ? high : val;
+  return (low < m) ? m : low;
+}
+__device__ __forceinline__ float SQRf(float x) { return x * x; }
+
+// --------------------------------------------------------- border fill
+__device__ void xtrans_border_px(const XtArgs& A, int row, int col) {
+  const float weight[3][3] = {{0.25f, 0.5f, 0.25f}, {0.5f, 0.f, 0.5f}, {0.25f, 0.5f, 0.25f}};
+  const int W = A.W, H = A.H;
+  float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  int v = (row == 0) ? 0 : -1;
+  for (int y = (row > 0) ? row - 1 : 0; y < row + 2 && y < H; y++, v++) {
+    int h = (col == 0) ? 0 : -1;
+    for (int x = (col > 0) ? col - 1 : 0; x < col + 2 && x < W; x++, h++) {
+      const int f = xfc(A.P, y, x);
+      sum[f] += xraw(A, y, x) * weight[v + 1][h + 1];
+      sum[f + 3] += weight[v + 1][h + 1];
+    }
+  }
+  float* o = A.rgb_out + ((size_t)row * W + col) * 3;
+  switch (xfc(A.P, row, col)) {
+    case 0:
+      o[0] = xraw(A, row, col);
+      o[1] = (sum[1] / sum[4]);
+      o[2] = (sum[2] / sum[5]);
+      break;
+    case 1:
+      if (sum[3] == 0.f) {
+        const float r = xraw(A, row, col);
+        o[0] = o[1] = o[2] = r;
+      } else {
+        o[0] = (sum[0] / sum[3]);
+        o[1] = xraw(A, row, col);
+        o[2] = (sum[2] / sum[5]);
+      }
+      break;
+    case 2:
+      o[0] = (sum[0] / sum[3]);
+      o[1] = (sum[1] / sum[4]);
+      o[2] = xraw(A, row, col);
+      break;
+  }
+}
+
+__global__ void k_xtrans_border(XtArgs A, int border) {
+  const int W = A.W, H = A.H;
+  const long long n_tb = 2LL * border * W;
+  const long long n_lr = 2LL * border * (H - 2 * border > 0 ? H - 2 * border : 0);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n_tb + n_lr; k += (long long)gridDim.x * blockDim.x) {
+    int row, col;
+    if (k < n_tb) {
+      const int b = (int)(k / W);
+      col = (int)(k % W);
+      row = b < border ? b : H - 2 * border + b;
+    } else {
+      const long long q = k - n_tb;
+      const int b = (int)(q % (2 * border));
+      row = border + (int)(q / (2 * border));
+      col = b < border ? b : W - 2 * border + b;
+    }
+    if (row < 0 || row >= H || col < 0 || col >= W) continue;
+    if (col >= border && col < W - border && row >= border && row < H - border) continue;
+    xtrans_border_px(A, row, col);
+  }
+}
+
+// --------------------------------------------------------- 1-pass (:2679-2762)
+__global__ void k_xtrans_1pass(XtArgs A) {
+  const float weight[3][3] = {{0.25f, 0.5f, 0.25f}, {0.5f, 0.0f, 0.5f}, {0.25f, 0.5f, 0.25f}};
+  const int W = A.W, H = A.H;
+  const long long n = (long long)(H - 2) * (W - 2);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int row = 1 + (int)(k / (W - 2)), col = 1 + (int)(k % (W - 2));
+    float sum[3] = {0.f, 0.f, 0.f};
+    for (int v = -1; v <= 1; v++)
+      for (int h = -1; h <= 1; h++) {
+        const int sr = row + v, sc = col + h;
+        const int c = xfc(A.P, sr, sc);
+        const float raw_val = xraw(A, sr, sc);
+        sum[c] += raw_val * weight[v + 1][h + 1];
+      }
+    float rgb[3];
+    switch (xfc(A.P, row, col)) {
+      case 0:
+        rgb[0] = xraw(A, row, col);
+        rgb[1] = sum[1] * 0.5f;
+        rgb[2] = sum[2];
+        break;
+      case 1: {
+        rgb[1] = xraw(A, row, col);
+        if (xfc(A.P, row, col - 1) == xfc(A.P, row, col + 1)) {
+          rgb[0] = sum[0];
+          rgb[2] = sum[2];
+        } else {
+          rgb[0] = sum[0] * 1.3333333f;
+          rgb[2] = sum[2] * 1.3333333f;
+        }
+      } break;
+      default:
+        rgb[0] = sum[0];
+        rgb[1] = sum[1] * 0.5f;
+        rgb[2] = xraw(A, row, col);
+        break;
+    }
+    float* o = A.rgb_out + ((size_t)row * W + col) * 3;
+    o[0] = rgb[0];
+    o[1] = rgb[1];
+    o[2] = rgb[2];
+  }
+}
+
+// --------------------------------------------------------- 3-pass
+__global__ void __launch_bounds__(XT_THREADS) k_xtrans_3pass(XtArgs A) {
+  const int ts = XTS;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const XtParams& P = A.P;
+  XtSlab S = make_xt_slab(A.scratch + (size_t)blockIdx.x * kXtSlabBytes);
+  __shared__ int s_tile;
+  const int W = A.W, H = A.H;
+  const int dirv[4] = {1, ts, ts + 1, ts - 1};
+
+  for (;;) {
+    if (tid == 0) s_tile = atomicAdd(A.tile_counter, 1);
+    __syncthreads();
+    const int tile = s_tile;
+    __syncthreads();
+    if (tile >= A.n_top * A.n_left) break;
+    const int top = 3 + (tile / A.n_left) * (ts - 16);
+    const int left = 3 + (tile % A.n_left) * (ts - 16);
+    const int mrow_g = min(top + ts, H - 3);  // global row bound of the computations
+    const int mcol_g = min(left + ts, W - 3);
+
+    // fresh scratch (zeros)
+    {
+      float4* z = reinterpret_cast<float4*>(S.rgb);
+      const size_t n4 = kXtSlabBytes / 16;
+      for (size_t i = tid; i < n4; i += nth) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    float* rgb = S.rgb;
+    auto RGB = [&](int d, int lr, int lc) -> float* { return rgb + (((size_t)d * ts + lr) * ts + lc) * 3; };
+
+    // (a) green min / max per row (:1968-2053), one row per thread
+    for (int row = top + tid; row < mrow_g; row += nth) {
+      int leftstart = left;
+      for (; leftstart < mcol_g; leftstart++)
+        if (!xisgreen(P, row, leftstart)) break;
+      int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1 + (xfc(P, row, leftstart + 1) & 1));
+      float2* g = S.gmm + (size_t)(row - top) * (ts / 2);
+      auto mm = [&](int col, const short* hex) {
+        float minval = FLT_MAX, maxval = 0.f;
+        for (int c = 0; c < 6; c++) {
+          const float val = xraw_hex(A, row, col, hex[c]);
+          minval = minval < val ? minval : val;
+          maxval = maxval > val ? maxval : val;
+        }
+        return make_float2(minval, maxval);
+      };
+      if (coloffset == 3) {
+        const short* hex = P.allhex0[row % 3][leftstart % 3];
+        for (int col = leftstart; col < mcol_g; col += coloffset) g[(col - left) >> 1] = mm(col, hex);
+      } else {
+        int col = leftstart;
+        if (coloffset == 2) {
+          const short* hex = P.allhex0[row % 3][col % 3];
+          g[(col - left) >> 1] = mm(col, hex);
+          col += 2;
+        }
+        const short* hex = P.allhex0[row % 3][col % 3];
+        for (; col < mcol_g - 1; col += 3) {
+          const float2 v = mm(col, hex);
+          g[(col - left) >> 1] = v;
+          g[(col + 1 - left) >> 1] = v;
+        }
+        if (col < mcol_g) g[(col - left) >> 1] = mm(col, hex);
+      }
+    }
+    // native samples into direction 0 (:2055-2061)
+    for (int i = tid; i < (mrow_g - top) * (mcol_g - left); i += nth) {
+      const int lr = i / (mcol_g - left), lc = i % (mcol_g - left);
+      const int row = top + lr, col = left + lc;
+      RGB(0, lr, lc)[xfc(P, row, col)] = xraw(A, row, col);
+    }
+    __syncthreads();
+    // copy direction 0 to 1..3, all but the last float (:2067-2069)
+    for (int i = tid; i < ts * ts * 3 - 1; i += nth) {
+      const float v = rgb[i];
+      rgb[(size_t)1 * ts * ts * 3 + i] = v;
+      rgb[(size_t)2 * ts * ts * 3 + i] = v;
+      rgb[(size_t)3 * ts * ts * 3 + i] = v;
+    }
+    __syncthreads();
+    // (b) green in 4 directions (:2071-2127), one row per thread
+    for (int row = top + tid; row < mrow_g; row += nth) {
+      int leftstart = left;
+      for (; leftstart < mcol_g; leftstart++)
+        if (!xisgreen(P, row, leftstart)) break;
+      int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1 + (xfc(P, row, leftstart + 1) & 1));
+      const float2* g = S.gmm + (size_t)(row - top) * (ts / 2);
+      auto colors = [&](int col, const short* hex, float* color) {
+        color[0] = 0.6796875f * (xraw_hex(A, row, col, hex[1]) + xraw_hex(A, row, col, hex[0])) -
+                   0.1796875f * (xraw_hex(A, row, col, 2 * hex[1]) + xraw_hex(A, row, col, 2 * hex[0]));
+        color[1] = 0.87109375f * xraw_hex(A, row, col, hex[3]) + xraw_hex(A, row, col, hex[2]) * 0.12890625f +
+                   0.359375f * (xraw_hex(A, row, col, 0) - xraw_hex(A, row, col, -hex[2]));
+        for (int c = 0; c < 2; c++)
+          color[2 + c] = 0.640625f * xraw_hex(A, row, col, hex[4 + c]) + 0.359375f * xraw_hex(A, row, col, -2 * hex[4 + c]) +
+                         0.12890625f * (2.f * xraw_hex(A, row, col, 0) - xraw_hex(A, row, col, 3 * hex[4 + c]) -
+                                        xraw_hex(A, row, col, -3 * hex[4 + c]));
+      };
+      if (coloffset == 3) {
+        const short* hex = P.allhex0[row % 3][leftstart % 3];
+        for (int col = leftstart; col < mcol_g; col += coloffset) {
+          float color[4];
+          colors(col, hex, color);
+          const float2 mmv = g[(col - left) >> 1];
+          for (int c = 0; c < 4; c++) RGB(c, row - top, col - left)[1] = LIMf(color[c], mmv.x, mmv.y);
+        }
+      } else {
+        const short* hexmod[2] = {P.allhex0[row % 3][leftstart % 3], P.allhex0[row % 3][(leftstart + coloffset) % 3]};
+        for (int col = leftstart, hexindex = 0; col < mcol_g; col += coloffset, coloffset ^= 3, hexindex ^= 1) {
+          const short* hex = hexmod[hexindex];
+          float color[4];
+          colors(col, hex, color);
+          const float2 mmv = g[(col - left) >> 1];
+          for (int c = 0; c < 4; c++) RGB(c ^ 1, row - top, col - left)[1] = LIMf(color[c], mmv.x, mmv.y);
+        }
+      }
+    }
+    __syncthreads();
+
+    for (int pass = 0; pass < 3; pass++) {
+      if (pass == 1) {
+        // copy directions 0..3 into 4..7, all but the last float (:2131-2136)
+        const size_t n = (size_t)4 * ts * ts * 3 - 1;
+        for (size_t i = tid; i < n; i += nth) S.rgb[(size_t)4 * ts * ts * 3 + i] = S.rgb[i];
+        __syncthreads();
+        rgb = S.rgb + (size_t)4 * ts * ts * 3;
+      }
+      // (c) recalculate green from closer pixels (:2138-2183)
+      if (pass) {
+        for (int row = top + 2 + tid; row < mrow_g - 2; row += nth) {
+          int leftstart = left + 2;
+          for (; leftstart < mcol_g - 2; leftstart++)
+            if (!xisgreen(P, row, leftstart)) break;
+          int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1 + (xfc(P, row, leftstart + 1) & 1));
+          const float2* g = S.gmm + (size_t)(row - top) * (ts / 2);
+          if (coloffset == 3) {
+            int f = xfc(P, row, leftstart);
+            const short* hex = P.allhex1[row % 3][leftstart % 3];
+            for (int col = leftstart; col < mcol_g - 2; col += coloffset, f ^= 2) {
+              for (int d = 3; d < 6; d++) {
+                float* rix = RGB(d - 2, row - top, col - left);
+                const int o1 = hex[d] * 3, o2 = -2 * hex[d] * 3;
+                const float val =
+                    0.33333333f * (rix[o2 + 1] + 2 * (rix[o1 + 1] - rix[o1 + f]) - rix[o2 + f]) + rix[f];
+                const float2 mmv = g[(col - left) >> 1];
+                rix[1] = LIMf(val, mmv.x, mmv.y);
+              }
+            }
+          } else {
+            int f = xfc(P, row, leftstart);
+            const short* hexmod[2] = {P.allhex1[row % 3][leftstart % 3], P.allhex1[row % 3][(leftstart + coloffset) % 3]};
+            for (int col = leftstart, hexindex = 0; col < mcol_g - 2;
+                 col += coloffset, coloffset ^= 3, f = f ^ (coloffset & 2), hexindex ^= 1) {
+              const short* hex = hexmod[hexindex];
+              for (int d = 3; d < 6; d++) {
+                float* rix = RGB((d - 2) ^ 1, row - top, col - left);
+                const int o1 = hex[d] * 3, o2 = -2 * hex[d] * 3;
+                const float val =
+                    0.33333333f * (rix[o2 + 1] + 2 * (rix[o1 + 1] - rix[o1 + f]) - rix[o2 + f]) + rix[f];
+                const float2 mmv = g[(col - left) >> 1];
+                rix[1] = LIMf(val, mmv.x, mmv.y);
+              }
+            }
+          }
+        }
+        __syncthreads();
+      }
+      // (d) R/B at solitary green pixels (:2185-2222)
+      {
+        const int sgstartcol = (left - P.sgcol + 4) / 3 * 3 + P.sgcol;
+        const int row0 = (top - P.sgrow + 4) / 3 * 3 + P.sgrow;
+        for (int row = row0 + 3 * tid; row < mrow_g - 2; row += 3 * nth) {
+          float color[3][6];
+          for (int col = sgstartcol, h = xfc(P, row, col + 1); col < mcol_g - 2; col += 3, h ^= 2) {
+            float* rix = RGB(0, row - top, col - left);
+            float diff[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            for (int i = 1, d = 0; d < 6; d++, i ^= ts ^ 1, h ^= 2) {
+              for (int c = 0; c < 2; c++, h ^= 2) {
+                const int op = i * (1 << c) * 3, om = -i * (1 << c) * 3;
+                const float g = rix[1] + rix[1] - rix[op + 1] - rix[om + 1];
+                color[h][d] = g + rix[op + h] + rix[om + h];
+                if (d > 1) diff[d] += SQRf(rix[op + 1] - rix[om + 1] - rix[op + h] + rix[om + h]) + SQRf(g);
+              }
+              if (d > 2 && (d & 1))
+                if (diff[d - 1] < diff[d])
+                  for (int c = 0; c < 2; c++) color[c * 2][d] = color[c * 2][d - 1];
+              if ((d & 1) || d < 2) {
+                for (int c = 0; c < 2; c++) rix[c * 2] = 0.5f * color[c * 2][d];
+                rix += (size_t)ts * ts * 3;
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();
+      // (e) red for blue pixels and vice versa (:2224-2264)
+      for (int row = top + 3 + tid; row < mrow_g - 3; row += nth) {
+        int leftstart = left + 3;
+        for (; leftstart < mcol_g - 1; leftstart++)
+          if (!xisgreen(P, row, leftstart)) break;
+        int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1);
+        const int c = ((row - P.sgrow) % 3) ? ts : 1;
+        const int h = 3 * (c ^ ts ^ 1);
+        auto body = [&](int col, int f) {
+          float* rix = RGB(0, row - top, col - left);
+          for (int d = 0; d < 4; d++, rix += (size_t)ts * ts * 3) {
+            const int i = d > 1 || ((d ^ c) & 1) ||
+                                  ((fabsf(rix[1] - rix[c * 3 + 1]) + fabsf(rix[1] - rix[-c * 3 + 1])) <
+                                   2.f * (fabsf(rix[1] - rix[h * 3 + 1]) + fabsf(rix[1] - rix[-h * 3 + 1])))
+                              ? c
+                              : h;
+            rix[f] = rix[1] + 0.5f * (rix[i * 3 + f] + rix[-i * 3 + f] - rix[i * 3 + 1] - rix[-i * 3 + 1]);
+          }
+        };
+        if (coloffset == 3) {
+          int f = 2 - xfc(P, row, leftstart);
+          for (int col = leftstart; col < mcol_g - 3; col += coloffset, f ^= 2) body(col, f);
+        } else {
+          coloffset = xfc(P, row, leftstart + 1) == 1 ? 2 : 1;
+          int f = 2 - xfc(P, row, leftstart);
+          for (int col = leftstart; col < mcol_g - 3; col += coloffset, coloffset ^= 3, f = f ^ (coloffset & 2)) body(col, f);
+        }
+      }
+      __syncthreads();
+      // (f) R and B for 2x2 green blocks (:2266-2310)
+      {
+        int topstart = top + 2;
+        for (; topstart < mrow_g - 2; topstart++)
+          if ((topstart - P.sgrow) % 3) break;
+        int leftstart = left + 2;
+        for (; leftstart < mcol_g - 2; leftstart++)
+          if ((leftstart - P.sgcol) % 3) break;
+        const int coloffsetstart = 2 - (xfc(P, topstart, leftstart + 1) & 1);
+        for (int row = topstart + tid; row < mrow_g - 2; row += nth) {
+          if (!((row - P.sgrow) % 3)) continue;
+          const short* hexmod[2] = {P.allhex1[row % 3][leftstart % 3], P.allhex1[row % 3][(leftstart + coloffsetstart) % 3]};
+          for (int col = leftstart, coloffset = coloffsetstart, hexindex = 0; col < mcol_g - 2;
+               col += coloffset, coloffset ^= 3, hexindex ^= 1) {
+            float* rix = RGB(0, row - top, col - left);
+            const short* hex = hexmod[hexindex];
+            for (int d = 0; d < NDIR; d += 2, rix += (size_t)ts * ts * 3) {
+              const int o0 = hex[d] * 3, o1 = hex[d + 1] * 3;
+              if (hex[d] + hex[d + 1]) {
+                const float g = 3 * rix[1] - 2 * rix[o0 + 1] - rix[o1 + 1];
+                for (int c = 0; c < 4; c += 2) rix[c] = (g + 2 * rix[o0 + c] + rix[o1 + c]) * 0.33333333f;
+              } else {
+                const float g = 2 * rix[1] - rix[o0 + 1] - rix[o1 + 1];
+                for (int c = 0; c < 4; c += 2) rix[c] = (g + rix[o0 + c] + rix[o1 + c]) * 0.5f;
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+    rgb = S.rgb;
+    int mrow = mrow_g - top;
+    int mcol = mcol_g - left;
+
+    // (g) YPbPr derivatives (:2346-2405), yuv recomputed at the 3 taps
+    {
+      const int dn = XTS - 10;
+      const int rows = mrow - 10, cols = mcol - 10;
+      for (int i = tid; i < NDIR * rows * cols; i += nth) {
+        const int d = i / (rows * cols);
+        const int rem = i % (rows * cols);
+        const int row = 5 + rem / cols, col = 5 + rem % cols;
+        int f = dirv[d & 3];
+        f = f == 1 ? 1 : f - 8;
+        // yuv buffer offset f (width ts-8) -> tile offset
+        const int fr = (f == 1) ? 0 : 1, fc = (f == 1) ? 1 : (f - (XTS - 8));
+        auto yuv = [&](int r, int c, float& y, float& u, float& v) {
+          const float* p = RGB(d, r, c);
+          y = 0.2627f * p[0] + 0.6780f * p[1] + 0.0593f * p[2];
+          u = (p[2] - y) * 0.56433f;
+          v = (p[0] - y) * 0.67815f;
+        };
+        float y0, u0, v0, yp, up, vp, ym, um, vm;
+        yuv(row, col, y0, u0, v0);
+        yuv(row + fr, col + fc, yp, up, vp);
+        yuv(row - fr, col - fc, ym, um, vm);
+        S.drv[((size_t)d * dn + (row - 5)) * dn + (col - 5)] =
+            SQRf(2 * y0 - yp - ym) + SQRf(2 * u0 - up - um) + SQRf(2 * v0 - vp - vm);
+      }
+    }
+    __syncthreads();
+    // (h) homogeneity maps (:2407-2496)
+    {
+      const int dn = XTS - 10;
+      const int rows = mrow - 12, cols = mcol - 12;
+      for (int i = tid; i < rows * cols; i += nth) {
+        const int row = 6 + i / cols, col = 6 + i % cols;
+        auto D = [&](int d, int r, int c) { return S.drv[((size_t)d * dn + (r - 5)) * dn + (c - 5)]; };
+        float tr = D(0, row, col) < D(1, row, col) ? D(0, row, col) : D(1, row, col);
+        for (int d = 2; d < NDIR; d++) tr = (D(d, row, col) < tr ? D(d, row, col) : tr);
+        tr *= 8;
+        for (int d = 0; d < NDIR; d++) {
+          unsigned char temp = 0;
+          for (int v = -1; v <= 1; v++)
+            for (int h = -1; h <= 1; h++) temp += (D(d, row + v, col + h) <= tr ? 1 : 0);
+          S.homo[((size_t)d * ts + row) * ts + col] = temp;
+        }
+      }
+    }
+    __syncthreads();
+    if (H - top < ts + 4) mrow = H - top + 2;
+    if (W - left < ts + 4) mcol = W - left + 2;
+    // (j) 5x5 homogeneity sums and their max (:2504-2612)
+    const int r0 = min(top, 8), c0 = min(left, 8);
+    {
+      const int rows = mrow - 8 - r0, cols = mcol - 8 - c0;
+      for (int i = tid; i < rows * cols; i += nth) {
+        const int row = r0 + i / cols, col = c0 + i % cols;
+        unsigned char maxval = 0;
+        for (int d = 0; d < NDIR; d++) {
+          int s = 0;
+          for (int v = -2; v <= 2; v++)
+            for (int h = -2; h <= 2; h++) s += S.homo[((size_t)d * ts + row + v) * ts + col + h];
+          const unsigned char hs = (unsigned char)s;
+          S.homosum[((size_t)d * ts + row) * ts + col] = hs;
+          if (d == 0 || maxval < hs) maxval = hs;
+        }
+        maxval -= maxval >> 3;
+        S.homosummax[(size_t)row * ts + col] = maxval;
+      }
+    }
+    __syncthreads();
+    // (l) average the most homogeneous directions (:2614-2650)
+    {
+      const int rows = mrow - 8 - r0, cols = mcol - 8 - c0;
+      for (int i = tid; i < rows * cols; i += nth) {
+        const int row = r0 + i / cols, col = c0 + i % cols;
+        unsigned char hm[8];
+        for (int d = 0; d < 4; d++) hm[d] = S.homosum[((size_t)d * ts + row) * ts + col];
+        for (int d = 4; d < NDIR; d++) {
+          hm[d] = S.homosum[((size_t)d * ts + row) * ts + col];
+          if (hm[d - 4] < hm[d]) hm[d - 4] = 0;
+          else if (hm[d - 4] > hm[d]) hm[d] = 0;
+        }
+        float avg[4] = {0.f, 0.f, 0.f, 0.f};
+        const unsigned char maxval = S.homosummax[(size_t)row * ts + col];
+        for (int d = 0; d < NDIR; d++)
+          if (hm[d] >= maxval) {
+            const float* p = RGB(d, row, col);
+            for (int c = 0; c < 3; c++) avg[c] += p[c];
+            avg[3] += 1.f;
+          }
+        float* o = A.rgb_out + ((size_t)(row + top) * W + (col + left)) * 3;
+        o[0] = fmaxf(0.f, avg[0] / avg[3]);
+        o[1] = fmaxf(0.f, avg[1] / avg[3]);
+        o[2] = fmaxf(0.f, avg[2] / avg[3]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// allhex / solitary green / RightShift tables (:1887-1940), host side.
+XtParams make_xt_params(const char* xtrans, int width) {
+  XtParams P;
+  memcpy(P.xt, xtrans, 36);
+  const short orth[12] = {1, 0, 0, 1, -1, 0, 0, -1, 1, 0, 0, 1};
+  const short patt[2][16] = {{0, 1, 0, -1, 2, 0, -1, 0, 1, 1, 1, -1, 0, 0, 0, 0},
+                             {0, 1, 0, -2, 1, 0, -2, 0, 1, 1, -2, -2, 1, -1, -1, 1}};
+  auto isg = [&](int row, int col) { return P.xt[row % 3][col % 3] & 1; };
+  memset(P.allhex0, 0, sizeof(P.allhex0));
+  memset(P.allhex1, 0, sizeof(P.allhex1));
+  unsigned short sgrow = 0, sgcol = 0;
+  for (int row = 0; row < 3; row++)
+    for (int col = 0; col < 3; col++) {
+      const int gint = isg(row, col);
+      for (int ng = 0, d = 0; d < 10; d += 2) {
+        if (isg(row + orth[d] + 6, col + orth[d + 2] + 6)) ng = 0;
+        else ng++;
+        if (ng == 4) {
+          sgrow = row;
+          sgcol = col;
+        }
+        if (ng == gint + 1)
+          for (int c = 0; c < 8; c++) {
+            const int v = orth[d] * patt[gint][c * 2] + orth[d + 1] * patt[gint][c * 2 + 1];
+            const int h = orth[d + 2] * patt[gint][c * 2] + orth[d + 3] * patt[gint][c * 2 + 1];
+            P.allhex0[row][col][c ^ (gint * 2 & d)] = (short)(h + v * width);
+            P.allhex1[row][col][c ^ (gint * 2 & d)] = (short)(h + v * XTS);
+          }
+      }
+    }
+  P.sgrow = sgrow;
+  P.sgcol = sgcol;
+  for (int row = 0; row < 3; row++) {
+    int greencount = 0;
+    for (int col = 0; col < 3; col++) greencount += isg(row, col);
+    P.right_shift[row] = (greencount == 2);
+  }
+  return P;
+}
+
+}  // namespace
+
+size_t ws_bytes_xtrans(size_t w, size_t h, int passes) {
+  (void)w;
+  (void)h;
+  return passes == 1 ? 0 : 148u * kXtSlabBytes + 4096;
+}
+
+lre_status launch_xtrans(Context* c, const float* raw, int cstride, float* rgb, size_t w, size_t h, const char* xtrans,
+                         float maximum_value, int passes) {
+  XtArgs A;
+  A.raw = raw;
+  A.cstride = cstride;
+  A.rgb_out = rgb;
+  A.W = (int)w;
+  A.H = (int)h;
+  A.maximum = maximum_value;
+  // hexagon offsets are 16-bit (h + v * width, |v| <= 2), as in the reference
+  if (2 * w + 2 > 32767 && passes != 1)
+    return fail(c, LRE_ERR_INVALID_ARGUMENT, "demosaic_xtrans_3pass: width above 16382 overflows the hexagon offsets");
+  A.P = make_xt_params(xtrans, (int)w);
+  if (passes == 1) {
+    // border (1 px) first, then the interior (:2681-2760)
+    k_xtrans_border<<<grid_for(4 * (w + h), 256, c->sm_count * 2), 256, 0, c->stream>>>(A, 1);
+    if (w > 2 && h > 2)
+      k_xtrans_1pass<<<grid_for((w - 2) * (h - 2), 256, c->sm_count * 8), 256, 0, c->stream>>>(A);
+    count_launch(c, 2);
+    return check_launch(c, "demosaic_xtrans_1pass");
+  }
+  // tile grid of :1968-1969
+  int n_top = 0, n_left = 0;
+  for (int top = 3; top < (int)h - 19; top += XTS - 16) n_top++;
+  for (int left = 3; left < (int)w - 19; left += XTS - 16) n_left++;
+  A.n_top = n_top;
+  A.n_left = n_left;
+  const int tiles = n_top * n_left;
+  if (tiles > 0) {
+    int nblk = std::min(tiles, c->sm_count);
+    A.scratch = reinterpret_cast<unsigned char*>(c->ws.take((size_t)nblk * kXtSlabBytes));
+    A.tile_counter = reinterpret_cast<int*>(c->ws.take(256));
+    if (!A.scratch || !A.tile_counter) return fail(c, LRE_ERR_OUT_OF_MEMORY, "demosaic_xtrans_3pass: workspace too small");
+    LRE_CUDA_TRY(c, cudaMemsetAsync(A.tile_counter, 0, sizeof(int), c->stream));
+    k_xtrans_3pass<<<nblk, XT_THREADS, 0, c->stream>>>(A);
+    count_launch(c);
+  }
+  k_xtrans_border<<<grid_for(16 * (w + h), 256, c->sm_count * 2), 256, 0, c->stream>>>(A, 8);
+  count_launch(c);
+  return check_launch(c, "demosaic_xtrans_3pass");
+}
+
+}  // namespace lre

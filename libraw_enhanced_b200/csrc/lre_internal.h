@@ -1,0 +1,138 @@
+// lre_internal.h -- host-side runtime shared by the CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/lre_cuda.h"
+
+namespace lre {
+
+// One 256-byte-aligned bump arena on the device.  `reset()` releases every
+// allocation at once; the arena only grows (reallocation synchronises the
+// stream first, so pointers handed out earlier in the same call stay valid
+// only until the next reset).
+class Workspace {
+ public:
+  ~Workspace();
+  cudaError_t reserve(size_t bytes, cudaStream_t s);
+  // Returns nullptr when the arena is too small; callers size it first with
+  // reserve() from the plan of the stage they run.
+  void* take(size_t bytes);
+  void reset() { used_ = 0; }
+  void rewind(size_t mark) { used_ = mark; }
+  size_t capacity() const { return cap_; }
+  size_t used() const { return used_; }
+
+ private:
+  char* base_ = nullptr;
+  size_t cap_ = 0;
+  size_t used_ = 0;
+};
+
+// Planner for workspace use: stage code first sums its buffers with add(),
+// the context reserves the total, then the same sizes are taken in order.
+struct WsPlan {
+  size_t total = 0;
+  size_t add(size_t bytes) {
+    size_t off = total;
+    total += (bytes + 255) & ~size_t(255);
+    return off;
+  }
+};
+
+struct Context {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  Workspace ws;
+  std::string last_error;
+  std::atomic<uint64_t> launches{0};
+  int inject_countdown = 0;
+  // staging for host-buffer entry points
+  void* d_in = nullptr;
+  size_t d_in_cap = 0;
+  void* d_out = nullptr;
+  size_t d_out_cap = 0;
+  void* d_aux = nullptr;
+  size_t d_aux_cap = 0;
+  float* d_scalars = nullptr;  // 64 floats of per-call scalars (reductions)
+  std::mutex mu;               // one host-buffer call at a time per context
+  int sm_count = 148;
+};
+
+// Status helpers.
+lre_status fail(Context* c, lre_status st, const std::string& msg);
+lre_status cuda_fail(Context* c, cudaError_t e, const char* what);
+lre_status check_launch(Context* c, const char* what);
+lre_status check_injection(Context* c);
+
+#define LRE_CUDA_TRY(ctx, call)                                        \
+  do {                                                                 \
+    cudaError_t _e = (call);                                           \
+    if (_e != cudaSuccess) return ::lre::cuda_fail((ctx), _e, #call);  \
+  } while (0)
+
+#define LRE_TRY(expr)                    \
+  do {                                   \
+    lre_status _s = (expr);              \
+    if (_s != LRE_OK) return _s;         \
+  } while (0)
+
+// Grow-only device buffers used by the host-buffer entry points.
+lre_status ensure_buffer(Context* c, void** p, size_t* cap, size_t bytes);
+
+inline unsigned grid_for(size_t n, unsigned block, unsigned max_blocks = 148u * 16u) {
+  size_t g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > max_blocks) g = max_blocks;
+  return (unsigned)g;
+}
+
+inline void count_launch(Context* c, uint64_t n = 1) { c->launches.fetch_add(n); }
+
+// --- stage launchers (device pointers, enqueue on c->stream) -------------
+lre_status launch_tone_mapping(Context* c, const float* in, float* out, size_t n_px, float after_scale);
+lre_status launch_white_balance(Context* c, const uint16_t* raw4, float* rgb, size_t w, size_t h,
+                                const float wb[4], uint32_t filters, const char* xtrans);
+lre_status launch_black_level(Context* c, uint16_t* raw4, size_t w, size_t h, const unsigned* cblack,
+                              size_t cblack_len, unsigned black, unsigned maximum);
+lre_status launch_cfa_max(Context* c, const float* raw, int raw_c_stride, size_t w, size_t h,
+                          uint32_t filters, float* d_out);
+lre_status launch_quantize_u16(Context* c, const float* in, uint16_t* out, size_t n);
+lre_status launch_quantize_u8(Context* c, const float* in, uint8_t* out, size_t n);
+lre_status launch_pack_cfa(Context* c, const float* raw_rgb, float* dense, size_t w, size_t h,
+                           uint32_t filters, const char* xtrans);
+lre_status launch_channel_max(Context* c, const float* rgb, size_t n_px, int channel, float* d_out,
+                              bool clamp0);
+lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, size_t h, int radius,
+                           float eps, float strength, const float* d_max_g);
+lre_status launch_defringe(Context* c, const float* in, float* out, size_t w, size_t h, float radius,
+                           float edge_thr, float chroma_thr, float strength, bool green,
+                           float green_scale, const float* d_max_g);
+lre_status launch_detail_tonemap(Context* c, const float* in, float* out, size_t w, size_t h);
+lre_status launch_micro_contrast(Context* c, const float* in, float* out, size_t w, size_t h,
+                                 float threshold, float strength, float target, const float* mask);
+lre_status launch_lateral_ca(Context* c, const float* in, float* out, size_t w, size_t h, int cell,
+                             int iters, float max_shift, float min_conf, int levels);
+lre_status launch_amaze(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
+                        uint32_t filters, const float cam_mul[4], float maximum_value);
+lre_status launch_xtrans(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w,
+                         size_t h, const char* xtrans, float maximum_value, int passes);
+
+// Workspace bytes each stage needs for a w x h image (0 when none).
+size_t ws_bytes_axial(size_t w, size_t h, int radius);
+size_t ws_bytes_defringe(size_t w, size_t h, float radius);
+size_t ws_bytes_detail_tonemap(size_t w, size_t h);
+size_t ws_bytes_micro_contrast(size_t w, size_t h);
+size_t ws_bytes_lateral(size_t w, size_t h, int cell, int levels, bool in_place);
+size_t ws_bytes_amaze(size_t w, size_t h);
+size_t ws_bytes_xtrans(size_t w, size_t h, int passes);
+
+}  // namespace lre

@@ -1,0 +1,203 @@
+// pipeline.cu -- the plain per-image develop: one upload of the CFA mosaic,
+// every stage on device-resident buffers, one download.
+//
+// Stage order follows process_raw_to_rgb (core/libraw_wrapper.cpp:1477-1853):
+// demosaic -> tone map -> lateral CA -> axial CA -> defringe, or, with
+// stage_order = 1, demosaic -> defringe -> axial CA -> tone map (the order of
+// the 51 MP develop workload).  Only the axial guided filter reads a
+// neighbourhood of the previous stage's output after writing, so it is the
+// one stage run out of place (ping-pong between two RGB buffers); every
+// other stage runs in place.
+#include <algorithm>
+#include <cstring>
+
+#include "lre_internal.h"
+
+using lre::Context;
+
+namespace {
+
+Context* C(lre_ctx* p) { return reinterpret_cast<Context*>(p); }
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+size_t stage_ws(const lre_develop_params& p, size_t w, size_t h) {
+  size_t m = 0;
+  if (p.filters == LRE_FILTERS_XTRANS)
+    m = std::max(m, lre::ws_bytes_xtrans(w, h, p.xtrans_passes));
+  else
+    m = std::max(m, lre::ws_bytes_amaze(w, h));
+  if (p.lateral_ca_correction)
+    m = std::max(m, lre::ws_bytes_lateral(w, h, p.lateral_ca_cell_size, p.lateral_ca_pyramid_levels, true));
+  if (p.defringe) m = std::max(m, lre::ws_bytes_defringe(w, h, p.defringe_radius));
+  if (p.tone_mapping == 2) m = std::max(m, lre::ws_bytes_detail_tonemap(w, h));
+  return m + 4096;
+}
+
+lre_status validate(Context* c, const lre_develop_params* p, size_t w, size_t h) {
+  if (!p) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: null params");
+  if (w < 32 || h < 32) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: image smaller than 32x32");
+  if (w > (1u << 20) || h > (1u << 20) || w * h > (size_t(1) << 31))
+    return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: image too large");
+  if (p->filters != LRE_FILTERS_XTRANS && p->filters < 1000)
+    return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: filters is neither a Bayer word nor X-Trans");
+  if (p->output_bits != 32 && p->output_bits != 16)
+    return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: output_bits must be 32 or 16");
+  if (p->axial_ca_correction && p->axial_ca_radius > 16)
+    return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: axial_ca_radius > 16 is not supported");
+  return LRE_OK;
+}
+
+// Runs the stage chain on device buffers; returns the buffer holding the
+// final RGB in *result.
+lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb_b, size_t w, size_t h,
+                     const lre_develop_params& p, float** result) {
+  float* cur = rgb_a;
+  float* other = rgb_b;
+  const size_t mark = c->ws.used();
+  if (p.filters == LRE_FILTERS_XTRANS) {
+    LRE_TRY(lre::launch_xtrans(c, d_mosaic, 1, cur, w, h, p.xtrans, p.maximum_value, p.xtrans_passes == 1 ? 1 : 3));
+  } else {
+    LRE_TRY(lre::launch_amaze(c, d_mosaic, 1, cur, w, h, p.filters, p.cam_mul, p.maximum_value));
+  }
+  c->ws.rewind(mark);
+  auto tone = [&]() -> lre_status {
+    if (p.tone_mapping == 1) LRE_TRY(lre::launch_tone_mapping(c, cur, cur, w * h, p.tone_after_scale));
+    if (p.tone_mapping == 2) {
+      LRE_TRY(lre::launch_detail_tonemap(c, cur, cur, w, h));
+      c->ws.rewind(mark);
+    }
+    return LRE_OK;
+  };
+  auto lateral = [&]() -> lre_status {
+    if (!p.lateral_ca_correction) return LRE_OK;
+    LRE_TRY(lre::launch_lateral_ca(c, cur, cur, w, h, p.lateral_ca_cell_size, p.lateral_ca_max_iterations,
+                                   p.lateral_ca_max_shift, p.lateral_ca_min_confidence, p.lateral_ca_pyramid_levels));
+    c->ws.rewind(mark);
+    return LRE_OK;
+  };
+  auto axial = [&]() -> lre_status {
+    if (!p.axial_ca_correction) return LRE_OK;
+    float* dmax = c->d_scalars + 1;
+    LRE_TRY(lre::launch_channel_max(c, cur, w * h, 1, dmax, true));
+    LRE_TRY(lre::launch_axial_ca(c, cur, other, w, h, p.axial_ca_radius, p.axial_ca_epsilon, p.axial_ca_strength, dmax));
+    std::swap(cur, other);
+    c->ws.rewind(mark);
+    return LRE_OK;
+  };
+  auto defringe = [&]() -> lre_status {
+    if (!p.defringe) return LRE_OK;
+    LRE_TRY(lre::launch_defringe(c, cur, cur, w, h, p.defringe_radius, p.defringe_edge_threshold,
+                                 p.defringe_chroma_threshold, p.defringe_strength, p.defringe_green != 0,
+                                 p.defringe_green_strength, nullptr));
+    c->ws.rewind(mark);
+    return LRE_OK;
+  };
+  if (p.stage_order == 1) {
+    LRE_TRY(defringe());
+    LRE_TRY(axial());
+    LRE_TRY(tone());
+  } else {
+    LRE_TRY(tone());
+    LRE_TRY(lateral());
+    LRE_TRY(axial());
+    LRE_TRY(defringe());
+  }
+  *result = cur;
+  return LRE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void lre_develop_params_default(lre_develop_params* p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  // ProcessingParams defaults (core/accelerator.h:83-177)
+  p->filters = 0x94949494u;  // RGGB
+  p->cam_mul[0] = p->cam_mul[1] = p->cam_mul[2] = p->cam_mul[3] = 1.f;
+  p->maximum_value = 1.f;
+  p->xtrans_passes = 3;
+  p->lateral_ca_correction = 0;
+  p->lateral_ca_cell_size = 96;
+  p->lateral_ca_max_iterations = 3;
+  p->lateral_ca_max_shift = 6.0f;
+  p->lateral_ca_min_confidence = 0.02f;
+  p->lateral_ca_pyramid_levels = 3;
+  p->axial_ca_correction = 0;
+  p->axial_ca_radius = 6;
+  p->axial_ca_epsilon = 1e-4f;
+  p->axial_ca_strength = 0.3f;
+  p->defringe = 0;
+  p->defringe_radius = 10.0f;
+  p->defringe_edge_threshold = 0.1f;
+  p->defringe_chroma_threshold = 0.15f;
+  p->defringe_strength = 10.0f;
+  p->defringe_green = 0;
+  p->defringe_green_strength = 0.3f;
+  p->tone_mapping = 0;
+  p->tone_after_scale = 1.0f;
+  p->output_bits = 32;
+  p->stage_order = 0;
+}
+
+lre_status lre_dev_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t w, size_t h,
+                           const lre_develop_params* params) {
+  Context* c = C(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  if (!mosaic || !out) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: null buffer");
+  LRE_TRY(validate(c, params, w, h));
+  cudaSetDevice(c->device);
+  LRE_TRY(lre::check_injection(c));
+  const lre_develop_params& p = *params;
+  const size_t rgb_bytes = align256(w * h * 12);
+  const bool float_out = p.output_bits == 32;
+  c->ws.reset();
+  LRE_CUDA_TRY(c, c->ws.reserve((float_out ? 1 : 2) * rgb_bytes + stage_ws(p, w, h), c->stream));
+  float* rgb_a = float_out ? reinterpret_cast<float*>(out) : reinterpret_cast<float*>(c->ws.take(rgb_bytes));
+  float* rgb_b = reinterpret_cast<float*>(c->ws.take(rgb_bytes));
+  if (!rgb_a || !rgb_b) return lre::fail(c, LRE_ERR_OUT_OF_MEMORY, "develop: workspace too small");
+  float* res = nullptr;
+  LRE_TRY(run_chain(c, mosaic, rgb_a, rgb_b, w, h, p, &res));
+  if (float_out) {
+    if (res != out) LRE_CUDA_TRY(c, cudaMemcpyAsync(out, res, w * h * 12, cudaMemcpyDeviceToDevice, c->stream));
+  } else {
+    LRE_TRY(lre::launch_quantize_u16(c, res, reinterpret_cast<uint16_t*>(out), w * h * 3));
+  }
+  return LRE_OK;
+}
+
+lre_status lre_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t w, size_t h,
+                       const lre_develop_params* params) {
+  Context* c = C(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  if (!mosaic || !out) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: null buffer");
+  LRE_TRY(validate(c, params, w, h));
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  LRE_TRY(lre::check_injection(c));
+  const lre_develop_params& p = *params;
+  const size_t in_bytes = w * h * 4;
+  const size_t out_bytes = w * h * 3 * (p.output_bits == 16 ? 2 : 4);
+  LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, in_bytes));
+  LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, out_bytes));
+  const size_t rgb_bytes = align256(w * h * 12);
+  c->ws.reset();
+  LRE_CUDA_TRY(c, c->ws.reserve(2 * rgb_bytes + stage_ws(p, w, h), c->stream));
+  float* rgb_a = reinterpret_cast<float*>(c->ws.take(rgb_bytes));
+  float* rgb_b = reinterpret_cast<float*>(c->ws.take(rgb_bytes));
+  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, mosaic, in_bytes, cudaMemcpyHostToDevice, c->stream));
+  float* res = nullptr;
+  LRE_TRY(run_chain(c, reinterpret_cast<const float*>(c->d_in), rgb_a, rgb_b, w, h, p, &res));
+  if (p.output_bits == 16) {
+    LRE_TRY(lre::launch_quantize_u16(c, res, reinterpret_cast<uint16_t*>(c->d_out), w * h * 3));
+    LRE_CUDA_TRY(c, cudaMemcpyAsync(out, c->d_out, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    LRE_CUDA_TRY(c, cudaMemcpyAsync(out, res, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+  }
+  LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return LRE_OK;
+}
+
+}  // extern "C"

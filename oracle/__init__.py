@@ -1,0 +1,274 @@
+"""TEST INFRASTRUCTURE -- the oracle the CUDA develop path is checked against.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg import this package.  The product (``libraw_enhanced_b200``) never does.
+
+Two libraries back it, both built by ``oracle/Makefile``:
+
+* ``ref``  -- ``oracle/_ref/liblre_ref.so``: uniuyuni/libraw_enhanced's own
+  ``CPUAccelerator`` (core/cpu_accelerator.cpp) compiled from the reference
+  sources, behind the C ABI in ``oracle/ref_capi.cpp``.  This is the parity
+  reference for AMaZE, X-Trans, white balance, defringe, axial/lateral CA,
+  ACES tone mapping and micro-contrast.
+* ``port`` -- ``oracle/liblre_oracle.so``: a plain-C restatement
+  (``oracle/lre_oracle.c``) of the LibRaw-dependent pieces that cannot be
+  compiled here (black level, adjust_maximum, detail-preserving tone map,
+  output quantization, WB-multiplier derivation) plus restatements of ACES,
+  white balance, CFA indexing and border interpolation that are pinned against
+  ``ref`` by the CPU test-suite.
+
+All images are numpy arrays in the reference's layouts: float32 (H, W, 3)
+interleaved, uint16 (H, W, 4) raw.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "liblre_ref.so")
+PORT_SO = os.path.join(HERE, "liblre_oracle.so")
+
+_f = C.c_float
+_sz = C.c_size_t
+_p = C.c_void_p
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _img(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    assert a.ndim == 3 and a.shape[2] == 3, a.shape
+    return a
+
+
+class _Lib:
+    def __init__(self, path, sigs):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library missing: {path} (run `make -C oracle`)")
+        self.lib = C.CDLL(path)
+        for name, (res, args) in sigs.items():
+            fn = getattr(self.lib, name)
+            fn.restype = res
+            fn.argtypes = args
+
+
+_REF_SIGS = {
+    "ref_num_threads": (C.c_int, []),
+    "ref_set_num_threads": (None, [C.c_int]),
+    "ref_demosaic_bayer_amaze": (C.c_int, [_p, _p, _sz, _sz, C.c_uint32, _p, _f]),
+    "ref_demosaic_xtrans": (C.c_int, [_p, _p, _sz, _sz, _p, _p, _f, C.c_int]),
+    "ref_apply_white_balance": (C.c_int, [_p, _p, _sz, _sz, _p, C.c_uint32, _p]),
+    "ref_tone_mapping": (C.c_int, [_p, _p, _sz, _sz, _f]),
+    "ref_enhance_micro_contrast": (C.c_int, [_p, _p, _sz, _sz, _f, _f, _f, _p]),
+    "ref_defringe": (C.c_int, [_p, _p, _sz, _sz, _f, _f, _f, _f, C.c_int, _f]),
+    "ref_ca_register_lateral": (C.c_int, [_p, _p, _sz, _sz, C.c_int, C.c_int, _f, _f, C.c_int]),
+    "ref_ca_axial_cleanup": (C.c_int, [_p, _p, _sz, _sz, C.c_int, _f, _f]),
+    "ref_pre_interpolate": (C.c_int, [_p, _sz, _sz, C.c_uint32, _p, C.c_int]),
+}
+
+_PORT_SIGS = {
+    "port_fcol_bayer_native": (C.c_uint, [C.c_uint, C.c_uint, C.c_uint32]),
+    "port_fcol_bayer": (C.c_uint, [C.c_uint, C.c_uint, C.c_uint32]),
+    "port_fcol_xtrans": (C.c_uint, [C.c_uint, C.c_uint, _p]),
+    "port_black_level": (None, [_p, _sz, _sz, _p, C.c_uint, C.c_uint]),
+    "port_white_balance": (None, [_p, _p, _sz, _sz, _p, C.c_uint32, _p]),
+    "port_adjust_maximum": (_f, [_p, _sz, _sz, C.c_uint32, _f, C.POINTER(_f), _f]),
+    "port_tone_mapping": (None, [_p, _p, _sz, _f]),
+    "port_detail_tonemap": (C.c_longlong, [_p, _sz, _sz]),
+    "port_quantize_u16": (None, [_p, _p, _sz]),
+    "port_quantize_u8": (None, [_p, _p, _sz]),
+    "port_scale_mul": (None, [_p, C.c_int, _f, _p]),
+    "port_auto_wb": (None, [_p, _sz, _sz, C.c_uint32, _p, _p]),
+    "port_border_interpolate": (None, [_p, _sz, _sz, C.c_uint32, _sz]),
+}
+
+_ref = None
+_port = None
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        _ref = _Lib(REF_SO, _REF_SIGS).lib
+    return _ref
+
+
+def port():
+    global _port
+    if _port is None:
+        _port = _Lib(PORT_SO, _PORT_SIGS).lib
+    return _port
+
+
+def _xt(xtrans):
+    if xtrans is None:
+        return np.zeros(36, dtype=np.int8)
+    return np.ascontiguousarray(np.asarray(xtrans, dtype=np.int8).reshape(36))
+
+
+# ---------------------------------------------------------------- reference
+def set_threads(n: int) -> None:
+    ref().ref_set_num_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(ref().ref_num_threads())
+
+
+def amaze(raw_sparse, filters, cam_mul=(2.0, 1.0, 1.5, 1.0), maximum=1.0):
+    raw = _img(raw_sparse)
+    h, w, _ = raw.shape
+    out = np.zeros_like(raw)
+    cm = np.asarray(cam_mul, dtype=np.float32)
+    ok = ref().ref_demosaic_bayer_amaze(_ptr(raw), _ptr(out), w, h, int(filters), _ptr(cm), float(maximum))
+    assert ok
+    return out
+
+
+def xtrans(raw_sparse, xtrans_pattern, passes=3, maximum=1.0, color_matrix=None):
+    raw = _img(raw_sparse)
+    h, w, _ = raw.shape
+    out = np.zeros_like(raw)
+    cm = np.zeros(12, np.float32) if color_matrix is None else np.asarray(color_matrix, np.float32).reshape(12)
+    xt = _xt(xtrans_pattern)
+    ok = ref().ref_demosaic_xtrans(_ptr(raw), _ptr(out), w, h, _ptr(xt), _ptr(cm), float(maximum), int(passes))
+    assert ok
+    return out
+
+
+def white_balance(raw4, wb, filters, xtrans_pattern=None, out=None):
+    raw4 = np.ascontiguousarray(raw4, dtype=np.uint16)
+    h, w, _ = raw4.shape
+    out = np.zeros((h, w, 3), np.float32) if out is None else np.ascontiguousarray(out, np.float32)
+    wbv = np.asarray(wb, dtype=np.float32)
+    ok = ref().ref_apply_white_balance(_ptr(raw4), _ptr(out), w, h, _ptr(wbv), int(filters), _ptr(_xt(xtrans_pattern)))
+    assert ok
+    return out
+
+
+def tone_mapping(img, after_scale=1.0):
+    a = _img(img)
+    out = np.empty_like(a)
+    assert ref().ref_tone_mapping(_ptr(a), _ptr(out), a.shape[1], a.shape[0], float(after_scale))
+    return out
+
+
+def micro_contrast(img, threshold=0.5, strength=8.0, target=0.06, mask=None):
+    a = _img(img)
+    out = np.empty_like(a)
+    mp = None
+    if mask is not None:
+        mask = np.ascontiguousarray(mask, dtype=np.float32)
+        mp = _ptr(mask)
+    assert ref().ref_enhance_micro_contrast(
+        _ptr(a), _ptr(out), a.shape[1], a.shape[0], float(threshold), float(strength), float(target), mp
+    )
+    return out
+
+
+def defringe(img, radius=10.0, edge=0.1, chroma=0.15, strength=10.0, green=False, green_scale=0.3):
+    a = _img(img)
+    out = np.empty_like(a)
+    assert ref().ref_defringe(
+        _ptr(a), _ptr(out), a.shape[1], a.shape[0], float(radius), float(edge), float(chroma),
+        float(strength), int(bool(green)), float(green_scale),
+    )
+    return out
+
+
+def lateral_ca(img, cell=96, iters=3, max_shift=6.0, min_conf=0.02, levels=3):
+    a = _img(img)
+    out = np.empty_like(a)
+    assert ref().ref_ca_register_lateral(
+        _ptr(a), _ptr(out), a.shape[1], a.shape[0], int(cell), int(iters), float(max_shift), float(min_conf), int(levels)
+    )
+    return out
+
+
+def axial_ca(img, radius=6, eps=1e-4, strength=0.3):
+    a = _img(img)
+    out = np.empty_like(a)
+    assert ref().ref_ca_axial_cleanup(_ptr(a), _ptr(out), a.shape[1], a.shape[0], int(radius), float(eps), float(strength))
+    return out
+
+
+# ---------------------------------------------------------------- restatement
+def black_level(raw4, cblack, black, maximum):
+    """cblack: sequence of 6 + n ints (LibRaw layout)."""
+    a = np.ascontiguousarray(raw4, dtype=np.uint16).copy()
+    cb = np.zeros(6 + 4104, dtype=np.uint32)
+    cb[: len(cblack)] = np.asarray(cblack, dtype=np.uint32)
+    port().port_black_level(_ptr(a), a.shape[1], a.shape[0], _ptr(cb), int(black), int(maximum))
+    return a
+
+
+def port_white_balance(raw4, wb, filters, xtrans_pattern=None, out=None):
+    raw4 = np.ascontiguousarray(raw4, dtype=np.uint16)
+    h, w, _ = raw4.shape
+    out = np.zeros((h, w, 3), np.float32) if out is None else np.ascontiguousarray(out, np.float32).copy()
+    wbv = np.asarray(wb, dtype=np.float32)
+    port().port_white_balance(_ptr(raw4), _ptr(out), w, h, _ptr(wbv), int(filters), _ptr(_xt(xtrans_pattern)))
+    return out
+
+
+def adjust_maximum(rgb, filters, threshold, data_maximum, maximum):
+    a = _img(rgb)
+    dm = C.c_float(float(data_maximum))
+    m = port().port_adjust_maximum(_ptr(a), a.shape[1], a.shape[0], int(filters), float(threshold), C.byref(dm), float(maximum))
+    return float(m), float(dm.value)
+
+
+def port_tone_mapping(img, after_scale=1.0):
+    a = _img(img)
+    out = np.empty_like(a)
+    port().port_tone_mapping(_ptr(a), _ptr(out), a.shape[0] * a.shape[1], float(after_scale))
+    return out
+
+
+def detail_tonemap(img):
+    a = _img(img).copy()
+    port().port_detail_tonemap(_ptr(a), a.shape[1], a.shape[0])
+    return a
+
+
+def quantize_u16(img):
+    a = np.ascontiguousarray(img, dtype=np.float32)
+    out = np.empty(a.shape, np.uint16)
+    port().port_quantize_u16(_ptr(a), _ptr(out), a.size)
+    return out
+
+
+def quantize_u8(img):
+    a = np.ascontiguousarray(img, dtype=np.float32)
+    out = np.empty(a.shape, np.uint8)
+    port().port_quantize_u8(_ptr(a), _ptr(out), a.size)
+    return out
+
+
+def scale_mul(pre_mul, colors=3, maximum=1.0):
+    pm = np.asarray(pre_mul, dtype=np.float32)
+    out = np.empty(4, np.float32)
+    port().port_scale_mul(_ptr(pm), int(colors), float(maximum), _ptr(out))
+    return out
+
+
+def auto_wb(raw4, filters, xtrans_pattern=None):
+    a = np.ascontiguousarray(raw4, dtype=np.uint16)
+    out = np.empty(4, np.float32)
+    port().port_auto_wb(_ptr(a), a.shape[1], a.shape[0], int(filters), _ptr(_xt(xtrans_pattern)), _ptr(out))
+    return out
+
+
+def border_interpolate(rgb, filters, border=4):
+    a = _img(rgb).copy()
+    port().port_border_interpolate(_ptr(a), a.shape[1], a.shape[0], int(filters), int(border))
+    return a

@@ -1,0 +1,295 @@
+/*
+ * lre_oracle.c -- TEST INFRASTRUCTURE (oracle), never part of the product.
+ *
+ * A plain-C restatement of the pieces of libraw_enhanced's develop path that
+ * live in LibRaw-dependent files and therefore cannot be compiled from the
+ * reference here (LibRaw is not vendored).  Each function states the reference
+ * lines it follows.  Integer pieces are bit-exact restatements; the float
+ * pieces keep the reference's operation order (build with -ffp-contract=off).
+ *
+ * The rest of the hot path (AMaZE, X-Trans, defringe, axial/lateral CA, ACES,
+ * micro-contrast, white balance) is checked against the reference itself,
+ * compiled from its sources into oracle/_ref/liblre_ref.so.  A few of those
+ * are also restated here (ACES, white balance, border interpolation, CFA
+ * indexing) so the restatement can be pinned against the compiled reference.
+ */
+#include <math.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* core/metal/shader_common.h:63-75 */
+unsigned port_fcol_bayer_native(unsigned row, unsigned col, uint32_t filters) {
+  return filters >> ((((row << 1) & 14) | (col & 1)) << 1) & 3;
+}
+unsigned port_fcol_bayer(unsigned row, unsigned col, uint32_t filters) {
+  static const unsigned to3[4] = {0, 1, 2, 1};
+  return to3[port_fcol_bayer_native(row, col, filters)];
+}
+unsigned port_fcol_xtrans(unsigned row, unsigned col, const char xtrans[36]) {
+  return (unsigned)xtrans[((row + 6) % 6) * 6 + (col + 6) % 6];
+}
+
+/*
+ * core/libraw_wrapper.cpp:401-491 (apply_black_level_correction).
+ * mode 2: positional cblack[6+...] plus per-channel cblack[c];
+ * mode 1: per-channel cblack[c]; mode 0: global `black`.
+ * Every result is clamped to [0, maximum] and stored back as uint16.
+ * The mode is chosen exactly as the reference chooses it.
+ */
+void port_black_level(uint16_t* img4, size_t w, size_t h, const unsigned* cblack /* >= 6 + 4096 */,
+                      unsigned black, unsigned maximum) {
+  size_t total = w * h;
+  if (cblack[4] && cblack[5]) {
+    for (size_t q = 0; q < total; q++) {
+      int row = (int)(q / w), col = (int)(q % w);
+      int pos_black = (int)cblack[6 + (row % cblack[4]) * cblack[5] + (col % cblack[5])];
+      for (int c = 0; c < 4; c++) {
+        int v = img4[q * 4 + c];
+        v -= pos_black;
+        v -= (int)cblack[c];
+        if (v < 0) v = 0;
+        if (v > (int)maximum) v = (int)maximum;
+        img4[q * 4 + c] = (uint16_t)v;
+      }
+    }
+  } else if (cblack[0] || cblack[1] || cblack[2] || cblack[3]) {
+    for (size_t q = 0; q < total; q++)
+      for (int c = 0; c < 4; c++) {
+        int v = img4[q * 4 + c] - (int)cblack[c];
+        if (v < 0) v = 0;
+        if (v > (int)maximum) v = (int)maximum;
+        img4[q * 4 + c] = (uint16_t)v;
+      }
+  } else {
+    for (size_t q = 0; q < total; q++)
+      for (int c = 0; c < 4; c++) {
+        int v = img4[q * 4 + c] - (int)black;
+        if (v < 0) v = 0;
+        if (v > (int)maximum) v = (int)maximum;
+        img4[q * 4 + c] = (uint16_t)v;
+      }
+  }
+}
+
+/* core/cpu_accelerator.cpp:2808-2869 (apply_wb_bayer / apply_wb_xtrans) */
+void port_white_balance(const uint16_t* raw4, float* rgb, size_t w, size_t h, const float wb[4],
+                        uint32_t filters, const char xtrans[36]) {
+  for (size_t row = 0; row < h; row++)
+    for (size_t col = 0; col < w; col++) {
+      size_t i = row * w + col;
+      unsigned c = filters == 9 ? port_fcol_xtrans((unsigned)row, (unsigned)col, xtrans)
+                                : port_fcol_bayer_native((unsigned)row, (unsigned)col, filters);
+      float v = (float)raw4[i * 4 + c] * wb[c];
+      if (c == 3) c = 1;
+      rgb[i * 3 + c] = v;
+    }
+}
+
+/*
+ * core/libraw_wrapper.cpp:1010-1087 (adjust_maximum).  Returns the (possibly
+ * adjusted) maximum; *data_maximum is updated when it was 0 and had to be
+ * scanned from the CFA samples.
+ */
+float port_adjust_maximum(const float* rgb, size_t w, size_t h, uint32_t filters, float threshold,
+                          float* data_maximum, float maximum) {
+  if (threshold < 0.00001f) return maximum;
+  float thr = threshold > 0.99999f ? 0.75f : threshold;
+  float real_max = *data_maximum;
+  if (real_max == 0.f && rgb) {
+    float m = 0.f;
+    for (size_t row = 0; row < h; row++)
+      for (size_t col = 0; col < w; col++) {
+        float v = rgb[(row * w + col) * 3 + port_fcol_bayer((unsigned)row, (unsigned)col, filters)];
+        if (v > m) m = v;
+      }
+    real_max = m;
+    *data_maximum = m;
+  }
+  if (real_max > 0 && real_max < maximum && real_max > maximum * thr) return real_max;
+  return maximum;
+}
+
+/* core/cpu_accelerator.cpp:3034-3068 (ACES tone map, no clamp) */
+static float port_aces(float x) {
+  const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+  return (x * (a * x + b)) / (x * (c * x + d) + e);
+}
+void port_tone_mapping(const float* in, float* out, size_t n_px, float after_scale) {
+  for (size_t i = 0; i < n_px * 3; i++) out[i] = port_aces(in[i]) * after_scale;
+}
+
+/*
+ * core/libraw_wrapper.cpp:45-116 (box_filter_normalized): a separable
+ * sliding-window box mean with an edge-truncated window.  The running sum is
+ * updated add-after-emit exactly as the reference does; the order matters.
+ */
+static void port_box_filter(const float* src, float* dst, float* tmp, size_t w, size_t h, int r) {
+  size_t R = (size_t)r;
+  for (size_t y = 0; y < h; y++) {
+    const float* s = src + y * w;
+    float* t = tmp + y * w;
+    float sum = 0.f;
+    size_t first = w - 1 < R ? w - 1 : R;
+    for (size_t x = 0; x <= first; x++) sum += s[x];
+    for (size_t x = 0; x < w; x++) {
+      size_t left = x > R ? x - R : 0;
+      size_t right = w - 1 < x + R ? w - 1 : x + R;
+      t[x] = sum / (float)(right - left + 1);
+      size_t rm = x >= R ? x - R : w;
+      size_t add = x + R + 1;
+      if (rm < w) sum -= s[rm];
+      if (add < w) sum += s[add];
+    }
+  }
+  for (size_t x = 0; x < w; x++) {
+    float sum = 0.f;
+    size_t first = h - 1 < R ? h - 1 : R;
+    for (size_t y = 0; y <= first; y++) sum += tmp[y * w + x];
+    for (size_t y = 0; y < h; y++) {
+      size_t top = y > R ? y - R : 0;
+      size_t bot = h - 1 < y + R ? h - 1 : y + R;
+      dst[y * w + x] = sum / (float)(bot - top + 1);
+      size_t rm = y >= R ? y - R : h;
+      size_t add = y + R + 1;
+      if (rm < h) sum -= tmp[rm * w + x];
+      if (add < h) sum += tmp[add * w + x];
+    }
+  }
+}
+
+/*
+ * core/libraw_wrapper.cpp:1389-1471 (apply_detail_preserving_tonemap),
+ * in place on an interleaved (H,W,3) float image.  Returns the count of
+ * pixels whose gain was applied (the reference's `mapped_pixels`).
+ */
+long long port_detail_tonemap(float* rgb, size_t w, size_t h) {
+  size_t n = w * h;
+  if (n == 0) return 0;
+  const int radius = 12;
+  const float eps = 0.0025f, edge0 = 0.55f, edge1 = 0.90f;
+  float* guide = (float*)malloc(n * sizeof(float));
+  float* mean = (float*)malloc(n * sizeof(float));
+  float* work = (float*)malloc(n * sizeof(float));
+  float* b = (float*)malloc(n * sizeof(float));
+  float* tmp = (float*)malloc(n * sizeof(float));
+  for (size_t i = 0; i < n; i++) {
+    const float* p = rgb + i * 3;
+    float m = p[1] > p[2] ? p[1] : p[2];
+    m = p[0] > m ? p[0] : m;
+    guide[i] = m > 0.0f ? m : 0.0f;
+    work[i] = guide[i] * guide[i];
+  }
+  port_box_filter(guide, mean, tmp, w, h, radius);
+  port_box_filter(work, work, tmp, w, h, radius);
+  for (size_t i = 0; i < n; i++) {
+    float var = work[i] - mean[i] * mean[i];
+    var = var > 0.0f ? var : 0.0f;
+    float a = var / (var + eps);
+    work[i] = a;
+    b[i] = mean[i] * (1.0f - a);
+  }
+  port_box_filter(work, work, tmp, w, h, radius);
+  port_box_filter(b, b, tmp, w, h, radius);
+  long long mapped = 0;
+  for (size_t i = 0; i < n; i++) {
+    float base = work[i] * guide[i] + b[i];
+    base = base > 1e-6f ? base : 1e-6f;
+    float gain = port_aces(base) / base;
+    gain = gain < 0.0f ? 0.0f : (gain > 1.0f ? 1.0f : gain);
+    float t = (base - edge0) / (edge1 - edge0);
+    t = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
+    t = t * t * (3.0f - 2.0f * t);
+    if (t <= 0.0f) continue;
+    gain = 1.0f + (gain - 1.0f) * t;
+    rgb[i * 3 + 0] *= gain;
+    rgb[i * 3 + 1] *= gain;
+    rgb[i * 3 + 2] *= gain;
+    mapped++;
+  }
+  free(guide);
+  free(mean);
+  free(work);
+  free(b);
+  free(tmp);
+  return mapped;
+}
+
+/* core/python_bindings.cpp:235-257 (ProcessedImageData.to_numpy) */
+void port_quantize_u16(const float* in, uint16_t* out, size_t n) {
+  for (size_t i = 0; i < n; i++) {
+    float v = in[i];
+    v = v < 0.f ? 0.f : (v > 1.f ? 1.f : v);
+    out[i] = (uint16_t)(v * 65535.0f + 0.5f);
+  }
+}
+void port_quantize_u8(const float* in, uint8_t* out, size_t n) {
+  for (size_t i = 0; i < n; i++) {
+    float v = in[i];
+    v = v < 0.f ? 0.f : (v > 1.f ? 1.f : v);
+    out[i] = (uint8_t)(v * 255.0f + 0.5f);
+  }
+}
+
+/*
+ * core/libraw_wrapper.cpp:746-845 (scale_colors, camera-WB branch without a
+ * white-point sample): scale_mul[c] = pre_mul[c] / min(pre_mul), after the
+ * reference's pre_mul[1]/pre_mul[3] defaults; all ones when the minimum is
+ * not positive or maximum <= 0.
+ */
+void port_scale_mul(const float pre_mul_in[4], int colors, float maximum, float scale_mul[4]) {
+  float pre[4] = {pre_mul_in[0], pre_mul_in[1], pre_mul_in[2], pre_mul_in[3]};
+  if (pre[1] == 0) pre[1] = 1;
+  if (pre[3] == 0) pre[3] = colors < 4 ? pre[1] : 1;
+  double dmin = 1.7976931348623157e308;
+  for (int c = 0; c < 4; c++)
+    if (dmin > pre[c]) dmin = pre[c];
+  for (int c = 0; c < 4; c++) scale_mul[c] = (dmin > 0.00001 && maximum > 0) ? (float)(pre[c] / dmin) : 1.0f;
+}
+
+/*
+ * core/libraw_wrapper.cpp:632-661 (scale_colors, auto-WB branch, p = 1):
+ * per-CFA-channel means of the uint16[4] samples, G2 folded into G,
+ * pre_mul = (G/R, 1, G/B, 1).  Double accumulation as in the reference.
+ */
+void port_auto_wb(const uint16_t* raw4, size_t w, size_t h, uint32_t filters, const char xtrans[36],
+                  float pre_mul[4]) {
+  double norm[4] = {0, 0, 0, 0}, count[4] = {0, 0, 0, 0};
+  for (size_t row = 0; row < h; row++)
+    for (size_t col = 0; col < w; col++) {
+      unsigned c = filters == 9 ? port_fcol_xtrans((unsigned)row, (unsigned)col, xtrans)
+                                : port_fcol_bayer_native((unsigned)row, (unsigned)col, filters);
+      norm[c] += pow((double)raw4[(row * w + col) * 4 + c], 1.0);
+      count[c] += 1;
+    }
+  norm[1] += norm[3];
+  count[1] += count[3];
+  for (int c = 0; c < 3; c++) norm[c] = pow(norm[c] / count[c], 1.0);
+  pre_mul[0] = (float)(norm[1] / norm[0]);
+  pre_mul[1] = 1.0f;
+  pre_mul[2] = (float)(norm[1] / norm[2]);
+  pre_mul[3] = 1.0f;
+}
+
+/*
+ * core/cpu_accelerator.cpp:2984-3028 (border_interpolate): for pixels within
+ * `border` of the frame, each non-native channel becomes the mean of that
+ * colour's samples in the clipped 3x3 neighbourhood (G2 folded into G).
+ */
+void port_border_interpolate(float* rgb, size_t w, size_t h, uint32_t filters, size_t border) {
+  for (size_t row = 0; row < h; row++)
+    for (size_t col = 0; col < w; col++) {
+      if (col >= border && col < w - border && row >= border && row < h - border) continue;
+      float sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (size_t y = row > 0 ? row - 1 : 0; y < row + 2 && y < h; y++)
+        for (size_t x = col > 0 ? col - 1 : 0; x < col + 2 && x < w; x++) {
+          unsigned f = port_fcol_bayer((unsigned)y, (unsigned)x, filters);
+          sum[f] += rgb[(y * w + x) * 3 + f];
+          sum[f + 4]++;
+        }
+      unsigned f = port_fcol_bayer((unsigned)row, (unsigned)col, filters);
+      for (unsigned c = 0; c < 3; c++)
+        if (c != f && sum[c + 4] > 0) rgb[(row * w + col) * 3 + c] = sum[c] / sum[c + 4];
+    }
+}
