@@ -326,7 +326,8 @@ def develop_params(**kw) -> DevelopParams:
         elif np.ndim(cfa) == 2:
             p.filters = FILTERS_XTRANS
             x = np.asarray(cfa, dtype=np.int8).reshape(36)
-            C.memmove(p.xtrans, x.ctypes.data, 36)
+            # write through the struct's own storage (reading p.xtrans yields a copy)
+            C.memmove(C.addressof(p) + DevelopParams.xtrans.offset, x.ctypes.data, 36)
         else:
             p.filters = int(cfa)
     if "cam_mul" in kw:

@@ -40,3 +40,60 @@ def frame_mask(h, w, band):
     m = np.zeros((h, w), bool)
     m[band : h - band, band : w - band] = True
     return m
+
+
+def amaze_stale_mask(h, w):
+    """Pixels whose reference AMaZE value depends on per-thread scratch.
+
+    The reference never fills the 16x16 apron corners of the tiles that touch
+    two image edges (core/cpu_accelerator.cpp:1326), so those cells hold what
+    the OpenMP thread's previous tile left there.  Their influence reaches (a)
+    the outputs next to each image corner and (b), through pmwt being stored
+    half-indexed over dirwts1 (:1507) and dirwts1 being read full-indexed in
+    stage 9 (:1556), a band of tile rows near rrmax/2 in the two bottom corner
+    tiles.  Returns True on those pixels; parity there is reported, not
+    asserted, because the reference itself varies with the thread split.
+    """
+    TS = 160
+    m = np.zeros((h, w), bool)
+    for top in range(-16, h, TS - 32):
+        for left in range(-16, w, TS - 32):
+            bottom, right = min(top + TS, h + 16), min(left + TS, w + 16)
+            rr1, cc1 = bottom - top, right - left
+            rows, cols = [], []
+            if top < 0:
+                rows.append((0, 16))
+            if bottom > h:
+                rrmax = h - top
+                rows.append((rrmax, min(rrmax + 16, rr1)))
+            if left < 0:
+                cols.append((0, 16))
+            if right > w:
+                ccmax = w - left
+                cols.append((ccmax, min(ccmax + 16, cc1)))
+            for r0, r1 in rows:
+                for c0, c1 in cols:
+                    # outputs next to the unfilled corner cells
+                    y0, y1 = max(0, top + r0 - 20), min(h, top + r1 + 20)
+                    x0, x1 = max(0, left + c0 - 20), min(w, left + c1 + 20)
+                    m[y0:y1, x0:x1] = True
+                    if r0 == 0:
+                        continue  # top corners never reach stage 9's dirwts1 rows
+                    # pmwt rows r0-2 .. min(r1, rr1-8)+2 land on dirwts1 rows /2
+                    a0 = max(0, (r0 - 3) // 2 - 6)
+                    a1 = (min(r1, rr1 - 8) + 2) // 2 + 6
+                    p0, p1 = max(0, c0 // 2 - 3), (c1 + 1) // 2 + 3
+                    for base in (0, TS // 2):
+                        xx0, xx1 = max(0, left + base + p0 - 6), min(w, left + base + p1 + 6)
+                        m[max(0, top + a0) : min(h, top + a1), xx0:xx1] = True
+    return m
+
+
+def dilate(mask, r):
+    """Binary dilation by a (2r+1)^2 square (numpy only)."""
+    out = mask.copy()
+    h, w = mask.shape
+    ys, xs = np.nonzero(mask)
+    for y, x in zip(ys, xs):
+        out[max(0, y - r) : y + r + 1, max(0, x - r) : x + r + 1] = True
+    return out
