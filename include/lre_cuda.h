@@ -181,6 +181,28 @@ lre_status lre_dev_defringe(lre_ctx* ctx, const float* in, float* out, size_t wi
                             float strength, int defringe_green, float green_strength_scale);
 lre_status lre_dev_quantize_u16(lre_ctx* ctx, const float* in, uint16_t* out, size_t n);
 
+/* Axial CA guided filter that allocates nothing.  This entry point has no
+ * counterpart in the reference.  It serves callers that cannot allocate device
+ * memory while they process a frame: a plug-in host that only lends
+ * pre-reserved pools, a capture thread that must not block in cudaMalloc
+ * (which synchronises the device), an application whose memory budget is
+ * already committed.  It needs no lre_ctx.
+ *
+ * Arguments and arithmetic are those of lre_dev_ca_axial_cleanup (device
+ * pointers; `in == out` allowed), enqueued on `cuda_stream` (NULL = legacy
+ * default stream).  Its scratch (the max-G normaliser and, for in-place calls,
+ * a copy of the input) is one file-scope device array sized for images of at
+ * most 2,097,152 pixels (1920x1080 fits); larger images, radius > 16 or null
+ * pointers return LRE_ERR_INVALID_ARGUMENT before any work.  Every GPU that
+ * loads the library keeps the array (about 24 MiB) until the process exits.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the one array: the
+ * scratch is re-initialised by every call, but calls that overlap on the GPU
+ * (different streams, or several host threads) race on it, so serialise them. */
+lre_status lre_dev_ca_axial_cleanup_noalloc(const float* in, float* out, size_t width, size_t height,
+                                            int radius, float epsilon, float strength,
+                                            void* cuda_stream);
+
 /* ------------------------------------------------ develop pipeline */
 /* Stage switches and parameters of one develop request.  Field names and
  * defaults follow ProcessingParams (core/accelerator.h:83-177); `cfa` is a

@@ -113,6 +113,7 @@ SIGNATURES = {
     "lre_dev_ca_axial_cleanup": (_st, [_p, _p, _p, _sz, _sz, _i, _f, _f]),
     "lre_dev_defringe": (_st, [_p, _p, _p, _sz, _sz, _f, _f, _f, _f, _i, _f]),
     "lre_dev_quantize_u16": (_st, [_p, _p, _p, _sz]),
+    "lre_dev_ca_axial_cleanup_noalloc": (_st, [_p, _p, _sz, _sz, _i, _f, _f, _p]),
     "lre_develop_params_default": (None, [C.POINTER(DevelopParams)]),
     "lre_develop": (_st, [_p, _p, _p, _sz, _sz, C.POINTER(DevelopParams)]),
     "lre_dev_develop": (_st, [_p, _p, _p, _sz, _sz, C.POINTER(DevelopParams)]),

@@ -21,6 +21,8 @@
 // shared memory, so HBM sees 12 B/px in + 12 B/px out (the algorithmic
 // minimum) plus halo re-reads that hit L2.  The only other pass is the global
 // max(G) reduction that the normalisation needs before any tile can start.
+#include <mutex>
+
 #include "common.cuh"
 #include "lre_internal.h"
 
@@ -342,4 +344,92 @@ lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, si
   return check_launch(c, "ca_axial_cleanup");
 }
 
+// ---------------------------------------------------------------------------
+// Axial CA without any device allocation.
+//
+// Some callers cannot allocate device memory when they filter a frame: a
+// plug-in host that hands out only pre-reserved memory pools, a real-time
+// capture thread that must not block on cudaMalloc (it synchronises the
+// device), or an application that has already pinned its memory budget.
+// This variant keeps its scratch -- the max(G) normaliser and, for in-place
+// calls, a copy of the input -- in one file-scope device array, so a call
+// allocates nothing.  The array is sized for images up to
+// kNoAllocMaxPixels; larger images are rejected.  Every GPU that loads the
+// library holds the array until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocMaxPixels = size_t(1) << 21;  // 2,097,152 px, e.g. 1920x1080
+constexpr size_t kNoAllocHead = 64;                     // floats ahead of the image copy (256 B)
+static __device__ __align__(256) float g_axial_noalloc_scratch[kNoAllocHead + kNoAllocMaxPixels * 3];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+float* g_noalloc_addr[kNoAllocMaxDevices] = {nullptr};
+
+__global__ void k_noalloc_zero(float* p) { *p = 0.0f; }
+
+// max(0, max G) over the image, into *out (which must start at 0).
+__global__ void k_noalloc_max_g(const float* __restrict__ rgb, size_t n, float* out) {
+  float m = 0.0f;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    m = fmaxf(m, rgb[i * 3 + 1]);
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) atomic_max_float(out, m);
+}
+
+}  // namespace
+
 }  // namespace lre
+
+extern "C" lre_status lre_dev_ca_axial_cleanup_noalloc(const float* in, float* out, size_t w, size_t h, int radius,
+                                                       float epsilon, float strength, void* cuda_stream) {
+  using namespace lre;
+  if (!in || !out || w == 0 || h == 0) return LRE_ERR_INVALID_ARGUMENT;
+  if (w > (1u << 20) || h > (1u << 20) || w * h > kNoAllocMaxPixels) return LRE_ERR_INVALID_ARGUMENT;
+  if (radius < 1) radius = 1;
+  if (radius > 16) return LRE_ERR_INVALID_ARGUMENT;
+  strength = fminf(fmaxf(strength, 0.f), 1.f);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+
+  // One-time set-up per device: the device address of the scratch array.
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return LRE_ERR_CUDA;
+  float* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_axial_noalloc_scratch) != cudaSuccess || !p) {
+        cudaGetLastError();
+        return LRE_ERR_CUDA;
+      }
+      g_noalloc_addr[dev] = static_cast<float*>(p);
+    }
+    base = g_noalloc_addr[dev];
+  }
+  float* d_max = base;                 // cleared below on every call
+  float* staging = base + kNoAllocHead;
+
+  const size_t n = w * h;
+  k_noalloc_zero<<<1, 1, 0, s>>>(d_max);
+  k_noalloc_max_g<<<grid_for(n, 256, 148u * 4u), 256, 0, s>>>(in, n, d_max);
+  const float* src = in;
+  if (in == out) {
+    if (cudaMemcpyAsync(staging, in, n * 3 * sizeof(float), cudaMemcpyDeviceToDevice, s) != cudaSuccess) return LRE_ERR_CUDA;
+    src = staging;
+  }
+  const int T = pick_tile(radius);
+  const AxGeom g = ax_geom(T, radius);
+  dim3 grid((unsigned)((w + T - 1) / T), (unsigned)((h + T - 1) / T));
+  if (T == 32) {
+    if (cudaFuncSetAttribute(k_axial_fused<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.bytes) != cudaSuccess)
+      return LRE_ERR_CUDA;
+    k_axial_fused<32><<<grid, AX_THREADS, g.bytes, s>>>(src, out, (int)w, (int)h, radius, epsilon, strength, d_max);
+  } else {
+    if (cudaFuncSetAttribute(k_axial_fused<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.bytes) != cudaSuccess)
+      return LRE_ERR_CUDA;
+    k_axial_fused<16><<<grid, AX_THREADS, g.bytes, s>>>(src, out, (int)w, (int)h, radius, epsilon, strength, d_max);
+  }
+  return cudaGetLastError() == cudaSuccess ? LRE_OK : LRE_ERR_CUDA;
+}
