@@ -14,13 +14,23 @@
 //   * pmwt is stored half-indexed in dirwts1's memory (:1507), and stage 9
 //     later reads dirwts1 full-indexed (:1556), so part of what it reads is
 //     pmwt -- that aliasing is reproduced explicitly below (dirwts1_eff).
-// This kernel therefore runs the reference's tiles one CTA per tile, stage by
-// stage, with the sequential chains on individual threads and the
-// Gauss-Seidel sweeps as row-synchronous wavefronts.  Per-tile planes live in
-// a per-CTA global scratch slab (they do not fit in shared memory: ~20 planes
-// of 160x160).  Scratch positions the reference reads without writing in the
-// same tile hold zeros (a fresh, zero-initialised buffer), and the unfilled
-// 16x16 apron corners at the image corners are zero as well.
+//
+// Device design: a persistent CTA per SM pulls the reference's tiles from a
+// counter and runs each one stage by stage.
+//   * Scratch: one slab per CTA of 7 full planes (160x160 floats) plus one
+//     half plane; the reference's ~20 planes are mapped onto it by lifetime
+//     (a plane is reused once its last reader has run), the cheap gradient
+//     planes (dirwts0/1, delhvsqsum) are recomputed from cfa where read, and
+//     R/B-only quantities are stored half-indexed.  148 slabs (~117 MB) sit
+//     in L2.
+//   * hvwt and pmwt live in shared memory (2 x 51 KB), so both Gauss-Seidel
+//     sweeps chase their row-to-row dependency through SMEM; the work that
+//     only needs a site's final weight runs in a parallel pass afterwards.
+//   * Stage-3 chains run one chain per thread with the next step's operands
+//     loaded ahead of the dependent arithmetic.
+// Positions the reference reads without writing in the same tile read zeros
+// (a freshly allocated buffer): the 4-px frame of vcd/hcd/vcdalt/hcdalt, the
+// nyquist maps, Dgrb1, and the unfilled apron corners of corner tiles.
 #include "common.cuh"
 #include "lre_internal.h"
 
@@ -31,6 +41,7 @@ namespace {
 constexpr int TS = 160;
 constexpr int TSH = TS / 2;
 constexpr int TS2 = TS * TS;
+constexpr int HALF = TS * TSH;
 constexpr int AMZ_THREADS = 512;
 
 constexpr float eps = 1e-5f;
@@ -42,29 +53,51 @@ __device__ __forceinline__ float SQR(float x) { return x * x; }
 __device__ __forceinline__ float xmul2f(float x) { return x + x; }
 __device__ __forceinline__ float xdiv2f(float x) { return x * 0.5f; }
 
-// Scratch slab layout (floats unless noted).
+constexpr size_t kFull = 7;
+constexpr size_t kSlabBytes = kFull * TS2 * 4 + 2 * HALF + 256;  // + nyquist, nyquist2 bytes
+constexpr size_t kSmemBytes = 2 * HALF * 4;                       // hvwt + pmwt
+
+// Lifetime map of the reference's planes onto the slab (F0..F6 full planes;
+// "a"/"b" = first/second half of a full plane):
+//   F0 cfa                                   fill .. S10
+//   F1 vcd  (S2..S6)     -> a rbm, b rbp     (S8..S9)
+//   F2 hcd  (S2..S6)     -> a pmwt copy-out unused, b rbint (S9)
+//   F3 vcdalt (S2..S3)   -> a cddiffsq (S3..S5) then Dgrb0 (S6..S10), b rgbgreen@R/B (S6..S10)
+//   F4 hcdalt (S2..S3)   -> a Dgrb2h, b Dgrb2v (S6) -> a Dgrb1 (S9..S10)
+//   F5 dgintv (S2..S5)   -> a delp, b delm (S7..S8)
+//   F6 dginth (S2..S5)   -> a Dgrbsq1p, b Dgrbsq1m (S7..S8)
+//   SMEM: hvwt (S4..S10), pmwt (S8..S9)
 struct Slab {
-  float *cfa, *rgbgreen, *delhvsqsum, *dirwts0, *dirwts1, *vcd, *hcd, *vcdalt, *hcdalt, *cddiffsq, *dgintv, *dginth;
-  float *hvwt, *nyqutest, *Dgrb0, *Dgrb1, *Dgrb2h, *Dgrb2v, *delp, *delm, *Dgrbsq1p, *Dgrbsq1m, *rbm, *rbp, *pmwt, *rbint;
+  float *cfa, *vcd, *hcd, *vcdalt, *hcdalt, *dgintv, *dginth;
+  float *rbm, *rbp, *rbint, *cddiffsq, *Dgrb0, *rgbg, *Dgrb2h, *Dgrb2v, *Dgrb1, *delp, *delm, *Dq1p, *Dq1m;
   unsigned char *nyquist, *nyquist2;
 };
-constexpr size_t kFullPlanes = 12;
-constexpr size_t kHalfPlanes = 14;
-constexpr size_t kSlabBytes = (kFullPlanes * TS2 + kHalfPlanes * TS * TSH) * 4 + 2 * TS * TSH + 256;
 
 __device__ Slab make_slab(unsigned char* base) {
   Slab s;
-  float* f = reinterpret_cast<float*>(base);
-  float** full[kFullPlanes] = {&s.cfa, &s.rgbgreen, &s.delhvsqsum, &s.dirwts0, &s.dirwts1, &s.vcd,
-                               &s.hcd, &s.vcdalt,   &s.hcdalt,     &s.cddiffsq, &s.dgintv, &s.dginth};
-  for (size_t i = 0; i < kFullPlanes; i++) *full[i] = f + i * TS2;
-  f += kFullPlanes * TS2;
-  float** half[kHalfPlanes] = {&s.hvwt, &s.nyqutest, &s.Dgrb0,    &s.Dgrb1,    &s.Dgrb2h, &s.Dgrb2v, &s.delp,
-                               &s.delm, &s.Dgrbsq1p, &s.Dgrbsq1m, &s.rbm,      &s.rbp,    &s.pmwt,   &s.rbint};
-  for (size_t i = 0; i < kHalfPlanes; i++) *half[i] = f + i * TS * TSH;
-  f += kHalfPlanes * TS * TSH;
-  s.nyquist = reinterpret_cast<unsigned char*>(f);
-  s.nyquist2 = s.nyquist + TS * TSH;
+  float* F = reinterpret_cast<float*>(base);
+  s.cfa = F;
+  s.vcd = F + 1 * TS2;
+  s.hcd = F + 2 * TS2;
+  s.vcdalt = F + 3 * TS2;
+  s.hcdalt = F + 4 * TS2;
+  s.dgintv = F + 5 * TS2;
+  s.dginth = F + 6 * TS2;
+  s.rbm = s.vcd;
+  s.rbp = s.vcd + HALF;
+  s.rbint = s.hcd + HALF;
+  s.cddiffsq = s.vcdalt;
+  s.Dgrb0 = s.vcdalt;
+  s.rgbg = s.vcdalt + HALF;
+  s.Dgrb2h = s.hcdalt;
+  s.Dgrb2v = s.hcdalt + HALF;
+  s.Dgrb1 = s.hcdalt;
+  s.delp = s.dgintv;
+  s.delm = s.dgintv + HALF;
+  s.Dq1p = s.dginth;
+  s.Dq1m = s.dginth + HALF;
+  s.nyquist = reinterpret_cast<unsigned char*>(F + kFull * TS2);
+  s.nyquist2 = s.nyquist + HALF;
   return s;
 }
 
@@ -90,6 +123,57 @@ __device__ __forceinline__ float raw_at(const AmazeArgs& a, int row, int col) {
   return a.raw[i * 3 + fc_rt(a, row, col)];
 }
 
+// The reference's stage-1 planes (:1330-1339), recomputed from cfa.
+__device__ __forceinline__ float dirwts0_at(const float* cfa, int idx) {
+  const float delv = fabsf(cfa[idx + TS] - cfa[idx - TS]);
+  return eps + fabsf(cfa[idx + 2 * TS] - cfa[idx]) + fabsf(cfa[idx] - cfa[idx - 2 * TS]) + delv;
+}
+__device__ __forceinline__ float dirwts1_at(const float* cfa, int idx) {
+  const float delh = fabsf(cfa[idx + 1] - cfa[idx - 1]);
+  return eps + fabsf(cfa[idx + 2] - cfa[idx]) + fabsf(cfa[idx] - cfa[idx - 2]) + delh;
+}
+__device__ __forceinline__ float delhvsqsum_at(const float* cfa, int idx) {
+  const float delh = fabsf(cfa[idx + 1] - cfa[idx - 1]);
+  const float delv = fabsf(cfa[idx + TS] - cfa[idx - TS]);
+  return SQR(delh) + SQR(delv);
+}
+
+// One step of the stage-3 hcd (or, transposed, vcd) chain: `prev` is the
+// already-updated value two sites back, `cur`/`next` the stage-2 values,
+// `*alt` the alternates, `c`, `cm`, `cp` the cfa at the site and its two
+// neighbours along the chain direction.  Returns the updated value.
+__device__ __forceinline__ float s3_step(float prev, float cur, float next, float altp, float altc, float altn,
+                                         float c, float cm, float cp, bool green, float clip_pt) {
+  const float var = 3.f * (SQR(prev) + SQR(cur) + SQR(next)) - SQR(prev + cur + next);
+  const float altvar = 3.f * (SQR(altp) + SQR(altc) + SQR(altn)) - SQR(altp + altc + altn);
+  float h = cur;
+  if (altvar < var) h = altc;
+  float Gint;
+  if (green) {
+    Gint = -h + c;
+    if (h > 0) {
+      if (3.f * h > (Gint + c)) {
+        h = -median3(Gint, cm, cp) + c;
+      } else {
+        const float wt2 = 1.f - 3.f * h / (eps + Gint + c);
+        h = wt2 * h + (1.f - wt2) * (-median3(Gint, cm, cp) + c);
+      }
+    }
+  } else {
+    Gint = h + c;
+    if (h < 0) {
+      if (3.f * h < -(Gint + c)) {
+        h = median3(Gint, cm, cp) - c;
+      } else {
+        const float wt2 = 1.f + 3.f * h / (eps + Gint + c);
+        h = wt2 * h + (1.f - wt2) * (median3(Gint, cm, cp) - c);
+      }
+    }
+  }
+  if (Gint > clip_pt) h = (float)(green ? -1 : 1) * (median3(Gint, cm, cp) - c);
+  return h;
+}
+
 __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
   const int v1 = TS, v2 = 2 * TS, v3 = 3 * TS, p1 = -TS + 1, p2 = -2 * TS + 2, p3 = -3 * TS + 3, m1 = TS + 1,
             m2 = 2 * TS + 2, m3 = 3 * TS + 3;
@@ -99,9 +183,13 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
                               nyqthresh * 0.03099732204057846f, nyqthresh * 0.018413194161458882f};
   const float gausseven[2] = {0.13719494435797422f, 0.05640252782101291f};
   const float gquinc[4] = {0.169917f, 0.108947f, 0.069855f, 0.0287182f};
+  extern __shared__ __align__(16) float smem[];
+  float* hvwt = smem;         // [HALF]
+  float* pmwt = smem + HALF;  // [HALF]
   const int tid = threadIdx.x, nth = blockDim.x;
   const int W = A.W, H = A.H;
-  Slab S = make_slab(A.scratch + (size_t)blockIdx.x * kSlabBytes);
+  const Slab S = make_slab(A.scratch + (size_t)blockIdx.x * kSlabBytes);
+  float* cfa = S.cfa;
   __shared__ int s_tile;
   __shared__ int s_doNyq;
 
@@ -109,7 +197,6 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     if (tid == 0) s_tile = atomicAdd(A.tile_counter, 1);
     __syncthreads();
     const int tile = s_tile;
-    __syncthreads();
     if (tile >= A.n_top * A.n_left) break;
     const int top = -16 + (tile / A.n_left) * (TS - 32);
     const int left = -16 + (tile % A.n_left) * (TS - 32);
@@ -122,16 +209,32 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     const int rrmax = (bottom > H) ? H - top : rr1;
     const int ccmax = (right > W) ? W - left : cc1;
 
-    // ---- fresh scratch: zero every plane (reads outside a stage's written
-    // range see zeros, as in a newly allocated reference buffer).
-    {
-      float4* z = reinterpret_cast<float4*>(S.cfa);
-      const size_t n4 = (kSlabBytes - 256) / 16;
-      for (size_t i = tid; i < n4; i += nth) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    // ---- zero what this tile reads before writing (fresh-buffer semantics)
+    for (int i = tid; i < 2 * HALF / 16; i += nth)
+      reinterpret_cast<float4*>(S.nyquist)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = tid; i < rr1 * cc1; i += nth) {
+      const int rr = i / cc1, cc = i % cc1;
+      if (rr >= 4 && rr < rr1 - 4 && cc >= 4 && cc < cc1 - 4) continue;
+      const int idx = rr * TS + cc;
+      S.vcd[idx] = 0.f;
+      S.hcd[idx] = 0.f;
+      S.vcdalt[idx] = 0.f;
+      S.hcdalt[idx] = 0.f;
+    }
+    if ((rrmin > 0 || rrmax < rr1) && (ccmin > 0 || ccmax < cc1)) {
+      // unfilled 16x16 apron corners (:1326)
+      for (int i = tid; i < rr1 * cc1; i += nth) {
+        const int rr = i / cc1, cc = i % cc1;
+        const bool rc = (rrmin > 0 && rr < 16) || (rrmax < rr1 && rr >= rrmax);
+        const bool cc_ = (ccmin > 0 && cc < 16) || (ccmax < cc1 && cc >= ccmax);
+        if (rc && cc_) cfa[rr * TS + cc] = 0.f;
+      }
     }
     __syncthreads();
 
-    // ---- fill (:1254-1326)
+    // ---- fill (:1254-1326); the right apron is written last, wrapping into
+    // the next row when ccmax + 16 exceeds the tile width, as the reference's
+    // flat buffer does
     const float scale = A.scale;
     for (int i = tid; i < rr1 * cc1; i += nth) {
       const int rr = i / cc1, cc = i % cc1;
@@ -152,42 +255,31 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
         srow = min(max(top + rr, 0), H - 1);
         scol = min(max(W - (cc - ccmax) - 2, 0), W - 1);
       }
-      if (srow >= 0) {
-        const float val = raw_at(A, srow, scol) * scale;
-        S.cfa[rr * TS + cc] = val;
-        S.rgbgreen[rr * TS + cc] = val;
+      if (srow >= 0) cfa[rr * TS + cc] = raw_at(A, srow, scol) * scale;
+    }
+    if (ccmax < cc1 && ccmax + 16 > TS) {
+      __syncthreads();
+      for (int i = tid; i < (rrmax - rrmin) * 16; i += nth) {
+        const int rr = rrmin + i / 16, k = i % 16;
+        if (ccmax + k < TS || rr + 1 >= TS) continue;
+        const int srow = min(max(top + rr, 0), H - 1);
+        const int scol = min(max(W - k - 2, 0), W - 1);
+        cfa[(rr + 1) * TS + (ccmax + k - TS)] = raw_at(A, srow, scol) * scale;
       }
     }
     __syncthreads();
 
-    float* cfa = S.cfa;
-    float* dirwts0 = S.dirwts0;
-    float* dirwts1 = S.dirwts1;
-    // ---- S1 gradients (:1330-1339)
-    for (int i = tid; i < (rr1 - 4) * (cc1 - 4); i += nth) {
-      const int rr = 2 + i / (cc1 - 4), cc = 2 + i % (cc1 - 4);
-      const int idx = rr * TS + cc;
-      const float delh = fabsf(cfa[idx + 1] - cfa[idx - 1]);
-      const float delv = fabsf(cfa[idx + v1] - cfa[idx - v1]);
-      dirwts0[idx] = eps + fabsf(cfa[idx + v2] - cfa[idx]) + fabsf(cfa[idx] - cfa[idx - v2]) + delv;
-      dirwts1[idx] = eps + fabsf(cfa[idx + 2] - cfa[idx]) + fabsf(cfa[idx] - cfa[idx - 2]) + delh;
-      S.delhvsqsum[idx] = SQR(delh) + SQR(delv);
-    }
-    __syncthreads();
-
-    // ---- S2 colour differences (:1341-1373)
+    // ---- S2 colour differences (:1341-1373); S1 planes recomputed
     for (int i = tid; i < (rr1 - 8) * (cc1 - 8); i += nth) {
       const int rr = 4 + i / (cc1 - 8), cc = 4 + i % (cc1 - 8);
       const int idx = rr * TS + cc;
       const int sgn = (fc_rt(A, rr, cc) & 1) ? -1 : 1;
-      const float cru = cfa[idx - v1] * (dirwts0[idx - v2] + dirwts0[idx]) /
-                        (dirwts0[idx - v2] * (eps + cfa[idx]) + dirwts0[idx] * (eps + cfa[idx - v2]));
-      const float crd = cfa[idx + v1] * (dirwts0[idx + v2] + dirwts0[idx]) /
-                        (dirwts0[idx + v2] * (eps + cfa[idx]) + dirwts0[idx] * (eps + cfa[idx + v2]));
-      const float crl = cfa[idx - 1] * (dirwts1[idx - 2] + dirwts1[idx]) /
-                        (dirwts1[idx - 2] * (eps + cfa[idx]) + dirwts1[idx] * (eps + cfa[idx - 2]));
-      const float crr = cfa[idx + 1] * (dirwts1[idx + 2] + dirwts1[idx]) /
-                        (dirwts1[idx + 2] * (eps + cfa[idx]) + dirwts1[idx] * (eps + cfa[idx + 2]));
+      const float d0m2 = dirwts0_at(cfa, idx - v2), d00 = dirwts0_at(cfa, idx), d0p2 = dirwts0_at(cfa, idx + v2);
+      const float d1m2 = dirwts1_at(cfa, idx - 2), d10 = dirwts1_at(cfa, idx), d1p2 = dirwts1_at(cfa, idx + 2);
+      const float cru = cfa[idx - v1] * (d0m2 + d00) / (d0m2 * (eps + cfa[idx]) + d00 * (eps + cfa[idx - v2]));
+      const float crd = cfa[idx + v1] * (d0p2 + d00) / (d0p2 * (eps + cfa[idx]) + d00 * (eps + cfa[idx + v2]));
+      const float crl = cfa[idx - 1] * (d1m2 + d10) / (d1m2 * (eps + cfa[idx]) + d10 * (eps + cfa[idx - 2]));
+      const float crr = cfa[idx + 1] * (d1p2 + d10) / (d1p2 * (eps + cfa[idx]) + d10 * (eps + cfa[idx + 2]));
       const float guha = cfa[idx - v1] + xdiv2f(cfa[idx] - cfa[idx - v2]);
       const float gdha = cfa[idx + v1] + xdiv2f(cfa[idx] - cfa[idx + v2]);
       const float glha = cfa[idx - 1] + xdiv2f(cfa[idx] - cfa[idx - 2]);
@@ -196,16 +288,20 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
       float gdar = fabsf(1.f - crd) < arthresh ? cfa[idx] * crd : gdha;
       float glar = fabsf(1.f - crl) < arthresh ? cfa[idx] * crl : glha;
       float grar = fabsf(1.f - crr) < arthresh ? cfa[idx] * crr : grha;
-      const float hwt = dirwts1[idx - 1] / (dirwts1[idx - 1] + dirwts1[idx + 1]);
-      const float vwt = dirwts0[idx - v1] / (dirwts0[idx + v1] + dirwts0[idx - v1]);
+      const float d1m1 = dirwts1_at(cfa, idx - 1), d1p1 = dirwts1_at(cfa, idx + 1);
+      const float d0m1 = dirwts0_at(cfa, idx - v1), d0p1 = dirwts0_at(cfa, idx + v1);
+      const float hwt = d1m1 / (d1m1 + d1p1);
+      const float vwt = d0m1 / (d0p1 + d0m1);
       const float Gintvha = vwt * gdha + (1.f - vwt) * guha;
       const float Ginthha = hwt * grha + (1.f - hwt) * glha;
       const float fs = (float)sgn;
-      S.vcdalt[idx] = fs * (Gintvha - cfa[idx]);
-      S.hcdalt[idx] = fs * (Ginthha - cfa[idx]);
+      const float va = fs * (Gintvha - cfa[idx]);
+      const float ha = fs * (Ginthha - cfa[idx]);
+      S.vcdalt[idx] = va;
+      S.hcdalt[idx] = ha;
       if (cfa[idx] > A.clip_pt8 || Gintvha > A.clip_pt8 || Ginthha > A.clip_pt8) {
-        S.vcd[idx] = S.vcdalt[idx];
-        S.hcd[idx] = S.hcdalt[idx];
+        S.vcd[idx] = va;
+        S.hcd[idx] = ha;
         guar = guha;
         gdar = gdha;
         glar = glha;
@@ -219,105 +315,60 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     }
     __syncthreads();
 
-    // ---- S3 variance + bounding (:1375-1398): hcd chains along rows,
-    // vcd chains along columns (stride 2, in place, as the reference scans).
+    // ---- S3 (:1375-1398): hcd chains along rows, vcd chains down columns,
+    // each in the reference's scan order; operands of the next step are
+    // loaded before the dependent arithmetic of the current one
     {
-      const int nrows = rr1 - 8, ncols = cc1 - 8;
-      const int n_h = nrows * 2, n_v = ncols * 2;
+      const int n_h = (rr1 - 8) * 2, n_v = (cc1 - 8) * 2;
       for (int item = tid; item < n_h + n_v; item += nth) {
-        if (item < n_h) {
-          const int rr = 4 + item / 2, par = item % 2;
-          float* hcd = S.hcd;
-          const float* hcdalt = S.hcdalt;
-          for (int cc = 4 + par; cc < cc1 - 4; cc += 2) {
-            const int idx = rr * TS + cc;
-            const float hcdvar = 3.f * (SQR(hcd[idx - 2]) + SQR(hcd[idx]) + SQR(hcd[idx + 2])) -
-                                 SQR(hcd[idx - 2] + hcd[idx] + hcd[idx + 2]);
-            const float hcdaltvar = 3.f * (SQR(hcdalt[idx - 2]) + SQR(hcdalt[idx]) + SQR(hcdalt[idx + 2])) -
-                                    SQR(hcdalt[idx - 2] + hcdalt[idx] + hcdalt[idx + 2]);
-            float h = hcd[idx];
-            if (hcdaltvar < hcdvar) h = hcdalt[idx];
-            float Ginth;
-            if (fc_rt(A, rr, cc) & 1) {
-              Ginth = -h + cfa[idx];
-              if (h > 0) {
-                if (3.f * h > (Ginth + cfa[idx])) {
-                  h = -median3(Ginth, cfa[idx - 1], cfa[idx + 1]) + cfa[idx];
-                } else {
-                  const float hwt2 = 1.f - 3.f * h / (eps + Ginth + cfa[idx]);
-                  h = hwt2 * h + (1.f - hwt2) * (-median3(Ginth, cfa[idx - 1], cfa[idx + 1]) + cfa[idx]);
-                }
-              }
-            } else {
-              Ginth = h + cfa[idx];
-              if (h < 0) {
-                if (3.f * h < -(Ginth + cfa[idx])) {
-                  h = median3(Ginth, cfa[idx - 1], cfa[idx + 1]) - cfa[idx];
-                } else {
-                  const float hwt2 = 1.f + 3.f * h / (eps + Ginth + cfa[idx]);
-                  h = hwt2 * h + (1.f - hwt2) * (median3(Ginth, cfa[idx - 1], cfa[idx + 1]) - cfa[idx]);
-                }
-              }
-            }
-            if (Ginth > A.clip_pt)
-              h = (float)((fc_rt(A, rr, cc) & 1) ? -1 : 1) * (median3(Ginth, cfa[idx - 1], cfa[idx + 1]) - cfa[idx]);
-            hcd[idx] = h;
-          }
-        } else {
-          const int it = item - n_h;
-          const int cc = 4 + it / 2, par = it % 2;
-          float* vcd = S.vcd;
-          const float* vcdalt = S.vcdalt;
-          for (int rr = 4 + par; rr < rr1 - 4; rr += 2) {
-            const int idx = rr * TS + cc;
-            const float vcdvar = 3.f * (SQR(vcd[idx - v2]) + SQR(vcd[idx]) + SQR(vcd[idx + v2])) -
-                                 SQR(vcd[idx - v2] + vcd[idx] + vcd[idx + v2]);
-            const float vcdaltvar = 3.f * (SQR(vcdalt[idx - v2]) + SQR(vcdalt[idx]) + SQR(vcdalt[idx + v2])) -
-                                    SQR(vcdalt[idx - v2] + vcdalt[idx] + vcdalt[idx + v2]);
-            float v = vcd[idx];
-            if (vcdaltvar < vcdvar) v = vcdalt[idx];
-            float Gintv;
-            if (fc_rt(A, rr, cc) & 1) {
-              Gintv = -v + cfa[idx];
-              if (v > 0) {
-                if (3.f * v > (Gintv + cfa[idx])) {
-                  v = -median3(Gintv, cfa[idx - v1], cfa[idx + v1]) + cfa[idx];
-                } else {
-                  const float vwt2 = 1.f - 3.f * v / (eps + Gintv + cfa[idx]);
-                  v = vwt2 * v + (1.f - vwt2) * (-median3(Gintv, cfa[idx - v1], cfa[idx + v1]) + cfa[idx]);
-                }
-              }
-            } else {
-              Gintv = v + cfa[idx];
-              if (v < 0) {
-                if (3.f * v < -(Gintv + cfa[idx])) {
-                  v = median3(Gintv, cfa[idx - v1], cfa[idx + v1]) - cfa[idx];
-                } else {
-                  const float vwt2 = 1.f + 3.f * v / (eps + Gintv + cfa[idx]);
-                  v = vwt2 * v + (1.f - vwt2) * (median3(Gintv, cfa[idx - v1], cfa[idx + v1]) - cfa[idx]);
-                }
-              }
-            }
-            if (Gintv > A.clip_pt)
-              v = (float)((fc_rt(A, rr, cc) & 1) ? -1 : 1) * (median3(Gintv, cfa[idx - v1], cfa[idx + v1]) - cfa[idx]);
-            vcd[idx] = v;
-          }
+        const bool horiz = item < n_h;
+        const int it = horiz ? item : item - n_h;
+        const int line = 4 + it / 2, par = it % 2;
+        const int stride = horiz ? 2 : v2;      // chain step in the flat tile
+        const int nstride = horiz ? 1 : v1;     // neighbour along the direction
+        const int len = horiz ? cc1 : rr1;
+        float* d = horiz ? S.hcd : S.vcd;
+        const float* alt = horiz ? S.hcdalt : S.vcdalt;
+        int pos = 4 + par;
+        if (pos >= len - 4) continue;
+        int idx = horiz ? line * TS + pos : pos * TS + line;
+        float prev = d[idx - stride], cur = d[idx], altp = alt[idx - stride], altc = alt[idx];
+        float next = d[idx + stride], altn = alt[idx + stride];
+        for (; pos < len - 4; pos += 2, idx += stride) {
+          const float c = cfa[idx], cm = cfa[idx - nstride], cp = cfa[idx + nstride];
+          const int nidx = idx + 2 * stride;
+          const bool more = pos + 2 < len - 4;
+          const float next2 = more ? d[nidx] : 0.f;
+          const float altn2 = more ? alt[nidx] : 0.f;
+          const int rr = horiz ? line : pos, cc = horiz ? pos : line;
+          const float h = s3_step(prev, cur, next, altp, altc, altn, c, cm, cp, (fc_rt(A, rr, cc) & 1) != 0, A.clip_pt);
+          d[idx] = h;
+          prev = h;
+          cur = next;
+          altp = altc;
+          altc = altn;
+          next = next2;
+          altn = altn2;
         }
       }
     }
     __syncthreads();
-    for (int i = tid; i < (rr1 - 8) * (cc1 - 8); i += nth) {
-      const int rr = 4 + i / (cc1 - 8), cc = 4 + i % (cc1 - 8);
-      const int idx = rr * TS + cc;
-      S.cddiffsq[idx] = SQR(S.vcd[idx] - S.hcd[idx]);
+    // cddiffsq at R/B sites (read only there by stage 4/5), half-indexed
+    auto rb_count = [&](int a) { return (cc1 - a - a + 1) / 2 + 1; };
+    {
+      const int per_row = rb_count(4);
+      for (int i = tid; i < (rr1 - 8) * per_row; i += nth) {
+        const int rr = 4 + i / per_row;
+        const int cc = 4 + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        if (cc >= cc1 - 4) continue;
+        const int idx = rr * TS + cc;
+        S.cddiffsq[idx >> 1] = SQR(S.vcd[idx] - S.hcd[idx]);
+      }
     }
+    if (tid == 0) s_doNyq = 0;
     __syncthreads();
 
-    // R/B-site iteration helper: rows [a, rr1-a), cc = a + (fc(rr,2)&1) step 2, cc < cc1 - a.
-    auto rb_count = [&](int a) { return (cc1 - a - a + 1) / 2 + 1; };
-
     // ---- S4/5 directional variance + Nyquist test (:1400-1433)
-    if (tid == 0) s_doNyq = 0;
     {
       const int a = 6;
       const int per_row = rb_count(a);
@@ -336,8 +387,10 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
         const float Dgrbvvard = SQR(vcd[idx] - dave) + SQR(vcd[idx + v1] - dave) + SQR(vcd[idx + v2] - dave) + SQR(vcd[idx + v3] - dave);
         const float Dgrbhvarl = SQR(hcd[idx] - lave) + SQR(hcd[idx - 1] - lave) + SQR(hcd[idx - 2] - lave) + SQR(hcd[idx - 3] - lave);
         const float Dgrbhvarr = SQR(hcd[idx] - rave) + SQR(hcd[idx + 1] - rave) + SQR(hcd[idx + 2] - rave) + SQR(hcd[idx + 3] - rave);
-        const float hwt = dirwts1[idx - 1] / (dirwts1[idx - 1] + dirwts1[idx + 1]);
-        const float vwt = dirwts0[idx - v1] / (dirwts0[idx + v1] + dirwts0[idx - v1]);
+        const float d1m1 = dirwts1_at(cfa, idx - 1), d1p1 = dirwts1_at(cfa, idx + 1);
+        const float d0m1 = dirwts0_at(cfa, idx - v1), d0p1 = dirwts0_at(cfa, idx + v1);
+        const float hwt = d1m1 / (d1m1 + d1p1);
+        const float vwt = d0m1 / (d0p1 + d0m1);
         const float vcdvar = epssq + vwt * Dgrbvvard + (1.f - vwt) * Dgrbvvaru;
         const float hcdvar = epssq + hwt * Dgrbhvarr + (1.f - hwt) * Dgrbhvarl;
         const float* dgintv = S.dgintv;
@@ -350,21 +403,20 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
         const float hcdvar1 = epssq + hwt * Dgrbhvarr2 + (1.f - hwt) * Dgrbhvarl2;
         const float varwt = hcdvar / (vcdvar + hcdvar);
         const float diffwt = hcdvar1 / (vcdvar1 + hcdvar1);
-        S.hvwt[idx >> 1] =
+        hvwt[idx >> 1] =
             ((0.5f - varwt) * (0.5f - diffwt) > 0.f && fabsf(0.5f - diffwt) < fabsf(0.5f - varwt)) ? varwt : diffwt;
-        const float* cdd = S.cddiffsq;
-        const float* dhv = S.delhvsqsum;
+        const float* cdd = S.cddiffsq;  // half-indexed; every tap is an R/B site
+        auto dh = [&](int o) { return delhvsqsum_at(cfa, idx + o); };
         const float nt =
-            (gaussodd[0] * cdd[idx] + gaussodd[1] * (cdd[idx - m1] + cdd[idx + p1] + cdd[idx - p1] + cdd[idx + m1]) +
-             gaussodd[2] * (cdd[idx - v2] + cdd[idx - 2] + cdd[idx + 2] + cdd[idx + v2]) +
-             gaussodd[3] * (cdd[idx - m2] + cdd[idx + p2] + cdd[idx - p2] + cdd[idx + m2])) -
-            (gaussgrad[0] * dhv[idx] + gaussgrad[1] * (dhv[idx - v1] + dhv[idx + 1] + dhv[idx - 1] + dhv[idx + v1]) +
-             gaussgrad[2] * (dhv[idx - m1] + dhv[idx + p1] + dhv[idx - p1] + dhv[idx + m1]) +
-             gaussgrad[3] * (dhv[idx - v2] + dhv[idx - 2] + dhv[idx + 2] + dhv[idx + v2]) +
-             gaussgrad[4] * (dhv[idx - v2 - 1] + dhv[idx - v2 + 1] + dhv[idx - TS - 2] + dhv[idx - TS + 2] +
-                             dhv[idx + TS - 2] + dhv[idx + TS + 2] + dhv[idx + v2 - 1] + dhv[idx + v2 + 1]) +
-             gaussgrad[5] * (dhv[idx - m2] + dhv[idx + p2] + dhv[idx - p2] + dhv[idx + m2]));
-        S.nyqutest[idx >> 1] = nt;
+            (gaussodd[0] * cdd[idx >> 1] +
+             gaussodd[1] * (cdd[(idx - m1) >> 1] + cdd[(idx + p1) >> 1] + cdd[(idx - p1) >> 1] + cdd[(idx + m1) >> 1]) +
+             gaussodd[2] * (cdd[(idx - v2) >> 1] + cdd[(idx - 2) >> 1] + cdd[(idx + 2) >> 1] + cdd[(idx + v2) >> 1]) +
+             gaussodd[3] * (cdd[(idx - m2) >> 1] + cdd[(idx + p2) >> 1] + cdd[(idx - p2) >> 1] + cdd[(idx + m2) >> 1])) -
+            (gaussgrad[0] * dh(0) + gaussgrad[1] * (dh(-v1) + dh(1) + dh(-1) + dh(v1)) +
+             gaussgrad[2] * (dh(-m1) + dh(p1) + dh(-p1) + dh(m1)) + gaussgrad[3] * (dh(-v2) + dh(-2) + dh(2) + dh(v2)) +
+             gaussgrad[4] * (dh(-v2 - 1) + dh(-v2 + 1) + dh(-TS - 2) + dh(-TS + 2) + dh(TS - 2) + dh(TS + 2) +
+                             dh(v2 - 1) + dh(v2 + 1)) +
+             gaussgrad[5] * (dh(-m2) + dh(p2) + dh(-p2) + dh(m2)));
         if (nt > 0.f) {
           S.nyquist[idx >> 1] = 1;
           s_doNyq = 1;
@@ -414,16 +466,15 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
         areawt = xdiv2f(areawt);
         const float hcdvar2 = epssq + fabsf(areawt * sumsqh - sumh * sumh);
         const float vcdvar2 = epssq + fabsf(areawt * sumsqv - sumv * sumv);
-        S.hvwt[idx >> 1] = hcdvar2 / (vcdvar2 + hcdvar2);
+        hvwt[idx >> 1] = hcdvar2 / (vcdvar2 + hcdvar2);
       }
       __syncthreads();
     }
-    // Gauss-Seidel sweep over rows (row rr reads the updated row rr-1).
+    // Gauss-Seidel sweep of hvwt in shared memory (row rr reads row rr-1
+    // already updated), then the per-site green / Dgrb2 in parallel.
     {
       const int a = 8;
       const int per_row = rb_count(a);
-      float* hvwt = S.hvwt;
-      float* rgbgreen = S.rgbgreen;
       for (int rr = a; rr < rr1 - a; rr++) {
         for (int k = tid; k < per_row; k += nth) {
           const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * k;
@@ -431,18 +482,27 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
           const int idx = rr * TS + cc;
           const float hvwtalt =
               0.25f * (hvwt[(idx - m1) >> 1] + hvwt[(idx + p1) >> 1] + hvwt[(idx - p1) >> 1] + hvwt[(idx + m1) >> 1]);
-          const float hv = fabsf(0.5f - hvwt[idx >> 1]) < fabsf(0.5f - hvwtalt) ? hvwtalt : hvwt[idx >> 1];
-          hvwt[idx >> 1] = hv;
-          const float d0 = hv * S.vcd[idx] + (1.f - hv) * S.hcd[idx];
-          S.Dgrb0[idx >> 1] = d0;
-          const float g = cfa[idx] + d0;
-          rgbgreen[idx] = g;
-          const bool nq2 = S.nyquist2[idx >> 1] != 0;
-          S.Dgrb2h[idx >> 1] = nq2 ? SQR(g - xdiv2f(rgbgreen[idx - 1] + rgbgreen[idx + 1])) : 0.f;
-          S.Dgrb2v[idx >> 1] = nq2 ? SQR(g - xdiv2f(rgbgreen[idx - v1] + rgbgreen[idx + v1])) : 0.f;
+          const float cur = hvwt[idx >> 1];
+          hvwt[idx >> 1] = fabsf(0.5f - cur) < fabsf(0.5f - hvwtalt) ? hvwtalt : cur;
         }
         __syncthreads();
       }
+      for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
+        const int rr = a + i / per_row;
+        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        if (cc >= cc1 - a) continue;
+        const int idx = rr * TS + cc;
+        const float hv = hvwt[idx >> 1];
+        const float d0 = hv * S.vcd[idx] + (1.f - hv) * S.hcd[idx];
+        S.Dgrb0[idx >> 1] = d0;
+        const float g = cfa[idx] + d0;
+        S.rgbg[idx >> 1] = g;
+        const bool nq2 = S.nyquist2[idx >> 1] != 0;
+        // horizontal / vertical neighbours are G sites: their green is cfa
+        S.Dgrb2h[idx >> 1] = nq2 ? SQR(g - xdiv2f(cfa[idx - 1] + cfa[idx + 1])) : 0.f;
+        S.Dgrb2v[idx >> 1] = nq2 ? SQR(g - xdiv2f(cfa[idx - v1] + cfa[idx + v1])) : 0.f;
+      }
+      __syncthreads();
     }
     if (doNyquist) {
       const int a = 8;
@@ -467,7 +527,7 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
                      gquinc[3] * (D2v[(idx - m2) >> 1] + D2v[(idx + p2) >> 1] + D2v[(idx - p2) >> 1] + D2v[(idx + m2) >> 1]));
         const float d0 = (S.hcd[idx] * gvarv + S.vcd[idx] * gvarh) / (gvarv + gvarh);
         S.Dgrb0[idx >> 1] = d0;
-        S.rgbgreen[idx] = cfa[idx] + d0;
+        S.rgbg[idx >> 1] = cfa[idx] + d0;
       }
       __syncthreads();
     }
@@ -481,25 +541,25 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
       if ((fc_rt(A, rr, 2) & 1) == 0) {
         S.delp[idx >> 1] = fabsf(cfa[idx + p1] - cfa[idx - p1]);
         S.delm[idx >> 1] = fabsf(cfa[idx + m1] - cfa[idx - m1]);
-        S.Dgrbsq1p[idx >> 1] = SQR(cfa[idx + 1] - cfa[idx + 1 - p1]) + SQR(cfa[idx + 1] - cfa[idx + 1 + p1]);
-        S.Dgrbsq1m[idx >> 1] = SQR(cfa[idx + 1] - cfa[idx + 1 - m1]) + SQR(cfa[idx + 1] - cfa[idx + 1 + m1]);
+        S.Dq1p[idx >> 1] = SQR(cfa[idx + 1] - cfa[idx + 1 - p1]) + SQR(cfa[idx + 1] - cfa[idx + 1 + p1]);
+        S.Dq1m[idx >> 1] = SQR(cfa[idx + 1] - cfa[idx + 1 - m1]) + SQR(cfa[idx + 1] - cfa[idx + 1 + m1]);
       } else {
-        S.Dgrbsq1p[idx >> 1] = SQR(cfa[idx] - cfa[idx - p1]) + SQR(cfa[idx] - cfa[idx + p1]);
-        S.Dgrbsq1m[idx >> 1] = SQR(cfa[idx] - cfa[idx - m1]) + SQR(cfa[idx] - cfa[idx + m1]);
+        S.Dq1p[idx >> 1] = SQR(cfa[idx] - cfa[idx - p1]) + SQR(cfa[idx] - cfa[idx + p1]);
+        S.Dq1m[idx >> 1] = SQR(cfa[idx] - cfa[idx - m1]) + SQR(cfa[idx] - cfa[idx + m1]);
         S.delp[idx >> 1] = fabsf(cfa[idx + 1 + p1] - cfa[idx + 1 - p1]);
         S.delm[idx >> 1] = fabsf(cfa[idx + 1 + m1] - cfa[idx + 1 - m1]);
       }
     }
     __syncthreads();
 
-    // ---- S8 diagonal R/B interpolation (:1504-1532)
+    // ---- S8 diagonal R/B interpolation (:1504-1532); pmwt into SMEM
     {
       const int a = 8;
       const int per_row = rb_count(a);
       const float* delp = S.delp;
       const float* delm = S.delm;
-      const float* Dq1m = S.Dgrbsq1m;
-      const float* Dq1p = S.Dgrbsq1p;
+      const float* Dq1m = S.Dq1m;
+      const float* Dq1p = S.Dq1p;
       for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
         const int rr = a + i / per_row;
         const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
@@ -549,16 +609,15 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
                      gausseven[1] * (Dq1p[(idx - v2 - 1) >> 1] + Dq1p[(idx - v2 + 1) >> 1] + Dq1p[(idx - 2 - v1) >> 1] +
                                      Dq1p[(idx + 2 - v1) >> 1] + Dq1p[(idx - 2 + v1) >> 1] + Dq1p[(idx + 2 + v1) >> 1] +
                                      Dq1p[(idx + v2 - 1) >> 1] + Dq1p[(idx + v2 + 1) >> 1]));
-        S.pmwt[idx1] = rbvarm / (rbvarp + rbvarm);
+        pmwt[idx1] = rbvarm / (rbvarp + rbvarm);
       }
     }
     __syncthreads();
 
-    // ---- S9 (:1534-1592): Gauss-Seidel pmwt sweep + rbint
+    // ---- S9 (:1534-1592): Gauss-Seidel pmwt sweep in SMEM, then rbint
     {
       const int a = 10;
       const int per_row = rb_count(a);
-      float* pmwt = S.pmwt;
       for (int rr = a; rr < rr1 - a; rr++) {
         for (int k = tid; k < per_row; k += nth) {
           const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * k;
@@ -566,24 +625,34 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
           const int idx = rr * TS + cc, idx1 = idx >> 1;
           const float pmwtalt =
               0.25f * (pmwt[(idx - m1) >> 1] + pmwt[(idx + p1) >> 1] + pmwt[(idx - p1) >> 1] + pmwt[(idx + m1) >> 1]);
-          float pw = pmwt[idx1];
-          if (fabsf(0.5f - pw) < fabsf(0.5f - pmwtalt)) pw = pmwtalt;
-          pmwt[idx1] = pw;
-          S.rbint[idx1] = xdiv2f(cfa[idx] + S.rbm[idx1] * (1.f - pw) + S.rbp[idx1] * pw);
+          const float pw = pmwt[idx1];
+          if (fabsf(0.5f - pw) < fabsf(0.5f - pmwtalt)) pmwt[idx1] = pmwtalt;
         }
         __syncthreads();
       }
+      for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
+        const int rr = a + i / per_row;
+        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        if (cc >= cc1 - a) continue;
+        const int idx = rr * TS + cc, idx1 = idx >> 1;
+        const float pw = pmwt[idx1];
+        S.rbint[idx1] = xdiv2f(cfa[idx] + S.rbm[idx1] * (1.f - pw) + S.rbp[idx1] * pw);
+      }
     }
+    // Dgrb1 starts as zeros (its unwritten cells are read by the diagonal
+    // step); it occupies Dgrb2h's half plane, dead after stage 6
+    for (int i = tid; i < HALF / 4; i += nth) reinterpret_cast<float4*>(S.Dgrb1)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
     // dirwts1 as the reference reads it after pmwt was stored over it
     // (half index k of pmwt == float offset k of dirwts1).
     auto pm_written = [&](int p) -> bool {
-      if (p < 0 || p >= TS * TSH) return false;
+      if (p < 0 || p >= HALF) return false;
       const int r2 = (2 * p) / TS;
       const int c0 = (2 * p) % TS;
       const int crb = c0 + (int)(fc_rt(A, r2, 2) & 1);
       return r2 >= 8 && r2 < rr1 - 8 && crb >= 8 && crb < cc1 - 8;
     };
-    auto dirwts1_eff = [&](int p) -> float { return pm_written(p) ? S.pmwt[p] : dirwts1[p]; };
+    auto dirwts1_eff = [&](int p) -> float { return pm_written(p) ? pmwt[p] : dirwts1_at(cfa, p); };
     {
       const int a = 12;
       const int per_row = rb_count(a);
@@ -593,7 +662,7 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
         const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
         if (cc >= cc1 - a) continue;
         const int idx = rr * TS + cc, idx1 = idx >> 1;
-        if (fabsf(0.5f - S.pmwt[idx1]) >= fabsf(0.5f - S.hvwt[idx1])) continue;
+        if (fabsf(0.5f - pmwt[idx1]) >= fabsf(0.5f - hvwt[idx1])) continue;
         const float cru = xmul2f(cfa[idx - v1]) / (eps + rbint[idx1] + rbint[idx1 - v1]);
         const float crd = xmul2f(cfa[idx + v1]) / (eps + rbint[idx1] + rbint[idx1 + v1]);
         const float crl = xmul2f(cfa[idx - 1]) / (eps + rbint[idx1] + rbint[idx1 - 1]);
@@ -602,7 +671,8 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
         const float gd = fabsf(1.f - crd) < arthresh ? rbint[idx1] * crd : cfa[idx + v1] + xdiv2f(rbint[idx1] - rbint[idx1 + v1]);
         const float gl = fabsf(1.f - crl) < arthresh ? rbint[idx1] * crl : cfa[idx - 1] + xdiv2f(rbint[idx1] - rbint[idx1 - 1]);
         const float gr = fabsf(1.f - crr) < arthresh ? rbint[idx1] * crr : cfa[idx + 1] + xdiv2f(rbint[idx1] - rbint[idx1 + 1]);
-        float Gintv = (dirwts0[idx - v1] * gd + dirwts0[idx + v1] * gu) / (dirwts0[idx + v1] + dirwts0[idx - v1]);
+        const float d0m = dirwts0_at(cfa, idx - v1), d0p = dirwts0_at(cfa, idx + v1);
+        float Gintv = (d0m * gd + d0p * gu) / (d0p + d0m);
         const float d1m = dirwts1_eff(idx - 1), d1p = dirwts1_eff(idx + 1);
         float Ginth = (d1m * gr + d1p * gl) / (d1m + d1p);
         if (Gintv < rbint[idx1]) {
@@ -623,9 +693,9 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
         }
         if (Ginth > A.clip_pt) Ginth = median3(Ginth, cfa[idx - 1], cfa[idx + 1]);
         if (Gintv > A.clip_pt) Gintv = median3(Gintv, cfa[idx - v1], cfa[idx + v1]);
-        const float hv = S.hvwt[idx1];
+        const float hv = hvwt[idx1];
         const float g = Ginth * (1.f - hv) + Gintv * hv;
-        S.rgbgreen[idx] = g;
+        S.rgbg[idx1] = g;
         S.Dgrb0[idx1] = g - cfa[idx];
       }
     }
@@ -683,7 +753,6 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
       if (row < 0 || row >= H || col < 0 || col >= W) continue;
       const int t = rr * TS + cc;
       float r, g, b;
-      const float* hvwt = S.hvwt;
       const float* D0 = S.Dgrb0;
       const float* D1 = S.Dgrb1;
       if (fc_rt(A, row, col) == 1) {
@@ -699,7 +768,7 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
         r = g - r_diff;
         b = g - b_diff;
       } else {
-        g = S.rgbgreen[t];
+        g = S.rgbg[t >> 1];
         r = g - D0[t >> 1];
         b = g - D1[t >> 1];
       }
@@ -753,7 +822,7 @@ __global__ void k_border_interp(float* rgb, int W, int H, uint32_t filters, int 
 size_t ws_bytes_amaze(size_t w, size_t h) {
   (void)w;
   (void)h;
-  return 148u * 2u * kSlabBytes + 4096;
+  return 160u * kSlabBytes + 4096;
 }
 
 lre_status launch_amaze(Context* c, const float* raw, int cstride, float* rgb, size_t w, size_t h, uint32_t filters,
@@ -779,11 +848,11 @@ lre_status launch_amaze(Context* c, const float* raw, int cstride, float* rgb, s
     if (A.cfarray[0][0] == 0) { A.ey = 0; A.ex = 0; } else { A.ey = 1; A.ex = 1; }
   }
   A.scale = 1.0f / maximum_value;
-  A.n_top = (int)((h + 16 + (TS - 32) - 1) / (TS - 32));
-  A.n_left = (int)((w + 16 + (TS - 32) - 1) / (TS - 32));
-  // verify the tile count matches the reference's loop bounds
-  while (A.n_top > 0 && -16 + (A.n_top - 1) * (TS - 32) >= (int)h) A.n_top--;
-  while (A.n_left > 0 && -16 + (A.n_left - 1) * (TS - 32) >= (int)w) A.n_left--;
+  // tile grid of :1243-1246
+  A.n_top = 0;
+  for (int top = -16; top < (int)h; top += TS - 32) A.n_top++;
+  A.n_left = 0;
+  for (int left = -16; left < (int)w; left += TS - 32) A.n_left++;
   const int tiles = A.n_top * A.n_left;
   int nblk = std::min(tiles, c->sm_count);
   if (nblk < 1) nblk = 1;
@@ -791,7 +860,8 @@ lre_status launch_amaze(Context* c, const float* raw, int cstride, float* rgb, s
   A.tile_counter = reinterpret_cast<int*>(c->ws.take(256));
   if (!A.scratch || !A.tile_counter) return fail(c, LRE_ERR_OUT_OF_MEMORY, "demosaic_bayer_amaze: workspace too small");
   LRE_CUDA_TRY(c, cudaMemsetAsync(A.tile_counter, 0, sizeof(int), c->stream));
-  k_amaze<<<nblk, AMZ_THREADS, 0, c->stream>>>(A);
+  LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_amaze, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
+  k_amaze<<<nblk, AMZ_THREADS, kSmemBytes, c->stream>>>(A);
   const int band = 4;
   const long long nb = 2LL * band * (long long)w + 2LL * band * (long long)(h > 8 ? h - 8 : 0);
   k_border_interp<<<grid_for((size_t)nb, 256, c->sm_count * 2), 256, 0, c->stream>>>(rgb, (int)w, (int)h, filters, band);
