@@ -140,6 +140,16 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
   const float norm_ref = fmaxf(*d_maxg, 1e-6f);
   const float inv_norm = 1.f / norm_ref;
 
+  // Reciprocal window counts along x and y for every column / row of the
+  // input region (0 outside the image): a box mean is sum * inv_x * inv_y,
+  // within two double ulps of the reference's sum / area.
+  __shared__ double inv_x[T + 4 * 16], inv_y[T + 4 * 16];
+  for (int i = threadIdx.x; i < IN; i += blockDim.x) {
+    const int gx = ix0 + i, gy = iy0 + i;
+    inv_x[i] = (gx >= 0 && gx < W) ? 1.0 / (double)win_count(gx, r, W) : 0.0;
+    inv_y[i] = (gy >= 0 && gy < H) ? 1.0 / (double)win_count(gy, r, H) : 0.0;
+  }
+
   // 1. stage normalised R, G, B (zeros outside the image).
   for (int i = threadIdx.x; i < IN * IN; i += blockDim.x) {
     int gy = iy0 + i / IN, gx = ix0 + i % IN;
@@ -163,22 +173,12 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
     return (double)(v * v);
   });
   __syncthreads();
-  vsum(h0, AB, AB, r, [&](int j, int k, double s) {
-    int gy = ay0 + j, gx = ax0 + k;
-    double m = 0.0;
-    if (gx >= 0 && gx < W && gy >= 0 && gy < H) m = s / (double)(win_count(gx, r, W) * win_count(gy, r, H));
-    mI[j * AB + k] = m;
-  });
+  // a/b-region cell (j, k) sits at input-region index (j + r, k + r)
+  vsum(h0, AB, AB, r, [&](int j, int k, double s) { mI[j * AB + k] = s * (inv_x[k + r] * inv_y[j + r]); });
   __syncthreads();
   vsum(h1, AB, AB, r, [&](int j, int k, double s) {
-    int gy = ay0 + j, gx = ax0 + k;
-    double v = 0.0;
-    if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
-      double mII = s / (double)(win_count(gx, r, W) * win_count(gy, r, H));
-      double m = mI[j * AB + k];
-      v = mII - m * m;
-    }
-    vI[j * AB + k] = v;
+    const double m = mI[j * AB + k];
+    vI[j * AB + k] = s * (inv_x[k + r] * inv_y[j + r]) - m * m;
   });
   __syncthreads();
 
@@ -215,8 +215,8 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
           int gy = ay0 + j, gx = ax0 + k;
           float a_f = 0.f, b_f = 0.f;
           if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
-            double area = (double)(win_count(gx, r, W) * win_count(gy, r, H));
-            double mp = sp / area, mIp = sip / area;
+            const double inv_area = inv_x[k + r] * inv_y[j + r];
+            double mp = sp * inv_area, mIp = sip * inv_area;
             double mi = mI[j * AB + k];
             double cov = mIp - mi * mp;
             double a = cov / (vI[j * AB + k] + (double)eps);
@@ -247,9 +247,13 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
   }
   __syncthreads();
 
-  // 5. second box level and blend.  Each thread owns a fixed set of output
-  // pixels; the three sweeps (R, B, edge) keep their results in registers.
+  // 5. second box level and blend.  Each thread owns PER vertically adjacent
+  // output pixels of one column (its window sums slide down by one row per
+  // pixel); the three sweeps (R, B, edge) keep their results in registers.
   constexpr int PER = (T * T + AX_THREADS - 1) / AX_THREADS;
+  const int my_k = threadIdx.x % T;
+  const int my_j0 = (threadIdx.x / T) * PER;
+  const bool my_active = my_j0 < T;
   float qR[PER], qB[PER], ew[PER];
   for (int pass = 0; pass < 3; pass++) {
     if (pass < 2) {
@@ -261,28 +265,35 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
       hsum(h0, AB, T, r, [&](int j, int k) { return (double)er[j * AB + k]; });
     }
     __syncthreads();
-#pragma unroll
-    for (int q = 0; q < PER; q++) {
-      int i = threadIdx.x + q * AX_THREADS;
-      if (i >= T * T) break;
-      int j = i / T, k = i % T;
-      int gy = y0 + j, gx = x0 + k;
-      if (gx >= W || gy >= H) continue;
-      double area = (double)(win_count(gx, r, W) * win_count(gy, r, H));
+    if (my_active) {
+      const int k = my_k;
       double s0 = 0.0, s1 = 0.0;
       for (int t = 0; t <= 2 * r; t++) {
-        s0 += h0[(j + t) * T + k];
-        if (pass < 2) s1 += h1[(j + t) * T + k];
+        s0 += h0[(my_j0 + t) * T + k];
+        if (pass < 2) s1 += h1[(my_j0 + t) * T + k];
       }
-      if (pass < 2) {
-        double ma = s0 / area, mb = s1 / area;
-        float I = sG[(j + 2 * r) * IN + (k + 2 * r)];
-        float qv = (float)(ma * (double)I + mb);
-        if (pass == 0) qR[q] = qv; else qB[q] = qv;
-      } else {
-        double m = s0 / area;
-        float t = clampf(((float)m - 0.01f) / 0.05f, 0.f, 1.f);
-        ew[q] = t * t * (3.f - 2.f * t);
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const int j = my_j0 + q;
+        if (q > 0) {
+          s0 += h0[(j + 2 * r) * T + k];
+          s0 -= h0[(j - 1) * T + k];
+          if (pass < 2) {
+            s1 += h1[(j + 2 * r) * T + k];
+            s1 -= h1[(j - 1) * T + k];
+          }
+        }
+        const double inv_area = inv_x[k + 2 * r] * inv_y[j + 2 * r];
+        if (pass < 2) {
+          const double ma = s0 * inv_area, mb = s1 * inv_area;
+          const float I = sG[(j + 2 * r) * IN + (k + 2 * r)];
+          const float qv = (float)(ma * (double)I + mb);
+          if (pass == 0) qR[q] = qv; else qB[q] = qv;
+        } else {
+          const double m = s0 * inv_area;
+          const float t = clampf(((float)m - 0.01f) / 0.05f, 0.f, 1.f);
+          ew[q] = t * t * (3.f - 2.f * t);
+        }
       }
     }
     __syncthreads();
@@ -290,9 +301,8 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
 
 #pragma unroll
   for (int q = 0; q < PER; q++) {
-    int i = threadIdx.x + q * AX_THREADS;
-    if (i >= T * T) break;
-    int j = i / T, k = i % T;
+    if (!my_active) break;
+    const int j = my_j0 + q, k = my_k;
     int gy = y0 + j, gx = x0 + k;
     if (gx >= W || gy >= H) continue;
     int c = (j + 2 * r) * IN + (k + 2 * r);

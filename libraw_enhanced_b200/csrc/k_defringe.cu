@@ -168,6 +168,63 @@ __global__ void __launch_bounds__(256) k_df_blur(BlurJob job, GaussTaps taps, in
   }
 }
 
+// Register-tiled blur for a compile-time tap radius: planes are processed one
+// after another through the same 18 KB of shared memory (so 8 CTAs fit on an
+// SM), each thread produces 8 horizontal or 4 vertical outputs from operands
+// held in registers.  Tap order and clamping are those of k_df_blur.
+template <int KS>
+__global__ void __launch_bounds__(256) k_df_blur_fast(BlurJob job, GaussTaps taps, int W, int H, const DfScalars* sc) {
+  constexpr int E = BT + 2 * KS;
+  constexpr int LD = E + 1;  // odd row stride: conflict-light row reads
+  __shared__ float s_in[E * LD];
+  __shared__ float s_h[E * BT];
+  const int x0 = blockIdx.x * BT, y0 = blockIdx.y * BT;
+  float w[2 * KS + 1];
+#pragma unroll
+  for (int t = 0; t <= 2 * KS; t++) w[t] = taps.w[t];
+  for (int p = 0; p < job.np; p++) {
+    for (int i = threadIdx.x; i < E * E; i += blockDim.x) {
+      const int r = i / E, q = i % E;
+      const int gy = min(max(y0 - KS + r, 0), H - 1);
+      const int gx = min(max(x0 - KS + q, 0), W - 1);
+      s_in[r * LD + q] = blur_src(job, p, sc, gx, gy, W);
+    }
+    __syncthreads();
+    // horizontal: item = (halo row j, group of 8 output columns)
+    for (int item = threadIdx.x; item < E * (BT / 8); item += blockDim.x) {
+      const int j = item / (BT / 8), k0 = (item % (BT / 8)) * 8;
+      float x[8 + 2 * KS];
+#pragma unroll
+      for (int i = 0; i < 8 + 2 * KS; i++) x[i] = s_in[j * LD + k0 + i];
+#pragma unroll
+      for (int o = 0; o < 8; o++) {
+        float acc = 0.f;
+#pragma unroll
+        for (int t = 0; t <= 2 * KS; t++) acc += w[t] * x[o + t];
+        s_h[j * BT + k0 + o] = acc;
+      }
+    }
+    __syncthreads();
+    // vertical: item = (output column k, group of 4 output rows)
+    {
+      const int k = threadIdx.x % BT, j0 = (threadIdx.x / BT) * 4;
+      float x[4 + 2 * KS];
+#pragma unroll
+      for (int i = 0; i < 4 + 2 * KS; i++) x[i] = s_h[(j0 + i) * BT + k];
+      const int gx = x0 + k;
+#pragma unroll
+      for (int o = 0; o < 4; o++) {
+        float acc = 0.f;
+#pragma unroll
+        for (int t = 0; t <= 2 * KS; t++) acc += w[t] * x[o + t];
+        const int gy = y0 + j0 + o;
+        if (gx < W && gy < H) job.out[p][(size_t)gy * W + gx] = acc;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------- K3
 struct DfConst {
   float edge_thr, chroma_thr, strength, green_scale;
@@ -290,7 +347,7 @@ __global__ void __launch_bounds__(256) k_df_line(const float* __restrict__ src, 
 }
 
 // ---------------------------------------------------------------- K7
-__global__ void k_df_main(const float* src, float* dst, int W, int H, DfPlanes P, DfConst k, const DfScalars* sc) {
+__global__ void __launch_bounds__(256, 3) k_df_main(const float* src, float* dst, int W, int H, DfPlanes P, DfConst k, const DfScalars* sc) {
   const float sensitivity = sclamp(sqrtf(smax(k.strength, 1.0f)), 1.0f, 2.5f);
   const float inv_s = 1.0f / sensitivity;
   const float mask_cutoff = 0.02f * inv_s;
@@ -594,6 +651,12 @@ __global__ void k_df_maxg(const float* __restrict__ src, size_t n, DfScalars* sc
 }
 
 lre_status run_blur(Context* c, const BlurJob& job, const GaussTaps& taps, int W, int H, const DfScalars* sc) {
+  if (taps.ks == 10) {  // radius 10 (the reference default): sigma 10/3, 21 taps
+    dim3 grid((W + BT - 1) / BT, (H + BT - 1) / BT);
+    k_df_blur_fast<10><<<grid, 256, 0, c->stream>>>(job, taps, W, H, sc);
+    count_launch(c);
+    return check_launch(c, "defringe blur");
+  }
   const int E = BT + 2 * taps.ks;
   size_t smem = ((size_t)job.np * E * E + (size_t)job.np * E * BT) * sizeof(float);
   LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_df_blur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
