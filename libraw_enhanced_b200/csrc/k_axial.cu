@@ -49,7 +49,9 @@ __host__ __device__ inline AxGeom ax_geom(int T, int r) {
     o += (b + 15) & ~size_t(15);
     return cur;
   };
-  size_t in2 = (size_t)g.IN * g.IN, hb = (size_t)g.IN * g.AB, ab2 = (size_t)g.AB * g.AB;
+  // odd row strides (IN+1 floats, AB+1 doubles) keep warp accesses that walk
+  // down rows on distinct shared-memory banks
+  size_t in2 = (size_t)g.IN * (g.IN + 1), hb = (size_t)g.IN * (g.AB + 1), ab2 = (size_t)g.AB * g.AB;
   g.off_h0 = take(hb * 8);
   g.off_h1 = take(hb * 8);
   g.off_mi = take(ab2 * 8);
@@ -57,52 +59,65 @@ __host__ __device__ inline AxGeom ax_geom(int T, int r) {
   g.off_g = take(in2 * 4);
   g.off_r = take(in2 * 4);
   g.off_b = take(in2 * 4);
-  g.off_ar = take(ab2 * 4);
-  g.off_br = take(ab2 * 4);
-  g.off_ab = take(ab2 * 4);
-  g.off_bb = take(ab2 * 4);
-  g.off_er = take(ab2 * 4);
+  const size_t abp = (size_t)g.AB * (g.AB + 1);  // float planes, row stride AB + 1
+  g.off_ar = take(abp * 4);
+  g.off_br = take(abp * 4);
+  g.off_ab = take(abp * 4);
+  g.off_bb = take(abp * 4);
+  g.off_er = take(abp * 4);
   g.bytes = o;
   return g;
 }
 
 // Sliding horizontal window sums: dst[j][k] = sum_{t=0..2r} val(j, k + t)
-// for j < rows, k < cols_out.  Rows are split into segments so every thread
-// has work; inside a segment the sum slides with one add and one subtract.
+// for j < rows, k < cols_out, stored with row stride cols_out + 1.  Rows are
+// split into segments so every thread has work; inside a segment the sum
+// slides with one add and one subtract.  Consecutive threads take
+// consecutive rows of the same segment (distinct banks with odd strides).
 template <typename F>
 __device__ void hsum(double* dst, int rows, int cols_out, int r, F val) {
-  const int seg = 8;
+  const int seg = max(1, (rows * cols_out + (int)blockDim.x - 1) / (int)blockDim.x);
   const int nseg = (cols_out + seg - 1) / seg;
+  const int ld = cols_out + 1;
   for (int item = threadIdx.x; item < rows * nseg; item += blockDim.x) {
-    int j = item / nseg, s = item % nseg;
+    int j = item % rows, s = item / rows;
     int k0 = s * seg, k1 = min(cols_out, k0 + seg);
     double acc = 0.0;
     for (int t = 0; t <= 2 * r; t++) acc += val(j, k0 + t);
-    dst[j * cols_out + k0] = acc;
+    dst[j * ld + k0] = acc;
     for (int k = k0 + 1; k < k1; k++) {
       acc += val(j, k + 2 * r);
       acc -= val(j, k - 1);
-      dst[j * cols_out + k] = acc;
+      dst[j * ld + k] = acc;
     }
   }
 }
 
-// Sliding vertical sums over a row-major [rows_in][cols] double buffer:
-// out(j, k) = sum_{t=0..2r} src[(j+t)*cols + k], handed to `emit(j, k, sum)`.
-template <typename E>
-__device__ void vsum(const double* src, int rows_out, int cols, int r, E emit) {
-  const int seg = 8;
-  const int nseg = (rows_out + seg - 1) / seg;
-  for (int item = threadIdx.x; item < cols * nseg; item += blockDim.x) {
-    int k = item % cols, s = item / cols;
-    int j0 = s * seg, j1 = min(rows_out, j0 + seg);
-    double acc = 0.0;
-    for (int t = 0; t <= 2 * r; t++) acc += src[(j0 + t) * cols + k];
-    emit(j0, k, acc);
-    for (int j = j0 + 1; j < j1; j++) {
-      acc += src[(j + 2 * r) * cols + k];
-      acc -= src[(j - 1) * cols + k];
-      emit(j, k, acc);
+// Two horizontal window sums in one sweep (two independent accumulators per
+// thread, for quantities that are always consumed together).
+template <typename F0, typename F1>
+__device__ void hsum2(double* d0, double* d1, int rows, int cols_out, int r, F0 v0, F1 v1) {
+  // segment length chosen so one pass of the block covers every row segment
+  const int seg = max(1, (rows * cols_out + (int)blockDim.x - 1) / (int)blockDim.x);
+  const int nseg = (cols_out + seg - 1) / seg;
+  const int ld = cols_out + 1;
+  for (int item = threadIdx.x; item < rows * nseg; item += blockDim.x) {
+    int j = item % rows, s = item / rows;
+    int k0 = s * seg, k1 = min(cols_out, k0 + seg);
+    double a0 = 0.0, a1 = 0.0;
+    for (int t = 0; t <= 2 * r; t++) {
+      a0 += v0(j, k0 + t);
+      a1 += v1(j, k0 + t);
+    }
+    d0[j * ld + k0] = a0;
+    d1[j * ld + k0] = a1;
+    for (int k = k0 + 1; k < k1; k++) {
+      a0 += v0(j, k + 2 * r);
+      a1 += v1(j, k + 2 * r);
+      a0 -= v0(j, k - 1);
+      a1 -= v1(j, k - 1);
+      d0[j * ld + k] = a0;
+      d1[j * ld + k] = a1;
     }
   }
 }
@@ -150,9 +165,14 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
     inv_y[i] = (gy >= 0 && gy < H) ? 1.0 / (double)win_count(gy, r, H) : 0.0;
   }
 
+  const int SP = IN + 1;   // row stride of the staged planes (odd)
+  const int LDH = AB + 1;  // row stride of the level-1 window sums (odd)
+  const int LDB = AB + 1;  // row stride of the a/b/edge planes (odd)
+
   // 1. stage normalised R, G, B (zeros outside the image).
   for (int i = threadIdx.x; i < IN * IN; i += blockDim.x) {
-    int gy = iy0 + i / IN, gx = ix0 + i % IN;
+    const int j = i / IN, k = i % IN;
+    int gy = iy0 + j, gx = ix0 + k;
     float r_ = 0.f, g_ = 0.f, b_ = 0.f;
     if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
       const float* p = src + ((size_t)gy * W + gx) * 3;
@@ -160,26 +180,46 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
       g_ = p[1] * inv_norm;
       b_ = p[2] * inv_norm;
     }
-    sR[i] = r_;
-    sG[i] = g_;
-    sB[i] = b_;
+    sR[j * SP + k] = r_;
+    sG[j * SP + k] = g_;
+    sB[j * SP + k] = b_;
   }
   __syncthreads();
 
   // 2. guide statistics mean(G), var(G) over the a/b region.
-  hsum(h0, IN, AB, r, [&](int j, int k) { return (double)sG[j * IN + k]; });
-  hsum(h1, IN, AB, r, [&](int j, int k) {
-    float v = sG[j * IN + k];
-    return (double)(v * v);
-  });
+  hsum2(
+      h0, h1, IN, AB, r, [&](int j, int k) { return (double)sG[j * SP + k]; },
+      [&](int j, int k) {
+        float v = sG[j * SP + k];
+        return (double)(v * v);
+      });
   __syncthreads();
   // a/b-region cell (j, k) sits at input-region index (j + r, k + r)
-  vsum(h0, AB, AB, r, [&](int j, int k, double s) { mI[j * AB + k] = s * (inv_x[k + r] * inv_y[j + r]); });
-  __syncthreads();
-  vsum(h1, AB, AB, r, [&](int j, int k, double s) {
-    const double m = mI[j * AB + k];
-    vI[j * AB + k] = s * (inv_x[k + r] * inv_y[j + r]) - m * m;
-  });
+  {
+    const int seg = 8;
+    const int nseg = (AB + seg - 1) / seg;
+    for (int item = threadIdx.x; item < AB * nseg; item += blockDim.x) {
+      const int k = item % AB, s = item / AB;
+      const int j0 = s * seg, j1 = min(AB, j0 + seg);
+      double s0 = 0.0, s1 = 0.0;
+      for (int t = 0; t <= 2 * r; t++) {
+        s0 += h0[(j0 + t) * LDH + k];
+        s1 += h1[(j0 + t) * LDH + k];
+      }
+      for (int j = j0; j < j1; j++) {
+        if (j > j0) {
+          s0 += h0[(j + 2 * r) * LDH + k];
+          s1 += h1[(j + 2 * r) * LDH + k];
+          s0 -= h0[(j - 1) * LDH + k];
+          s1 -= h1[(j - 1) * LDH + k];
+        }
+        const double inv_area = inv_x[k + r] * inv_y[j + r];
+        const double m = s0 * inv_area;
+        mI[j * AB + k] = m;
+        vI[j * AB + k] = s1 * inv_area - m * m;
+      }
+    }
+  }
   __syncthreads();
 
   // 3. per-channel a, b (R then B), sharing the guide statistics.
@@ -187,8 +227,9 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
     const float* sX = ch == 0 ? sR : sB;
     float* aX = ch == 0 ? aR : aB;
     float* bX = ch == 0 ? bR : bB;
-    hsum(h0, IN, AB, r, [&](int j, int k) { return (double)sX[j * IN + k]; });
-    hsum(h1, IN, AB, r, [&](int j, int k) { return (double)(sG[j * IN + k] * sX[j * IN + k]); });
+    hsum2(
+        h0, h1, IN, AB, r, [&](int j, int k) { return (double)sX[j * SP + k]; },
+        [&](int j, int k) { return (double)(sG[j * SP + k] * sX[j * SP + k]); });
     __syncthreads();
     // mean(X) into aX temporarily as double is not possible (float); keep the
     // double mean in vI's sibling: reuse h0's first AB*AB doubles after the
@@ -202,15 +243,15 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
         int j0 = s * seg, j1 = min(AB, j0 + seg);
         double sp = 0.0, sip = 0.0;
         for (int t = 0; t <= 2 * r; t++) {
-          sp += h0[(j0 + t) * AB + k];
-          sip += h1[(j0 + t) * AB + k];
+          sp += h0[(j0 + t) * LDH + k];
+          sip += h1[(j0 + t) * LDH + k];
         }
         for (int j = j0; j < j1; j++) {
           if (j > j0) {
-            sp += h0[(j + 2 * r) * AB + k];
-            sp -= h0[(j - 1) * AB + k];
-            sip += h1[(j + 2 * r) * AB + k];
-            sip -= h1[(j - 1) * AB + k];
+            sp += h0[(j + 2 * r) * LDH + k];
+            sp -= h0[(j - 1) * LDH + k];
+            sip += h1[(j + 2 * r) * LDH + k];
+            sip -= h1[(j - 1) * LDH + k];
           }
           int gy = ay0 + j, gx = ax0 + k;
           float a_f = 0.f, b_f = 0.f;
@@ -224,8 +265,8 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
             a_f = (float)a;
             b_f = (float)b;
           }
-          aX[j * AB + k] = a_f;
-          bX[j * AB + k] = b_f;
+          aX[j * LDB + k] = a_f;
+          bX[j * LDB + k] = b_f;
         }
       }
     }
@@ -238,12 +279,12 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
     int gy = ay0 + j, gx = ax0 + k;
     float e = 0.f;
     if (gx >= 1 && gx < W - 1 && gy >= 1 && gy < H - 1) {
-      int c = (j + r) * IN + (k + r);
+      int c = (j + r) * SP + (k + r);
       float gxv = sG[c + 1] - sG[c - 1];
-      float gyv = sG[c + IN] - sG[c - IN];
+      float gyv = sG[c + SP] - sG[c - SP];
       e = sqrtf(gxv * gxv + gyv * gyv);
     }
-    er[i] = e;
+    er[j * LDB + k] = e;
   }
   __syncthreads();
 
@@ -259,34 +300,36 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
     if (pass < 2) {
       const float* aX = pass == 0 ? aR : aB;
       const float* bX = pass == 0 ? bR : bB;
-      hsum(h0, AB, T, r, [&](int j, int k) { return (double)aX[j * AB + k]; });
-      hsum(h1, AB, T, r, [&](int j, int k) { return (double)bX[j * AB + k]; });
+      hsum2(
+          h0, h1, AB, T, r, [&](int j, int k) { return (double)aX[j * LDB + k]; },
+          [&](int j, int k) { return (double)bX[j * LDB + k]; });
     } else {
-      hsum(h0, AB, T, r, [&](int j, int k) { return (double)er[j * AB + k]; });
+      hsum(h0, AB, T, r, [&](int j, int k) { return (double)er[j * LDB + k]; });
     }
     __syncthreads();
     if (my_active) {
       const int k = my_k;
+      const int LD2 = T + 1;
       double s0 = 0.0, s1 = 0.0;
       for (int t = 0; t <= 2 * r; t++) {
-        s0 += h0[(my_j0 + t) * T + k];
-        if (pass < 2) s1 += h1[(my_j0 + t) * T + k];
+        s0 += h0[(my_j0 + t) * LD2 + k];
+        if (pass < 2) s1 += h1[(my_j0 + t) * LD2 + k];
       }
 #pragma unroll
       for (int q = 0; q < PER; q++) {
         const int j = my_j0 + q;
         if (q > 0) {
-          s0 += h0[(j + 2 * r) * T + k];
-          s0 -= h0[(j - 1) * T + k];
+          s0 += h0[(j + 2 * r) * LD2 + k];
+          s0 -= h0[(j - 1) * LD2 + k];
           if (pass < 2) {
-            s1 += h1[(j + 2 * r) * T + k];
-            s1 -= h1[(j - 1) * T + k];
+            s1 += h1[(j + 2 * r) * LD2 + k];
+            s1 -= h1[(j - 1) * LD2 + k];
           }
         }
         const double inv_area = inv_x[k + 2 * r] * inv_y[j + 2 * r];
         if (pass < 2) {
           const double ma = s0 * inv_area, mb = s1 * inv_area;
-          const float I = sG[(j + 2 * r) * IN + (k + 2 * r)];
+          const float I = sG[(j + 2 * r) * SP + (k + 2 * r)];
           const float qv = (float)(ma * (double)I + mb);
           if (pass == 0) qR[q] = qv; else qB[q] = qv;
         } else {
@@ -305,7 +348,7 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
     const int j = my_j0 + q, k = my_k;
     int gy = y0 + j, gx = x0 + k;
     if (gx >= W || gy >= H) continue;
-    int c = (j + 2 * r) * IN + (k + 2 * r);
+    int c = (j + 2 * r) * SP + (k + 2 * r);
     float w = strength * ew[q];
     float r_out = sR[c] * (1.f - w) + qR[q] * w;
     float b_out = sB[c] * (1.f - w) + qB[q] * w;
