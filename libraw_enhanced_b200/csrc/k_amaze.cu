@@ -17,12 +17,13 @@
 //
 // Device design: a persistent CTA per SM pulls the reference's tiles from a
 // counter and runs each one stage by stage.
-//   * Scratch: one slab per CTA of 7 full planes (160x160 floats) plus one
+//   * Scratch: one slab per CTA of 6 full planes (160x160 floats) plus one
 //     half plane; the reference's ~20 planes are mapped onto it by lifetime
 //     (a plane is reused once its last reader has run), the cheap gradient
 //     planes (dirwts0/1, delhvsqsum) are recomputed from cfa where read, and
-//     R/B-only quantities are stored half-indexed.  148 slabs (~117 MB) sit
+//     R/B-only quantities are stored half-indexed.  148 slabs (~95 MB) sit
 //     in L2.
+//   * cfa (read by nearly every stage) lives in shared memory (102 KB).
 //   * hvwt and pmwt live in shared memory (2 x 51 KB), so both Gauss-Seidel
 //     sweeps chase their row-to-row dependency through SMEM; the work that
 //     only needs a site's final weight runs in a parallel pass afterwards.
@@ -42,47 +43,54 @@ constexpr int TS = 160;
 constexpr int TSH = TS / 2;
 constexpr int TS2 = TS * TS;
 constexpr int HALF = TS * TSH;
-constexpr int AMZ_THREADS = 512;
+constexpr int AMZ_THREADS = 640;
 
 constexpr float eps = 1e-5f;
 constexpr float epssq = 1e-10f;
 constexpr float arthresh = 0.75f;
 constexpr float nyqthresh = 0.5f;
 
+// Stencil weights of the reference (:1155-1161).
+__constant__ float gaussodd[4] = {0.14659727707323927f, 0.103592713382435f, 0.0732036125103057f, 0.0365543548389495f};
+__constant__ float gaussgrad[6] = {nyqthresh * 0.07384411893421103f, nyqthresh * 0.06207511968171489f,
+                                   nyqthresh * 0.0521818194747806f,  nyqthresh * 0.03687419286733595f,
+                                   nyqthresh * 0.03099732204057846f, nyqthresh * 0.018413194161458882f};
+__constant__ float gausseven[2] = {0.13719494435797422f, 0.05640252782101291f};
+__constant__ float gquinc[4] = {0.169917f, 0.108947f, 0.069855f, 0.0287182f};
+
 __device__ __forceinline__ float SQR(float x) { return x * x; }
 __device__ __forceinline__ float xmul2f(float x) { return x + x; }
 __device__ __forceinline__ float xdiv2f(float x) { return x * 0.5f; }
 
-constexpr size_t kFull = 7;
+constexpr size_t kFull = 6;
 constexpr size_t kSlabBytes = kFull * TS2 * 4 + 2 * HALF + 256;  // + nyquist, nyquist2 bytes
-constexpr size_t kSmemBytes = 2 * HALF * 4;                       // hvwt + pmwt
+constexpr size_t kSmemBytes = 2 * HALF * 4 + TS2 * 4;            // hvwt + pmwt + cfa
 
-// Lifetime map of the reference's planes onto the slab (F0..F6 full planes;
+// Lifetime map of the reference's planes onto the slab (F0..F5 full planes;
 // "a"/"b" = first/second half of a full plane):
-//   F0 cfa                                   fill .. S10
-//   F1 vcd  (S2..S6)     -> a rbm, b rbp     (S8..S9)
-//   F2 hcd  (S2..S6)     -> a pmwt copy-out unused, b rbint (S9)
-//   F3 vcdalt (S2..S3)   -> a cddiffsq (S3..S5) then Dgrb0 (S6..S10), b rgbgreen@R/B (S6..S10)
-//   F4 hcdalt (S2..S3)   -> a Dgrb2h, b Dgrb2v (S6) -> a Dgrb1 (S9..S10)
-//   F5 dgintv (S2..S5)   -> a delp, b delm (S7..S8)
-//   F6 dginth (S2..S5)   -> a Dgrbsq1p, b Dgrbsq1m (S7..S8)
-//   SMEM: hvwt (S4..S10), pmwt (S8..S9)
+//   F0 vcd  (S2..S6)     -> a rbm, b rbp     (S8..S9)
+//   F1 hcd  (S2..S6)     -> a pmwt copy-out unused, b rbint (S9)
+//   F2 vcdalt (S2..S3)   -> a cddiffsq (S3..S5) then Dgrb0 (S6..S10), b rgbgreen@R/B (S6..S10)
+//   F3 hcdalt (S2..S3)   -> a Dgrb2h, b Dgrb2v (S6) -> a Dgrb1 (S9..S10)
+//   F4 dgintv (S2..S5)   -> a delp, b delm (S7..S8)
+//   F5 dginth (S2..S5)   -> a Dgrbsq1p, b Dgrbsq1m (S7..S8)
+//   SMEM: cfa (fill..S10), hvwt (S4..S10), pmwt (S8..S9)
 struct Slab {
   float *cfa, *vcd, *hcd, *vcdalt, *hcdalt, *dgintv, *dginth;
   float *rbm, *rbp, *rbint, *cddiffsq, *Dgrb0, *rgbg, *Dgrb2h, *Dgrb2v, *Dgrb1, *delp, *delm, *Dq1p, *Dq1m;
   unsigned char *nyquist, *nyquist2;
 };
 
-__device__ Slab make_slab(unsigned char* base) {
+__device__ Slab make_slab(unsigned char* base, float* cfa_smem) {
   Slab s;
   float* F = reinterpret_cast<float*>(base);
-  s.cfa = F;
-  s.vcd = F + 1 * TS2;
-  s.hcd = F + 2 * TS2;
-  s.vcdalt = F + 3 * TS2;
-  s.hcdalt = F + 4 * TS2;
-  s.dgintv = F + 5 * TS2;
-  s.dginth = F + 6 * TS2;
+  s.cfa = cfa_smem;
+  s.vcd = F + 0 * TS2;
+  s.hcd = F + 1 * TS2;
+  s.vcdalt = F + 2 * TS2;
+  s.hcdalt = F + 3 * TS2;
+  s.dgintv = F + 4 * TS2;
+  s.dginth = F + 5 * TS2;
   s.rbm = s.vcd;
   s.rbp = s.vcd + HALF;
   s.rbint = s.hcd + HALF;
@@ -108,6 +116,7 @@ struct AmazeArgs {
   int W, H;
   uint32_t filters;
   unsigned cfarray[2][2];
+  unsigned cfpack;  // cfarray packed 2 bits per site: bit 2*((r&1)*2+(c&1))
   int ex, ey;
   float clip_pt, clip_pt8, scale;
   int n_top, n_left;
@@ -115,13 +124,26 @@ struct AmazeArgs {
   int* tile_counter;
 };
 
-__device__ __forceinline__ unsigned fc_rt(const AmazeArgs& a, int r, int c) { return a.cfarray[r & 1][c & 1]; }
+// (a packed lookup: indexing the parameter's array at run time would copy the
+// whole parameter block to local memory)
+__device__ __forceinline__ unsigned fc_rt(const AmazeArgs& a, int r, int c) {
+  return (a.cfpack >> (2 * (((r & 1) << 1) | (c & 1)))) & 3u;
+}
 
 __device__ __forceinline__ float raw_at(const AmazeArgs& a, int row, int col) {
   size_t i = (size_t)row * a.W + col;
   if (a.cstride == 1) return a.raw[i];
   return a.raw[i * 3 + fc_rt(a, row, col)];
 }
+
+// n / d for 0 <= n < 2^16 by a multiply-high (exact in that range): the
+// per-stage site loops map a flat index to (row, site) every iteration.
+struct FDiv {
+  unsigned m;
+  int d;
+  __device__ explicit FDiv(int d_) : m(d_ > 1 ? 0xFFFFFFFFu / (unsigned)d_ + 1u : 0u), d(d_) {}
+  __device__ __forceinline__ int div(int n) const { return (int)__umulhi((unsigned)n, m) + (d == 1 ? n : 0); }
+};
 
 // The reference's stage-1 planes (:1330-1339), recomputed from cfa.
 __device__ __forceinline__ float dirwts0_at(const float* cfa, int idx) {
@@ -138,16 +160,11 @@ __device__ __forceinline__ float delhvsqsum_at(const float* cfa, int idx) {
   return SQR(delh) + SQR(delv);
 }
 
-// One step of the stage-3 hcd (or, transposed, vcd) chain: `prev` is the
-// already-updated value two sites back, `cur`/`next` the stage-2 values,
-// `*alt` the alternates, `c`, `cm`, `cp` the cfa at the site and its two
-// neighbours along the chain direction.  Returns the updated value.
-__device__ __forceinline__ float s3_step(float prev, float cur, float next, float altp, float altc, float altn,
-                                         float c, float cm, float cp, bool green, float clip_pt) {
-  const float var = 3.f * (SQR(prev) + SQR(cur) + SQR(next)) - SQR(prev + cur + next);
-  const float altvar = 3.f * (SQR(altp) + SQR(altc) + SQR(altn)) - SQR(altp + altc + altn);
-  float h = cur;
-  if (altvar < var) h = altc;
+// Stage 3 (:1375-1398) after the step has chosen h (the stage-2 value or its
+// alternate): the clamp against the site's Gint and its two neighbours along
+// the chain direction.  A pure function of h, so both candidates can be
+// finished before the chain recurrence decides between them.
+__device__ __forceinline__ float s3_finish(float h, float c, float cm, float cp, bool green, float clip_pt) {
   float Gint;
   if (green) {
     Gint = -h + c;
@@ -174,22 +191,21 @@ __device__ __forceinline__ float s3_step(float prev, float cur, float next, floa
   return h;
 }
 
+// Directional variance of three consecutive chain values (:1380-1381).
+__device__ __forceinline__ float s3_var(float a, float b, float c) {
+  return 3.f * (SQR(a) + SQR(b) + SQR(c)) - SQR(a + b + c);
+}
+
 __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
   const int v1 = TS, v2 = 2 * TS, v3 = 3 * TS, p1 = -TS + 1, p2 = -2 * TS + 2, p3 = -3 * TS + 3, m1 = TS + 1,
             m2 = 2 * TS + 2, m3 = 3 * TS + 3;
-  const float gaussodd[4] = {0.14659727707323927f, 0.103592713382435f, 0.0732036125103057f, 0.0365543548389495f};
-  const float gaussgrad[6] = {nyqthresh * 0.07384411893421103f, nyqthresh * 0.06207511968171489f,
-                              nyqthresh * 0.0521818194747806f,  nyqthresh * 0.03687419286733595f,
-                              nyqthresh * 0.03099732204057846f, nyqthresh * 0.018413194161458882f};
-  const float gausseven[2] = {0.13719494435797422f, 0.05640252782101291f};
-  const float gquinc[4] = {0.169917f, 0.108947f, 0.069855f, 0.0287182f};
   extern __shared__ __align__(16) float smem[];
   float* hvwt = smem;         // [HALF]
   float* pmwt = smem + HALF;  // [HALF]
+  float* cfa = smem + 2 * HALF;  // [TS2], read by nearly every stage
   const int tid = threadIdx.x, nth = blockDim.x;
   const int W = A.W, H = A.H;
-  const Slab S = make_slab(A.scratch + (size_t)blockIdx.x * kSlabBytes);
-  float* cfa = S.cfa;
+  const Slab S = make_slab(A.scratch + (size_t)blockIdx.x * kSlabBytes, cfa);
   __shared__ int s_tile;
   __shared__ int s_doNyq;
 
@@ -208,12 +224,13 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     const int ccmin = (left < 0) ? 16 : 0;
     const int rrmax = (bottom > H) ? H - top : rr1;
     const int ccmax = (right > W) ? W - left : cc1;
+    const FDiv fdc(cc1), fd8(cc1 - 8), fd32(cc1 - 32);
 
     // ---- zero what this tile reads before writing (fresh-buffer semantics)
     for (int i = tid; i < 2 * HALF / 16; i += nth)
       reinterpret_cast<float4*>(S.nyquist)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = tid; i < rr1 * cc1; i += nth) {
-      const int rr = i / cc1, cc = i % cc1;
+      const int rr = fdc.div(i), cc = i - rr * cc1;
       if (rr >= 4 && rr < rr1 - 4 && cc >= 4 && cc < cc1 - 4) continue;
       const int idx = rr * TS + cc;
       S.vcd[idx] = 0.f;
@@ -224,7 +241,7 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     if ((rrmin > 0 || rrmax < rr1) && (ccmin > 0 || ccmax < cc1)) {
       // unfilled 16x16 apron corners (:1326)
       for (int i = tid; i < rr1 * cc1; i += nth) {
-        const int rr = i / cc1, cc = i % cc1;
+        const int rr = fdc.div(i), cc = i - rr * cc1;
         const bool rc = (rrmin > 0 && rr < 16) || (rrmax < rr1 && rr >= rrmax);
         const bool cc_ = (ccmin > 0 && cc < 16) || (ccmax < cc1 && cc >= ccmax);
         if (rc && cc_) cfa[rr * TS + cc] = 0.f;
@@ -237,7 +254,7 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     // flat buffer does
     const float scale = A.scale;
     for (int i = tid; i < rr1 * cc1; i += nth) {
-      const int rr = i / cc1, cc = i % cc1;
+      const int rr = fdc.div(i), cc = i - rr * cc1;
       int srow = -1, scol = -1;
       if (rr >= rrmin && rr < rrmax && cc >= ccmin && cc < ccmax) {
         srow = rr + top;
@@ -271,7 +288,7 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
 
     // ---- S2 colour differences (:1341-1373); S1 planes recomputed
     for (int i = tid; i < (rr1 - 8) * (cc1 - 8); i += nth) {
-      const int rr = 4 + i / (cc1 - 8), cc = 4 + i % (cc1 - 8);
+      const int q_ = fd8.div(i), rr = 4 + q_, cc = 4 + i - q_ * (cc1 - 8);
       const int idx = rr * TS + cc;
       const int sgn = (fc_rt(A, rr, cc) & 1) ? -1 : 1;
       const float d0m2 = dirwts0_at(cfa, idx - v2), d00 = dirwts0_at(cfa, idx), d0p2 = dirwts0_at(cfa, idx + v2);
@@ -316,39 +333,82 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     __syncthreads();
 
     // ---- S3 (:1375-1398): hcd chains along rows, vcd chains down columns,
-    // each in the reference's scan order; operands of the next step are
-    // loaded before the dependent arithmetic of the current one
+    // each in the reference's scan order.  Every operand of a step except
+    // the previous (already updated) site is an original value, so each
+    // group of G sites loads its operands together.
     {
-      const int n_h = (rr1 - 8) * 2, n_v = (cc1 - 8) * 2;
+      // transposed cfa in the (not yet used) hvwt/pmwt region, so that the
+      // row chains of a warp read distinct banks; diagonal order keeps both
+      // the reads and the writes of each 32x32 block conflict-free
+      float* cfaT = smem;
+      {
+        const int lane = tid & 31, warp = tid >> 5, nwarp = nth >> 5;
+        const int bx = (cc1 + 31) >> 5, by = (rr1 + 31) >> 5;
+        for (int b = warp; b < bx * by; b += nwarp) {
+          const int r0 = (b / bx) << 5, c0 = (b % bx) << 5;
+          const int r = r0 + lane;
+#pragma unroll 4
+          for (int k = 0; k < 32; k++) {
+            const int c = c0 + ((lane + k) & 31);
+            if (r < rr1 && c < cc1) cfaT[c * TS + r] = cfa[r * TS + c];
+          }
+        }
+      }
+      __syncthreads();
+      const int nlh = rr1 - 8, nlv = cc1 - 8;
+      const int n_h = 2 * nlh, n_v = 2 * nlv;
       for (int item = tid; item < n_h + n_v; item += nth) {
         const bool horiz = item < n_h;
         const int it = horiz ? item : item - n_h;
-        const int line = 4 + it / 2, par = it % 2;
+        const int nl = horiz ? nlh : nlv;
+        // row chains: the two chains of a row on neighbouring lanes (their
+        // sites share cache lines); column chains: grouped by the parity of
+        // line + start, i.e. by CFA colour, so a warp's lanes take the same
+        // branches and read consecutive columns of one row
+        int line, par;
+        if (horiz) {
+          line = 4 + (it >> 1);
+          par = it & 1;
+        } else {
+          const int grp = it >= nl;
+          line = 4 + (grp ? it - nl : it);
+          par = grp ? 1 - (line & 1) : (line & 1);
+        }
         const int stride = horiz ? 2 : v2;      // chain step in the flat tile
-        const int nstride = horiz ? 1 : v1;     // neighbour along the direction
         const int len = horiz ? cc1 : rr1;
         float* d = horiz ? S.hcd : S.vcd;
         const float* alt = horiz ? S.hcdalt : S.vcdalt;
-        int pos = 4 + par;
-        if (pos >= len - 4) continue;
-        int idx = horiz ? line * TS + pos : pos * TS + line;
-        float prev = d[idx - stride], cur = d[idx], altp = alt[idx - stride], altc = alt[idx];
-        float next = d[idx + stride], altn = alt[idx + stride];
-        for (; pos < len - 4; pos += 2, idx += stride) {
-          const float c = cfa[idx], cm = cfa[idx - nstride], cp = cfa[idx + nstride];
-          const int nidx = idx + 2 * stride;
-          const bool more = pos + 2 < len - 4;
-          const float next2 = more ? d[nidx] : 0.f;
-          const float altn2 = more ? alt[nidx] : 0.f;
-          const int rr = horiz ? line : pos, cc = horiz ? pos : line;
-          const float h = s3_step(prev, cur, next, altp, altc, altn, c, cm, cp, (fc_rt(A, rr, cc) & 1) != 0, A.clip_pt);
-          d[idx] = h;
-          prev = h;
-          cur = next;
-          altp = altc;
-          altc = altn;
-          next = next2;
-          altn = altn2;
+        const float* cf = horiz ? cfaT : cfa;   // cf[pos * TS + line] / cf[line + pos * TS]
+        const int pos0 = 4 + par;
+        if (pos0 >= len - 4) continue;
+        const bool green = (fc_rt(A, horiz ? line : pos0, horiz ? pos0 : line) & 1) != 0;
+        const int K = (len - 4 - pos0 + 1) / 2;  // sites pos0, pos0 + 2, ... < len - 4
+        int idx = horiz ? line * TS + pos0 : pos0 * TS + line;
+        int cidx = pos0 * TS + line;  // site in cf (both layouts: position-major)
+        float prev = d[idx - stride], altp = alt[idx - stride];
+        constexpr int G = 8;
+        for (int s0 = 0; s0 < K; s0 += G) {
+          const int g = min(G, K - s0);
+          float dv[G + 1], av[G + 1];
+#pragma unroll
+          for (int k = 0; k <= G; k++) {
+            dv[k] = k <= g ? d[idx + k * stride] : 0.f;
+            av[k] = k <= g ? alt[idx + k * stride] : 0.f;
+          }
+#pragma unroll
+          for (int k = 0; k < G; k++) {
+            if (k < g) {
+              const int ci = cidx + k * v2;
+              const float altvar = s3_var(altp, av[k], av[k + 1]);
+              const float h0 = (altvar < s3_var(prev, dv[k], dv[k + 1])) ? av[k] : dv[k];
+              const float h = s3_finish(h0, cf[ci], cf[ci - TS], cf[ci + TS], green, A.clip_pt);
+              d[idx + k * stride] = h;
+              prev = h;
+              altp = av[k];
+            }
+          }
+          idx += g * stride;
+          cidx += g * v2;
         }
       }
     }
@@ -357,9 +417,10 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     auto rb_count = [&](int a) { return (cc1 - a - a + 1) / 2 + 1; };
     {
       const int per_row = rb_count(4);
+      const FDiv fdr(per_row);
       for (int i = tid; i < (rr1 - 8) * per_row; i += nth) {
-        const int rr = 4 + i / per_row;
-        const int cc = 4 + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        const int q_ = fdr.div(i), rr = 4 + q_;
+        const int cc = 4 + (fc_rt(A, rr, 2) & 1) + 2 * (i - q_ * per_row);
         if (cc >= cc1 - 4) continue;
         const int idx = rr * TS + cc;
         S.cddiffsq[idx >> 1] = SQR(S.vcd[idx] - S.hcd[idx]);
@@ -372,9 +433,10 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     {
       const int a = 6;
       const int per_row = rb_count(a);
+      const FDiv fdr(per_row);
       for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
-        const int rr = a + i / per_row;
-        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        const int q_ = fdr.div(i), rr = a + q_;
+        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i - q_ * per_row);
         if (cc >= cc1 - a) continue;
         const int idx = rr * TS + cc;
         const float* vcd = S.vcd;
@@ -430,9 +492,10 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     if (doNyquist) {
       const int a = 8;
       const int per_row = rb_count(a);
+      const FDiv fdr(per_row);
       for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
-        const int rr = a + i / per_row;
-        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        const int q_ = fdr.div(i), rr = a + q_;
+        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i - q_ * per_row);
         if (cc >= cc1 - a) continue;
         const int idx = rr * TS + cc;
         const unsigned char* nq = S.nyquist;
@@ -442,8 +505,8 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
       }
       __syncthreads();
       for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
-        const int rr = a + i / per_row;
-        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        const int q_ = fdr.div(i), rr = a + q_;
+        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i - q_ * per_row);
         if (cc >= cc1 - a) continue;
         const int idx = rr * TS + cc;
         if (!S.nyquist2[idx >> 1]) continue;
@@ -475,6 +538,7 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     {
       const int a = 8;
       const int per_row = rb_count(a);
+      const FDiv fdr(per_row);
       for (int rr = a; rr < rr1 - a; rr++) {
         for (int k = tid; k < per_row; k += nth) {
           const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * k;
@@ -488,8 +552,8 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
         __syncthreads();
       }
       for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
-        const int rr = a + i / per_row;
-        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        const int q_ = fdr.div(i), rr = a + q_;
+        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i - q_ * per_row);
         if (cc >= cc1 - a) continue;
         const int idx = rr * TS + cc;
         const float hv = hvwt[idx >> 1];
@@ -507,11 +571,12 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     if (doNyquist) {
       const int a = 8;
       const int per_row = rb_count(a);
+      const FDiv fdr(per_row);
       const float* D2h = S.Dgrb2h;
       const float* D2v = S.Dgrb2v;
       for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
-        const int rr = a + i / per_row;
-        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        const int q_ = fdr.div(i), rr = a + q_;
+        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i - q_ * per_row);
         if (cc >= cc1 - a) continue;
         const int idx = rr * TS + cc;
         if (!S.nyquist2[idx >> 1]) continue;
@@ -533,10 +598,12 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     }
 
     // ---- S7 R/B gradients (:1483-1502)
-    for (int i = tid; i < (rr1 - 12) * ((cc1 - 12 + 1) / 2); i += nth) {
-      const int per_row = (cc1 - 12 + 1) / 2;
-      const int rr = 6 + i / per_row;
-      const int cc = 6 + 2 * (i % per_row);
+    const int per7 = (cc1 - 12 + 1) / 2;
+    const FDiv fd7(per7);
+    for (int i = tid; i < (rr1 - 12) * per7; i += nth) {
+      const int q_ = fd7.div(i);
+      const int rr = 6 + q_;
+      const int cc = 6 + 2 * (i - q_ * per7);
       const int idx = rr * TS + cc;
       if ((fc_rt(A, rr, 2) & 1) == 0) {
         S.delp[idx >> 1] = fabsf(cfa[idx + p1] - cfa[idx - p1]);
@@ -556,13 +623,14 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     {
       const int a = 8;
       const int per_row = rb_count(a);
+      const FDiv fdr(per_row);
       const float* delp = S.delp;
       const float* delm = S.delm;
       const float* Dq1m = S.Dq1m;
       const float* Dq1p = S.Dq1p;
       for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
-        const int rr = a + i / per_row;
-        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        const int q_ = fdr.div(i), rr = a + q_;
+        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i - q_ * per_row);
         if (cc >= cc1 - a) continue;
         const int idx = rr * TS + cc, idx1 = idx >> 1;
         const float crse = xmul2f(cfa[idx + m1]) / (eps + cfa[idx] + cfa[idx + m2]);
@@ -618,6 +686,7 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     {
       const int a = 10;
       const int per_row = rb_count(a);
+      const FDiv fdr(per_row);
       for (int rr = a; rr < rr1 - a; rr++) {
         for (int k = tid; k < per_row; k += nth) {
           const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * k;
@@ -631,8 +700,8 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
         __syncthreads();
       }
       for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
-        const int rr = a + i / per_row;
-        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        const int q_ = fdr.div(i), rr = a + q_;
+        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i - q_ * per_row);
         if (cc >= cc1 - a) continue;
         const int idx = rr * TS + cc, idx1 = idx >> 1;
         const float pw = pmwt[idx1];
@@ -656,10 +725,11 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     {
       const int a = 12;
       const int per_row = rb_count(a);
+      const FDiv fdr(per_row);
       const float* rbint = S.rbint;
       for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
-        const int rr = a + i / per_row;
-        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        const int q_ = fdr.div(i), rr = a + q_;
+        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i - q_ * per_row);
         if (cc >= cc1 - a) continue;
         const int idx = rr * TS + cc, idx1 = idx >> 1;
         if (fabsf(0.5f - pmwt[idx1]) >= fabsf(0.5f - hvwt[idx1])) continue;
@@ -721,9 +791,10 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
     {
       const int a = 14;
       const int per_row = rb_count(a);
+      const FDiv fdr(per_row);
       for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
-        const int rr = a + i / per_row;
-        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i % per_row);
+        const int q_ = fdr.div(i), rr = a + q_;
+        const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i - q_ * per_row);
         if (cc >= cc1 - a) continue;
         const int idx = rr * TS + cc;
         const int c = 1 - (int)fc_rt(A, rr, cc) / 2;
@@ -748,7 +819,7 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
 
     // ---- S10 output (:1594-1625)
     for (int i = tid; i < (rr1 - 32) * (cc1 - 32); i += nth) {
-      const int rr = 16 + i / (cc1 - 32), cc = 16 + i % (cc1 - 32);
+      const int q_ = fd32.div(i), rr = 16 + q_, cc = 16 + i - q_ * (cc1 - 32);
       const int row = rr + top, col = cc + left;
       if (row < 0 || row >= H || col < 0 || col >= W) continue;
       const int t = rr * TS + cc;
@@ -772,10 +843,12 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
         r = g - D0[t >> 1];
         b = g - D1[t >> 1];
       }
+      // streaming stores: the output is not re-read by this kernel, so it
+      // should not evict the slab planes from L2
       float* o = A.rgb + ((size_t)row * W + col) * 3;
-      o[0] = fmaxf(0.f, r);
-      o[1] = fmaxf(0.f, g);
-      o[2] = fmaxf(0.f, b);
+      __stcs(o + 0, fmaxf(0.f, r));
+      __stcs(o + 1, fmaxf(0.f, g));
+      __stcs(o + 2, fmaxf(0.f, b));
     }
     __syncthreads();
   }
@@ -842,6 +915,9 @@ lre_status launch_amaze(Context* c, const float* raw, int cstride, float* rgb, s
   A.clip_pt8 = 0.8f / initialGain;
   for (int r = 0; r < 2; r++)
     for (int q = 0; q < 2; q++) A.cfarray[r][q] = fcol3((unsigned)r, (unsigned)q, filters);
+  A.cfpack = 0;
+  for (int r = 0; r < 2; r++)
+    for (int q = 0; q < 2; q++) A.cfpack |= A.cfarray[r][q] << (2 * (r * 2 + q));
   if (A.cfarray[0][0] == 1) {
     if (A.cfarray[0][1] == 0) { A.ey = 0; A.ex = 1; } else { A.ey = 1; A.ex = 0; }
   } else {

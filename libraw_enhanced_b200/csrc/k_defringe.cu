@@ -109,18 +109,32 @@ struct BlurJob {
 
 constexpr int BT = 32;  // output tile edge
 
-__device__ __forceinline__ float blur_src(const BlurJob& j, int p, const DfScalars* sc, int x, int y, int W) {
+// Element p of a small parameter array through constant indices only: a
+// run-time index into a kernel parameter would copy the whole parameter block
+// to local memory.
+template <typename T>
+__device__ __forceinline__ T pick5(const T (&a)[5], int p) {
+  switch (p) {
+    case 0: return a[0];
+    case 1: return a[1];
+    case 2: return a[2];
+    case 3: return a[3];
+    default: return a[4];
+  }
+}
+
+__device__ __forceinline__ float blur_src(const float* in, int mode, const DfScalars* sc, int x, int y, int W) {
   size_t i = (size_t)y * W + x;
-  switch (j.mode[p]) {
+  switch (mode) {
     case BS_GUIDE_LINEAR:
-      return smax(j.in[p][i * 3 + 1], 0.f);
+      return smax(in[i * 3 + 1], 0.f);
     case BS_PLANE_EDGE_NORM: {
       float f = smax(sc->max_edge, 1e-6f);
       float inv = 1.f / f;
-      return j.in[p][i] * inv;
+      return in[i] * inv;
     }
     default:
-      return j.in[p][i];
+      return in[i];
   }
 }
 
@@ -134,10 +148,12 @@ __global__ void __launch_bounds__(256) k_df_blur(BlurJob job, GaussTaps taps, in
   float* s_in = sm;                       // [np][E][E]
   float* s_h = sm + (size_t)job.np * E * E;  // [np][E][BT]
   for (int p = 0; p < job.np; p++) {
+    const float* in = pick5(job.in, p);
+    const int mode = pick5(job.mode, p);
     for (int i = threadIdx.x; i < E * E; i += blockDim.x) {
       int gy = min(max(y0 - ks + i / E, 0), H - 1);
       int gx = min(max(x0 - ks + i % E, 0), W - 1);
-      s_in[(size_t)p * E * E + i] = blur_src(job, p, sc, gx, gy, W);
+      s_in[(size_t)p * E * E + i] = blur_src(in, mode, sc, gx, gy, W);
     }
   }
   __syncthreads();
@@ -157,13 +173,14 @@ __global__ void __launch_bounds__(256) k_df_blur(BlurJob job, GaussTaps taps, in
   // vertical pass
   for (int p = 0; p < job.np; p++) {
     const float* sh = s_h + (size_t)p * E * BT;
+    float* out = pick5(job.out, p);
     for (int i = threadIdx.x; i < BT * BT; i += blockDim.x) {
       int j = i / BT, k = i % BT;
       int gy = y0 + j, gx = x0 + k;
       if (gx >= W || gy >= H) continue;
       float acc = 0.f;
       for (int t = 0; t <= 2 * ks; t++) acc += taps.w[t] * sh[(j + t) * BT + k];
-      job.out[p][(size_t)gy * W + gx] = acc;
+      out[(size_t)gy * W + gx] = acc;
     }
   }
 }
@@ -183,11 +200,14 @@ __global__ void __launch_bounds__(256) k_df_blur_fast(BlurJob job, GaussTaps tap
 #pragma unroll
   for (int t = 0; t <= 2 * KS; t++) w[t] = taps.w[t];
   for (int p = 0; p < job.np; p++) {
+    const float* in = pick5(job.in, p);
+    const int mode = pick5(job.mode, p);
+    float* out = pick5(job.out, p);
     for (int i = threadIdx.x; i < E * E; i += blockDim.x) {
       const int r = i / E, q = i % E;
       const int gy = min(max(y0 - KS + r, 0), H - 1);
       const int gx = min(max(x0 - KS + q, 0), W - 1);
-      s_in[r * LD + q] = blur_src(job, p, sc, gx, gy, W);
+      s_in[r * LD + q] = blur_src(in, mode, sc, gx, gy, W);
     }
     __syncthreads();
     // horizontal: item = (halo row j, group of 8 output columns)
@@ -218,7 +238,7 @@ __global__ void __launch_bounds__(256) k_df_blur_fast(BlurJob job, GaussTaps tap
 #pragma unroll
         for (int t = 0; t <= 2 * KS; t++) acc += w[t] * x[o + t];
         const int gy = y0 + j0 + o;
-        if (gx < W && gy < H) job.out[p][(size_t)gy * W + gx] = acc;
+        if (gx < W && gy < H) out[(size_t)gy * W + gx] = acc;
       }
     }
     __syncthreads();
