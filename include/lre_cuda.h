@@ -249,6 +249,97 @@ lre_status lre_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t widt
 lre_status lre_dev_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t width,
                            size_t height, const lre_develop_params* params);
 
+/* ---------------------------------------------------------------- tuning */
+/* Kernel-shape choices that never change results, only speed. */
+typedef struct lre_tuning {
+  int lanes;         /* batch/server: concurrent per-image pipelines (streams) */
+  int axial_tile;    /* guided-filter output tile edge: 32 or 16             */
+  int axial_threads; /* guided-filter CTA size: 512 or 256                    */
+  int blur_tile;     /* defringe blur output tile edge: 32 or 64              */
+} lre_tuning;
+lre_status lre_set_tuning(lre_ctx* ctx, const lre_tuning* t);
+lre_status lre_get_tuning(const lre_ctx* ctx, lre_tuning* t);
+
+/* ------------------------------------------------------- batched develop */
+/* Not in the reference (which develops one image per call): many images of
+ * uneven sizes, CFA layouts and option sets in one call.  Images are spread
+ * over `lanes` pipelines, each with its own stream and device buffers, so
+ * the upload of one image and the download of another overlap the kernels
+ * of a third; with use_graph the whole batch is captured once as one CUDA
+ * graph and replayed while later calls repeat the same batch signature
+ * (same pointers, sizes and parameters). */
+typedef struct lre_image {
+  const float* mosaic;        /* dense float32 CFA mosaic, width*height        */
+  void* out;                  /* RGB out: float32 or uint16 per params.output_bits */
+  size_t width, height;
+  lre_develop_params params;  /* per image: CFA, WB, stages, output format     */
+} lre_image;
+
+typedef struct lre_batch_config {
+  int device;
+  int lanes;     /* 0: 3, or the autotuned value                              */
+  int use_graph; /* 1: capture / replay the batch as one CUDA graph            */
+  int autotune;  /* 1: time the kernel-shape choices on the first batch       */
+} lre_batch_config;
+
+typedef struct lre_batch_stats {
+  double ms;             /* host wall time of the call                        */
+  int graph;             /* 0 eager, 1 captured and launched, 2 replayed       */
+  int lanes;
+  uint64_t launches;     /* kernels enqueued by this call (a replay counts the graph's) */
+  double tune_ms;        /* time spent autotuning in this call (0 after the first) */
+} lre_batch_stats;
+
+typedef struct lre_batch lre_batch;
+lre_status lre_batch_create(const lre_batch_config* cfg, lre_batch** out);
+void lre_batch_destroy(lre_batch* b);
+const char* lre_batch_last_error(const lre_batch* b);
+/* Host buffers in and out; synchronous.  Pageable buffers are page-locked
+ * for the duration of the call (pass lre_host_alloc memory to avoid that);
+ * a call with any pageable buffer runs without a graph. */
+lre_status lre_batch_run(lre_batch* b, const lre_image* images, size_t n, lre_batch_stats* stats);
+/* Device buffers in and out; synchronous. */
+lre_status lre_dev_batch_run(lre_batch* b, const lre_image* images, size_t n, lre_batch_stats* stats);
+lre_status lre_batch_get_tuning(const lre_batch* b, lre_tuning* t);
+lre_status lre_batch_set_tuning(lre_batch* b, const lre_tuning* t);
+
+/* ------------------------------------------------------- request server */
+/* Not in the reference: a develop service with continuous batching.
+ * Requests (host buffers, any size and option set) are queued on submit and
+ * admitted onto a free lane as soon as one is idle and the device-memory
+ * budget covers the request's buffers; mosaic, intermediates and result
+ * stay on the device until the result is copied back.  Requests on
+ * different lanes run concurrently on the GPU.  A request's result does not
+ * depend on what else is in flight. */
+typedef struct lre_server_config {
+  int device;
+  int lanes;                  /* concurrent requests on the device (0: 4)     */
+  size_t device_budget_bytes; /* admission limit on resident buffers (0: 150 GB) */
+} lre_server_config;
+
+typedef struct lre_request_stats {
+  lre_status status;
+  int lane;
+  double queue_ms;  /* submit -> admitted                                     */
+  double run_ms;    /* admitted -> result in host memory                      */
+  double total_ms;  /* submit -> result in host memory                        */
+  size_t device_bytes;
+} lre_request_stats;
+
+typedef struct lre_server lre_server;
+lre_status lre_server_create(const lre_server_config* cfg, lre_server** out);
+/* Stops admitting, finishes every queued request, frees the device. */
+void lre_server_destroy(lre_server* s);
+const char* lre_server_last_error(const lre_server* s);
+/* Queue a request; the image's buffers must stay valid until it completes.
+ * Returns LRE_ERR_BUSY when the request alone exceeds the budget. */
+lre_status lre_server_submit(lre_server* s, const lre_image* img, uint64_t* ticket);
+/* Block until the request completes (timeout_ms < 0: no limit); LRE_ERR_TIMEOUT
+ * if it has not completed in time.  The ticket is released on completion. */
+lre_status lre_server_wait(lre_server* s, uint64_t ticket, double timeout_ms, lre_request_stats* stats);
+/* Device bytes currently held by admitted requests, and the peak so far. */
+lre_status lre_server_memory(const lre_server* s, size_t* in_use, size_t* peak);
+
 #ifdef __cplusplus
 }
 #endif

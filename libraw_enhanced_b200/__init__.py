@@ -15,6 +15,11 @@ develop hot path:
   with their argument names, defaults and shape errors.
 * :func:`develop` -- the plain per-image develop of a CFA mosaic
   (core/libraw_wrapper.cpp:1477-1853 stage order) through ``lre_develop``.
+* :class:`Batch` -- many images of uneven sizes and option sets per call,
+  pipelined over several streams (optionally one CUDA graph per batch) with
+  autotuned kernel shapes.
+* :class:`Server` -- a develop request server with continuous batching under
+  a device-memory budget, reporting per-request latency.
 
 Everything runs on the GPU; there is no CPU fallback.
 """
@@ -39,6 +44,9 @@ __all__ = [
     "tone_mapping",
     "enhance_micro_contrast",
     "default_accelerator",
+    "Batch",
+    "Server",
+    "develop_params",
 ]
 
 # LibRaw `filters` words of the four Bayer layouts.
@@ -308,6 +316,160 @@ class CudaAccelerator:
 
     def dev_develop(self, mosaic, out, width, height, params: DevelopParams):
         self._check(self._lib.lre_dev_develop(self._h, _dptr(mosaic), _dptr(out), int(width), int(height), C.byref(params)))
+
+    # ------------------------------------------------------------ tuning
+    def set_tuning(self, axial_tile=32, axial_threads=512, blur_tile=32) -> None:
+        t = _lib.Tuning(1, int(axial_tile), int(axial_threads), int(blur_tile))
+        self._check(self._lib.lre_set_tuning(self._h, C.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = _lib.Tuning()
+        self._check(self._lib.lre_get_tuning(self._h, C.byref(t)))
+        return {"axial_tile": t.axial_tile, "axial_threads": t.axial_threads, "blur_tile": t.blur_tile}
+
+
+def _out_for(h, w, params):
+    return np.empty((h, w, 3), np.float32 if params.output_bits == 32 else np.uint16)
+
+
+class Batch:
+    """Develop many images per call (``lre_batch_run``).
+
+    ``lanes`` concurrent per-image pipelines (0: autotuned or 3), ``use_graph``
+    captures the batch as one CUDA graph (replayed while the batch repeats),
+    ``autotune`` times the kernel-shape choices on the first batch.
+    """
+
+    def __init__(self, device: int = 0, lanes: int = 0, use_graph: bool = True, autotune: bool = True):
+        self._lib = _lib.load()
+        cfg = _lib.BatchConfig(int(device), int(lanes), int(bool(use_graph)), int(bool(autotune)))
+        h = C.c_void_p()
+        st = self._lib.lre_batch_create(C.byref(cfg), C.byref(h))
+        if st != _lib.LRE_OK:
+            raise LibRawError(st, "lre_batch_create failed")
+        self._h = h
+        self.last_stats = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.lre_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != _lib.LRE_OK:
+            msg = self._lib.lre_batch_last_error(self._h)
+            raise LibRawError(st, msg.decode() if msg else "")
+
+    @staticmethod
+    def _images(items, dev):
+        arr = (_lib.Image * len(items))()
+        for i, (m, o, w, h, p) in enumerate(items):
+            arr[i].mosaic = (_dptr(m) if dev else _ptr(m)).value
+            arr[i].out = (_dptr(o) if dev else _ptr(o)).value
+            arr[i].width, arr[i].height = int(w), int(h)
+            arr[i].params = p
+        return arr
+
+    def run(self, mosaics, params, outs=None):
+        """Host numpy mosaics (H, W) float32 -> list of RGB outputs.
+
+        ``params`` is one DevelopParams or a list (one per image)."""
+        ps = params if isinstance(params, (list, tuple)) else [params] * len(mosaics)
+        ms = [np.ascontiguousarray(m, dtype=np.float32) for m in mosaics]
+        if outs is None:
+            outs = [_out_for(m.shape[0], m.shape[1], p) for m, p in zip(ms, ps)]
+        items = [(m, o, m.shape[1], m.shape[0], p) for m, o, p in zip(ms, outs, ps)]
+        arr = self._images(items, False)
+        stats = _lib.BatchStats()
+        self._check(self._lib.lre_batch_run(self._h, arr, len(items), C.byref(stats)))
+        self.last_stats = stats
+        return outs
+
+    def dev_run(self, mosaics, outs, params):
+        """CUDA tensors in and out (synchronous)."""
+        ps = params if isinstance(params, (list, tuple)) else [params] * len(mosaics)
+        items = [(m, o, m.shape[1], m.shape[0], p) for m, o, p in zip(mosaics, outs, ps)]
+        arr = self._images(items, True)
+        stats = _lib.BatchStats()
+        self._check(self._lib.lre_dev_batch_run(self._h, arr, len(items), C.byref(stats)))
+        self.last_stats = stats
+        return outs
+
+    def get_tuning(self) -> dict:
+        t = _lib.Tuning()
+        self._check(self._lib.lre_batch_get_tuning(self._h, C.byref(t)))
+        return {"lanes": t.lanes, "axial_tile": t.axial_tile, "axial_threads": t.axial_threads, "blur_tile": t.blur_tile}
+
+    def set_tuning(self, lanes=3, axial_tile=32, axial_threads=512, blur_tile=32) -> None:
+        t = _lib.Tuning(int(lanes), int(axial_tile), int(axial_threads), int(blur_tile))
+        self._check(self._lib.lre_batch_set_tuning(self._h, C.byref(t)))
+
+
+class Server:
+    """Develop request server (``lre_server_*``): continuous batching under a
+    device-memory budget.  ``submit`` queues a request and returns a ticket;
+    ``wait`` returns the result and its latency record."""
+
+    def __init__(self, device: int = 0, lanes: int = 4, budget_bytes: int = 150 * 10**9):
+        self._lib = _lib.load()
+        cfg = _lib.ServerConfig(int(device), int(lanes), int(budget_bytes))
+        h = C.c_void_p()
+        st = self._lib.lre_server_create(C.byref(cfg), C.byref(h))
+        if st != _lib.LRE_OK:
+            raise LibRawError(st, "lre_server_create failed")
+        self._h = h
+        self._live = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.lre_server_destroy(self._h)
+            self._h = None
+            self._live.clear()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != _lib.LRE_OK:
+            msg = self._lib.lre_server_last_error(self._h)
+            raise LibRawError(st, msg.decode() if msg else "")
+
+    def submit(self, mosaic, params: DevelopParams, out=None) -> int:
+        m = np.ascontiguousarray(mosaic, dtype=np.float32)
+        if m.ndim != 2:
+            raise ValueError("submit: mosaic must be a dense (H, W) float32 CFA image")
+        h, w = m.shape
+        if out is None:
+            out = _out_for(h, w, params)
+        img = _lib.Image(m.ctypes.data, out.ctypes.data, w, h, params)
+        t = C.c_uint64()
+        self._check(self._lib.lre_server_submit(self._h, C.byref(img), C.byref(t)))
+        self._live[t.value] = (m, out)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: float = -1.0):
+        st = _lib.RequestStats()
+        r = self._lib.lre_server_wait(self._h, int(ticket), float(timeout_ms), C.byref(st))
+        if r == 5:  # LRE_ERR_TIMEOUT: still running
+            raise TimeoutError(f"request {ticket} not complete after {timeout_ms} ms")
+        m, out = self._live.pop(int(ticket), (None, None))
+        self._check(r)
+        return out, {"queue_ms": st.queue_ms, "run_ms": st.run_ms, "total_ms": st.total_ms, "lane": st.lane,
+                     "device_bytes": st.device_bytes}
+
+    def memory(self):
+        a, b = C.c_size_t(), C.c_size_t()
+        self._check(self._lib.lre_server_memory(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
 
 def develop_params(**kw) -> DevelopParams:

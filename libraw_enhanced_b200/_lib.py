@@ -67,6 +67,49 @@ class DevelopParams(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("lanes", C.c_int), ("axial_tile", C.c_int), ("axial_threads", C.c_int), ("blur_tile", C.c_int)]
+
+
+class Image(C.Structure):
+    _fields_ = [
+        ("mosaic", C.c_void_p),
+        ("out", C.c_void_p),
+        ("width", C.c_size_t),
+        ("height", C.c_size_t),
+        ("params", DevelopParams),
+    ]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("lanes", C.c_int), ("use_graph", C.c_int), ("autotune", C.c_int)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [
+        ("ms", C.c_double),
+        ("graph", C.c_int),
+        ("lanes", C.c_int),
+        ("launches", C.c_uint64),
+        ("tune_ms", C.c_double),
+    ]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("lanes", C.c_int), ("device_budget_bytes", C.c_size_t)]
+
+
+class RequestStats(C.Structure):
+    _fields_ = [
+        ("status", C.c_int),
+        ("lane", C.c_int),
+        ("queue_ms", C.c_double),
+        ("run_ms", C.c_double),
+        ("total_ms", C.c_double),
+        ("device_bytes", C.c_size_t),
+    ]
+
+
 _p = C.c_void_p
 _sz = C.c_size_t
 _f = C.c_float
@@ -117,6 +160,21 @@ SIGNATURES = {
     "lre_develop_params_default": (None, [C.POINTER(DevelopParams)]),
     "lre_develop": (_st, [_p, _p, _p, _sz, _sz, C.POINTER(DevelopParams)]),
     "lre_dev_develop": (_st, [_p, _p, _p, _sz, _sz, C.POINTER(DevelopParams)]),
+    "lre_set_tuning": (_st, [_p, C.POINTER(Tuning)]),
+    "lre_get_tuning": (_st, [_p, C.POINTER(Tuning)]),
+    "lre_batch_create": (_st, [C.POINTER(BatchConfig), C.POINTER(_p)]),
+    "lre_batch_destroy": (None, [_p]),
+    "lre_batch_last_error": (C.c_char_p, [_p]),
+    "lre_batch_run": (_st, [_p, C.POINTER(Image), _sz, C.POINTER(BatchStats)]),
+    "lre_dev_batch_run": (_st, [_p, C.POINTER(Image), _sz, C.POINTER(BatchStats)]),
+    "lre_batch_get_tuning": (_st, [_p, C.POINTER(Tuning)]),
+    "lre_batch_set_tuning": (_st, [_p, C.POINTER(Tuning)]),
+    "lre_server_create": (_st, [C.POINTER(ServerConfig), C.POINTER(_p)]),
+    "lre_server_destroy": (None, [_p]),
+    "lre_server_last_error": (C.c_char_p, [_p]),
+    "lre_server_submit": (_st, [_p, C.POINTER(Image), C.POINTER(C.c_uint64)]),
+    "lre_server_wait": (_st, [_p, C.c_uint64, C.c_double, C.POINTER(RequestStats)]),
+    "lre_server_memory": (_st, [_p, C.POINTER(_sz), C.POINTER(_sz)]),
 }
 
 _lib = None

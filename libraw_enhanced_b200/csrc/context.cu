@@ -30,6 +30,12 @@ cudaError_t Workspace::reserve(size_t bytes, cudaStream_t s) {
   return cudaSuccess;
 }
 
+void Workspace::release() {
+  if (base_) cudaFree(base_);
+  base_ = nullptr;
+  cap_ = used_ = 0;
+}
+
 void* Workspace::take(size_t bytes) {
   bytes = (bytes + 255) & ~size_t(255);
   if (used_ + bytes > cap_) return nullptr;

@@ -30,8 +30,6 @@ namespace lre {
 
 namespace {
 
-constexpr int AX_THREADS = 512;
-
 struct AxGeom {
   int T, r, IN, AB;
   size_t off_g, off_r, off_b, off_h0, off_h1, off_mi, off_vi, off_ar, off_br, off_ab, off_bb, off_er, bytes;
@@ -128,8 +126,8 @@ __device__ __forceinline__ int win_count(int p, int r, int n) {
   return hi - lo + 1;
 }
 
-template <int T>
-__global__ void __launch_bounds__(AX_THREADS, 1)
+template <int T, int NT>
+__global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1)
     k_axial_fused(const float* __restrict__ src, float* __restrict__ dst, int W, int H, int r, float eps,
                   float strength, const float* __restrict__ d_maxg) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -291,7 +289,7 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
   // 5. second box level and blend.  Each thread owns PER vertically adjacent
   // output pixels of one column (its window sums slide down by one row per
   // pixel); the three sweeps (R, B, edge) keep their results in registers.
-  constexpr int PER = (T * T + AX_THREADS - 1) / AX_THREADS;
+  constexpr int PER = (T * T + NT - 1) / NT;
   const int my_k = threadIdx.x % T;
   const int my_j0 = (threadIdx.x / T) * PER;
   const bool my_active = my_j0 < T;
@@ -360,7 +358,31 @@ __global__ void __launch_bounds__(AX_THREADS, 1)
   }
 }
 
-int pick_tile(int r) { return r <= 8 ? 32 : 16; }
+// Output tile edge: 32 (the default) or 16; radii above 8 need the smaller
+// tile to fit shared memory.
+int pick_tile(int r, int want) { return r > 8 ? 16 : (want == 16 ? 16 : 32); }
+
+template <int T, int NT>
+cudaError_t axial_launch(dim3 grid, size_t smem, cudaStream_t s, const float* src, float* out, int w, int h, int r,
+                         float eps, float strength, const float* d_max) {
+  cudaError_t e = cudaFuncSetAttribute(k_axial_fused<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_axial_fused<T, NT><<<grid, NT, smem, s>>>(src, out, w, h, r, eps, strength, d_max);
+  return cudaPeekAtLastError();
+}
+
+// Kernel variants: tile 32 or 16, 256 or 512 threads per CTA.
+cudaError_t axial_dispatch(int T, int NT, size_t w, size_t h, cudaStream_t s, const float* src, float* out, int r,
+                           float eps, float strength, const float* d_max) {
+  const AxGeom g = ax_geom(T, r);
+  dim3 grid((unsigned)((w + T - 1) / T), (unsigned)((h + T - 1) / T));
+  if (T == 32) {
+    if (NT == 256) return axial_launch<32, 256>(grid, g.bytes, s, src, out, (int)w, (int)h, r, eps, strength, d_max);
+    return axial_launch<32, 512>(grid, g.bytes, s, src, out, (int)w, (int)h, r, eps, strength, d_max);
+  }
+  if (NT == 512) return axial_launch<16, 512>(grid, g.bytes, s, src, out, (int)w, (int)h, r, eps, strength, d_max);
+  return axial_launch<16, 256>(grid, g.bytes, s, src, out, (int)w, (int)h, r, eps, strength, d_max);
+}
 
 }  // namespace
 
@@ -376,8 +398,7 @@ lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, si
   if (radius < 1) radius = 1;
   if (radius > 16) return fail(c, LRE_ERR_INVALID_ARGUMENT, "ca_axial_cleanup: radius > 16 is not supported");
   strength = fminf(fmaxf(strength, 0.f), 1.f);
-  int T = pick_tile(radius);
-  AxGeom g = ax_geom(T, radius);
+  const int T = pick_tile(radius, c->tune.axial_tile);
   const float* src = in;
   if (in == out) {
     float* tmp = reinterpret_cast<float*>(c->ws.take(w * h * 3 * sizeof(float)));
@@ -385,14 +406,7 @@ lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, si
     LRE_CUDA_TRY(c, cudaMemcpyAsync(tmp, in, w * h * 3 * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
     src = tmp;
   }
-  dim3 grid((unsigned)((w + T - 1) / T), (unsigned)((h + T - 1) / T));
-  if (T == 32) {
-    LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_axial_fused<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.bytes));
-    k_axial_fused<32><<<grid, AX_THREADS, g.bytes, c->stream>>>(src, out, (int)w, (int)h, radius, eps, strength, d_max_g);
-  } else {
-    LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_axial_fused<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.bytes));
-    k_axial_fused<16><<<grid, AX_THREADS, g.bytes, c->stream>>>(src, out, (int)w, (int)h, radius, eps, strength, d_max_g);
-  }
+  LRE_CUDA_TRY(c, axial_dispatch(T, c->tune.axial_threads, w, h, c->stream, src, out, radius, eps, strength, d_max_g));
   count_launch(c);
   return check_launch(c, "ca_axial_cleanup");
 }
@@ -472,17 +486,7 @@ extern "C" lre_status lre_dev_ca_axial_cleanup_noalloc(const float* in, float* o
     if (cudaMemcpyAsync(staging, in, n * 3 * sizeof(float), cudaMemcpyDeviceToDevice, s) != cudaSuccess) return LRE_ERR_CUDA;
     src = staging;
   }
-  const int T = pick_tile(radius);
-  const AxGeom g = ax_geom(T, radius);
-  dim3 grid((unsigned)((w + T - 1) / T), (unsigned)((h + T - 1) / T));
-  if (T == 32) {
-    if (cudaFuncSetAttribute(k_axial_fused<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.bytes) != cudaSuccess)
-      return LRE_ERR_CUDA;
-    k_axial_fused<32><<<grid, AX_THREADS, g.bytes, s>>>(src, out, (int)w, (int)h, radius, epsilon, strength, d_max);
-  } else {
-    if (cudaFuncSetAttribute(k_axial_fused<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.bytes) != cudaSuccess)
-      return LRE_ERR_CUDA;
-    k_axial_fused<16><<<grid, AX_THREADS, g.bytes, s>>>(src, out, (int)w, (int)h, radius, epsilon, strength, d_max);
-  }
+  if (axial_dispatch(pick_tile(radius, 32), 512, w, h, s, src, out, radius, epsilon, strength, d_max) != cudaSuccess)
+    return LRE_ERR_CUDA;
   return cudaGetLastError() == cudaSuccess ? LRE_OK : LRE_ERR_CUDA;
 }

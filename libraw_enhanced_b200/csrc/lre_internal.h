@@ -26,6 +26,8 @@ class Workspace {
   // reserve() from the plan of the stage they run.
   void* take(size_t bytes);
   void reset() { used_ = 0; }
+  // Frees the arena (the caller has synchronised every stream using it).
+  void release();
   void rewind(size_t mark) { used_ = mark; }
   size_t capacity() const { return cap_; }
   size_t used() const { return used_; }
@@ -47,8 +49,17 @@ struct WsPlan {
   }
 };
 
+// Kernel-shape choices that do not change results (picked by the batch
+// autotuner, or set with lre_set_tuning).
+struct Tuning {
+  int axial_tile = 32;      // guided-filter output tile edge: 32 or 16
+  int axial_threads = 512;  // guided-filter CTA size: 512 or 256
+  int blur_tile = 32;       // defringe register-tiled blur output tile edge: 32 or 64
+};
+
 struct Context {
   int device = 0;
+  Tuning tune;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   Workspace ws;
@@ -135,4 +146,13 @@ size_t ws_bytes_lateral(size_t w, size_t h, int cell, int levels, bool in_place)
 size_t ws_bytes_amaze(size_t w, size_t h);
 size_t ws_bytes_xtrans(size_t w, size_t h, int passes);
 
+}  // namespace lre
+
+namespace lre {
+// The per-image develop chain (pipeline.cu), shared by the plain entry
+// points, the batch runner and the request server.
+lre_status develop_validate(Context* c, const lre_develop_params* p, size_t w, size_t h);
+size_t develop_ws_bytes(const lre_develop_params& p, size_t w, size_t h);
+lre_status develop_device(Context* c, const float* mosaic, void* out, size_t w, size_t h,
+                          const lre_develop_params& p);
 }  // namespace lre

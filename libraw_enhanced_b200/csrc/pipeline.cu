@@ -109,6 +109,38 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
 
 }  // namespace
 
+namespace lre {
+
+lre_status develop_validate(Context* c, const lre_develop_params* p, size_t w, size_t h) { return validate(c, p, w, h); }
+
+size_t develop_ws_bytes(const lre_develop_params& p, size_t w, size_t h) {
+  const size_t rgb_bytes = align256(w * h * 12);
+  return (p.output_bits == 32 ? 1 : 2) * rgb_bytes + stage_ws(p, w, h) + 4096;
+}
+
+// The whole chain on device buffers, enqueued on c->stream (validated
+// parameters).  Float output doubles as the first RGB buffer.
+lre_status develop_device(Context* c, const float* mosaic, void* out, size_t w, size_t h,
+                          const lre_develop_params& p) {
+  const size_t rgb_bytes = align256(w * h * 12);
+  const bool float_out = p.output_bits == 32;
+  c->ws.reset();
+  LRE_CUDA_TRY(c, c->ws.reserve(develop_ws_bytes(p, w, h), c->stream));
+  float* rgb_a = float_out ? reinterpret_cast<float*>(out) : reinterpret_cast<float*>(c->ws.take(rgb_bytes));
+  float* rgb_b = reinterpret_cast<float*>(c->ws.take(rgb_bytes));
+  if (!rgb_a || !rgb_b) return fail(c, LRE_ERR_OUT_OF_MEMORY, "develop: workspace too small");
+  float* res = nullptr;
+  LRE_TRY(run_chain(c, mosaic, rgb_a, rgb_b, w, h, p, &res));
+  if (float_out) {
+    if (res != out) LRE_CUDA_TRY(c, cudaMemcpyAsync(out, res, w * h * 12, cudaMemcpyDeviceToDevice, c->stream));
+  } else {
+    LRE_TRY(launch_quantize_u16(c, res, reinterpret_cast<uint16_t*>(out), w * h * 3));
+  }
+  return LRE_OK;
+}
+
+}  // namespace lre
+
 extern "C" {
 
 void lre_develop_params_default(lre_develop_params* p) {
@@ -150,22 +182,7 @@ lre_status lre_dev_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t 
   LRE_TRY(validate(c, params, w, h));
   cudaSetDevice(c->device);
   LRE_TRY(lre::check_injection(c));
-  const lre_develop_params& p = *params;
-  const size_t rgb_bytes = align256(w * h * 12);
-  const bool float_out = p.output_bits == 32;
-  c->ws.reset();
-  LRE_CUDA_TRY(c, c->ws.reserve((float_out ? 1 : 2) * rgb_bytes + stage_ws(p, w, h), c->stream));
-  float* rgb_a = float_out ? reinterpret_cast<float*>(out) : reinterpret_cast<float*>(c->ws.take(rgb_bytes));
-  float* rgb_b = reinterpret_cast<float*>(c->ws.take(rgb_bytes));
-  if (!rgb_a || !rgb_b) return lre::fail(c, LRE_ERR_OUT_OF_MEMORY, "develop: workspace too small");
-  float* res = nullptr;
-  LRE_TRY(run_chain(c, mosaic, rgb_a, rgb_b, w, h, p, &res));
-  if (float_out) {
-    if (res != out) LRE_CUDA_TRY(c, cudaMemcpyAsync(out, res, w * h * 12, cudaMemcpyDeviceToDevice, c->stream));
-  } else {
-    LRE_TRY(lre::launch_quantize_u16(c, res, reinterpret_cast<uint16_t*>(out), w * h * 3));
-  }
-  return LRE_OK;
+  return lre::develop_device(c, mosaic, out, w, h, *params);
 }
 
 lre_status lre_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t w, size_t h,
