@@ -403,6 +403,10 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }
+        if world == 1 and not args.no_batch:
+            line["batched"] = run_batched(args, acc)
+        if world == 1 and not args.no_serve:
+            line["served"] = run_served(args)
         if not args.no_cpu_baseline and world == 1:
             try:
                 line["cpu_baseline"] = cpu_baseline()
@@ -439,6 +443,203 @@ def run_e2e(acc, mosaic, params, args, world, mp):
     return world * mp / (e_ms / 1e3), e_ms
 
 
+def _pinned(shape, dtype):
+    """A numpy view of page-locked host memory (torch's pinned allocator)."""
+    import numpy as np
+    import torch
+
+    n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+    return torch.empty(n, dtype=torch.uint8).pin_memory().numpy().view(dtype).reshape(shape)
+
+
+def run_batched(args, acc):
+    """The 32-image batched develop: sizes {4032x3024, 6000x4000, 8256x5504,
+    9504x6336}, CFAs and WB drawn by seed, AMaZE -> defringe -> axial CA,
+    16-bit output.  Host f32 mosaics in, host u16 RGB out (page-locked),
+    through lre_batch_run (lanes, one CUDA graph per batch, autotuned kernel
+    shapes); the plain path develops the same 32 images one lre_develop call
+    at a time for the comparison."""
+    import numpy as np
+    import torch
+
+    import libraw_enhanced_b200 as lre
+    from libraw_enhanced_b200 import scenes
+
+    specs = scenes.batch_specs(32, 100)
+    mos, outs, params = [], [], []
+    for seed, h, w, cfa, wb in specs:
+        d = scenes.mosaic_upscaled_torch(seed, h, w, cfa, wb)
+        hm = _pinned((h, w), np.float32)
+        torch.from_numpy(hm).copy_(d.cpu())
+        del d
+        mos.append(hm)
+        outs.append(_pinned((h, w, 3), np.uint16))
+        params.append(lre.develop_params(cfa=cfa, cam_mul=wb, defringe=1, axial_ca_correction=1,
+                                         output_bits=16, stage_order=1))
+    torch.cuda.empty_cache()
+    total_mp = sum(h * w for _, h, w, _, _ in specs) / 1e6
+    b = lre.Batch(acc.device, lanes=0, use_graph=True, autotune=True)
+    t0 = time.perf_counter()
+    b.run(mos, params, outs)  # autotune + capture
+    first_s = time.perf_counter() - t0
+    tune_ms = b.last_stats.tune_ms
+    b.run(mos, params, outs)  # replay (warm)
+    steps = max(2, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        b.run(mos, params, outs)
+    dt = (time.perf_counter() - t0) / steps
+    st = b.last_stats
+    tuning = b.get_tuning()
+    b.close()
+    # plain per-image path on the same images, same kernel shapes
+    acc.set_stream(None)
+    acc.set_tuning(tuning["axial_tile"], tuning["axial_threads"], tuning["blur_tile"])
+    acc.develop(mos[0], params[0], out=outs[0])
+    t0 = time.perf_counter()
+    for m, p, o in zip(mos, params, outs):
+        acc.develop(m, p, out=o)
+    dt_plain = time.perf_counter() - t0
+    acc.set_tuning()
+    del mos, outs
+    return {
+        "value": round(total_mp / dt, 2),
+        "unit": "MP/s",
+        "ms_per_batch": round(dt * 1e3, 1),
+        "images": len(specs),
+        "total_mp": round(total_mp, 1),
+        "plain_e2e": round(total_mp / dt_plain, 2),
+        "speedup_vs_plain": round(dt_plain / dt, 3),
+        "graph": int(st.graph),
+        "lanes": int(st.lanes),
+        "gpu_launches": int(st.launches),
+        "tuning": tuning,
+        "first_call_s": round(first_s, 2),
+        "tune_ms": round(tune_ms, 1),
+        "h2d_bytes_per_step": int(sum(h * w * 4 for _, h, w, _, _ in specs)),
+        "d2h_bytes_per_step": int(sum(h * w * 6 for _, h, w, _, _ in specs)),
+        "workload": "32 Bayer images (sizes/CFA/WB by seeds 100..131), AMaZE->defringe->axial CA, u16 out; "
+                    "host page-locked buffers in/out, timed per whole batch",
+    }
+
+
+def run_served(args):
+    """Poisson arrivals of develop requests through lre_server_*: 60% 6000x4000
+    Bayer, 25% 8256x5504 Bayer, 15% 6240x4160 X-Trans; defringe p=.5, axial
+    p=.5, lateral p=.2, ACES p=.3; 150 GB device budget, 4 lanes, u16 out.
+    Reports p50/p99 of submit -> result-in-host-memory per arrival rate, and
+    the throughput of a saturated queue."""
+    import threading
+
+    import numpy as np
+    import torch
+
+    import libraw_enhanced_b200 as lre
+    from libraw_enhanced_b200 import scenes
+
+    kinds = [("bayer", 4000, 6000, 0.60), ("bayer", 5504, 8256, 0.25), ("xtrans", 4160, 6240, 0.15)]
+    pool = []  # (kind index, mosaic, base params)
+    for ki, (kind, h, w, _) in enumerate(kinds):
+        for j in range(2):
+            seed = 500 + 10 * ki + j
+            if kind == "bayer":
+                cfa = ["RGGB", "BGGR", "GRBG", "GBRG"][(ki + j) % 4]
+                wb = (2.0 - 0.2 * j, 1.0, 1.5 + 0.1 * j, 1.0)
+                d = scenes.mosaic_upscaled_torch(seed, h, w, cfa, wb)
+                p = lre.develop_params(cfa=cfa, cam_mul=wb, output_bits=16)
+            else:
+                wb = (1.8, 1.0, 1.6, 1.0)
+                d = scenes.mosaic_upscaled_torch(seed, h, w, scenes.XTRANS_STD, wb)
+                p = lre.develop_params(cfa=scenes.XTRANS_STD, cam_mul=wb, output_bits=16)
+            hm = _pinned((h, w), np.float32)
+            torch.from_numpy(hm).copy_(d.cpu())
+            del d
+            pool.append((ki, hm, p))
+    torch.cuda.empty_cache()
+    n_ring = 24
+    max_px = max(h * w for _, h, w, _ in kinds)
+    ring = [_pinned((max_px * 3,), np.uint16) for _ in range(n_ring)]
+    rng = np.random.Generator(np.random.PCG64(500))
+
+    def make_request():
+        ki = int(rng.choice(3, p=[k[3] for k in kinds]))
+        cand = [e for e in pool if e[0] == ki]
+        _, m, base = cand[int(rng.integers(0, len(cand)))]
+        p = lre.DevelopParams.from_buffer_copy(base)
+        p.defringe = int(rng.random() < 0.5)
+        p.axial_ca_correction = int(rng.random() < 0.5)
+        p.lateral_ca_correction = int(rng.random() < 0.2)
+        p.tone_mapping = 1 if rng.random() < 0.3 else 0
+        return m, p
+
+    srv = lre.Server(0, lanes=4, budget_bytes=150 * 10**9)
+
+    def run_stream(n, lam):
+        reqs = [make_request() for _ in range(n)]
+        gaps = rng.exponential(1.0 / lam, size=n) if lam else np.zeros(n)
+        tickets = [None] * n
+        stats = [None] * n
+        done_evt = [threading.Event() for _ in range(n)]
+
+        def waiter():
+            for k in range(n):
+                while tickets[k] is None:
+                    time.sleep(0.0002)
+                out, s = srv.wait(tickets[k])
+                stats[k] = s
+                done_evt[k].set()
+
+        wt = threading.Thread(target=waiter)
+        wt.start()
+        t0 = time.perf_counter()
+        t_next = t0
+        for k, (m, p) in enumerate(reqs):
+            t_next += gaps[k]
+            dly = t_next - time.perf_counter()
+            if dly > 0:
+                time.sleep(dly)
+            if k >= n_ring:
+                done_evt[k - n_ring].wait()
+            h, w = m.shape
+            out = ring[k % n_ring][: h * w * 3].reshape(h, w, 3)
+            tickets[k] = srv.submit(m, p, out=out)
+        wt.join()
+        t_end = time.perf_counter()
+        lat = np.array([s["total_ms"] for s in stats])
+        mp = sum(m.shape[0] * m.shape[1] for m, _ in reqs) / 1e6
+        return {
+            "lambda": lam if lam else "saturated",
+            "n": n,
+            "p50_ms": round(float(np.percentile(lat, 50)), 1),
+            "p99_ms": round(float(np.percentile(lat, 99)), 1),
+            "mean_queue_ms": round(float(np.mean([s["queue_ms"] for s in stats])), 1),
+            "mp_s": round(mp / (t_end - t0), 1),
+            "mp_per_request": round(mp / n, 2),
+        }
+
+    run_stream(8, 0)  # warm-up: every lane sizes its buffers
+    rates = []
+    for lam in (5, 10, 20, 30, 45, 60):
+        rates.append(run_stream(48, lam))
+    sat = run_stream(48, 0)
+    _, peak = srv.memory()
+    srv.close()
+    del ring, pool
+    return {
+        "unit": "MP/s",
+        "rates": rates,
+        "saturated_mp_s": sat["mp_s"],
+        "saturated_p50_ms": sat["p50_ms"],
+        "saturated_p99_ms": sat["p99_ms"],
+        "lanes": 4,
+        "budget_gb": 150,
+        "peak_device_gb": round(peak / 1e9, 2),
+        "workload": "Poisson arrivals, 48 requests per rate: 60% 6000x4000 Bayer, 25% 8256x5504 Bayer, "
+                    "15% 6240x4160 X-Trans; defringe .5, axial .5, lateral .2, ACES .3; u16 out; "
+                    "latency = submit -> result in page-locked host memory",
+    }
+
+
 def scenes_filters():
     from libraw_enhanced_b200 import scenes
 
@@ -453,6 +654,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 32-image batched develop")
+    ap.add_argument("--no-serve", action="store_true", help="skip the request-server sweep")
     ap.add_argument("--size", default=None, help="WxH of a reduced case (profiling); default 8736x5856")
     args = ap.parse_args()
     if args.size:

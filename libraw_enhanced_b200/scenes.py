@@ -242,3 +242,46 @@ def xtrans_lateral_ca(seed: int = 3, h: int = 4160, w: int = 6240, wb=(1.8, 1.0,
 
 def random_cfa_name(rng) -> str:
     return ["RGGB", "BGGR", "GRBG", "GBRG"][int(rng.integers(0, 4))]
+
+
+# ------------------------------------------------------------ multi-image sets
+BATCH_SIZES = [(3024, 4032), (4000, 6000), (5504, 8256), (6336, 9504)]
+
+
+def batch_specs(n: int = 32, seed_base: int = 100):
+    """The batched-develop set: per image (seed, h, w, cfa, wb), drawn by seed
+    from the four sensor sizes and four Bayer layouts, WB R ~ U[1.5, 2.5],
+    B ~ U[1.2, 2.0], G = 1."""
+    out = []
+    for i in range(n):
+        rng = np.random.Generator(np.random.PCG64(seed_base + i))
+        h, w = BATCH_SIZES[int(rng.integers(0, 4))]
+        cfa = random_cfa_name(rng)
+        wb = (float(rng.uniform(1.5, 2.5)), 1.0, float(rng.uniform(1.2, 2.0)), 1.0)
+        out.append((seed_base + i, h, w, cfa, wb))
+    return out
+
+
+def mosaic_upscaled_torch(seed: int, h: int, w: int, cfa, wb, base=(512, 768), device="cuda"):
+    """A large seeded mosaic generated on the GPU (for multi-image benchmarks
+    where numpy generation would take minutes): the seeded scene at `base`
+    resolution, upscaled bilinearly, mosaiced through `cfa` (Bayer name or a
+    6x6 X-Trans pattern), Poisson-Gaussian noise (gain 1/4000, read sigma
+    0.002) and per-site WB.  Returns a float32 CUDA tensor (h, w)."""
+    import torch
+    import torch.nn.functional as F
+
+    small = torch.from_numpy(scene_rgb(base[0], base[1], seed)).to(device)
+    big = F.interpolate(small.permute(2, 0, 1)[None], size=(h, w), mode="bilinear", align_corners=False)[0]
+    period = 6 if isinstance(cfa, np.ndarray) else 2
+    idx = torch.from_numpy(cfa_map(period, period, cfa)).to(device)
+    ii = idx.repeat((h + period - 1) // period, (w + period - 1) // period)[:h, :w]
+    ch = torch.where(ii == 3, torch.ones_like(ii), ii)
+    x = torch.gather(big, 0, ch[None]).squeeze(0).clamp_min_(0)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed + 7919)
+    x = torch.poisson(x * 4000.0, generator=g) / 4000.0
+    x += torch.randn(x.shape, generator=g, device=device) * 0.002
+    x.clamp_min_(0)
+    gains = torch.tensor(list(wb), dtype=torch.float32, device=device)[ii]
+    return (x * gains).float().contiguous()
