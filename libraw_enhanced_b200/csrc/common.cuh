@@ -51,6 +51,20 @@ __device__ __forceinline__ float warp_max(float v) {
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
+// Max of a non-negative value over the CTA, folded into *addr with one
+// atomic per CTA (every thread of the CTA must call it).
+__device__ __forceinline__ void block_max_atomic(float v, float* addr) {
+  __shared__ float s_wmax[32];
+  v = warp_max(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) s_wmax[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    float x = lane < (int)((blockDim.x + 31) >> 5) ? s_wmax[lane] : 0.f;
+    x = warp_max(x);
+    if (lane == 0) atomic_max_float(addr, x);
+  }
+}
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -17,6 +17,7 @@
 //   K7  classification + correction (in-place safe)
 // Blurs stage a (T+2ks)^2 clamped halo tile in shared memory and run both
 // passes there; the line-link kernel stages a +-14 px clamped halo.
+#include <algorithm>
 #include <cmath>
 
 #include "lre_internal.h"
@@ -60,37 +61,62 @@ __device__ __forceinline__ float guide_signal_at(const float* __restrict__ src, 
   return sqrtf(sclamp(gg / max_guide, 0.f, 1.f));
 }
 
-__global__ void k_df_prep(const float* __restrict__ src, int W, int H, DfScalars* sc, float* __restrict__ lrg,
-                          float* __restrict__ lbg, float* __restrict__ er) {
+// K1 on 32 x 8 output tiles: the guide signal (a square root and a divide
+// per pixel) is staged once per pixel in shared memory with a 1-px halo and
+// the Sobel taps read it from there, instead of recomputing it for each of
+// the 8 neighbours that use it.
+constexpr int PT_X = 32, PT_Y = 8;
+
+__global__ void __launch_bounds__(256) k_df_prep_tiled(const float* __restrict__ src, int W, int H, DfScalars* sc,
+                                                       float* __restrict__ lrg, float* __restrict__ lbg,
+                                                       float* __restrict__ er) {
+  __shared__ float s_g[PT_Y + 2][PT_X + 3];
   const float max_guide = df_max_guide(sc);
   const float ratio_eps = smax(max_guide * 1e-4f, 1e-6f);
   const int limit_y = (H > 1) ? H - 1 : 1;
   const int limit_x = (W > 1) ? W - 1 : 1;
+  const int tiles_x = (W + PT_X - 1) / PT_X;
+  const int n_tiles = tiles_x * ((H + PT_Y - 1) / PT_Y);
   float local_max = 0.f;
-  size_t n = (size_t)W * H;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    int y = (int)(i / W), x = (int)(i % W);
-    const float* p = src + i * 3;
-    float r = p[0], g = p[1], b = p[2];
-    float gg = smax(g, 0.f);
-    lrg[i] = log_cr((smax(r, 0.f) + ratio_eps) / (gg + ratio_eps));
-    lbg[i] = log_cr((smax(b, 0.f) + ratio_eps) / (gg + ratio_eps));
-    float mag = 0.f;
-    if (y >= 1 && y < limit_y && x >= 1 && x < limit_x) {
-      float a00 = guide_signal_at(src, x - 1, y - 1, W, max_guide);
-      float a01 = guide_signal_at(src, x, y - 1, W, max_guide);
-      float a02 = guide_signal_at(src, x + 1, y - 1, W, max_guide);
-      float a10 = guide_signal_at(src, x - 1, y, W, max_guide);
-      float a12 = guide_signal_at(src, x + 1, y, W, max_guide);
-      float a20 = guide_signal_at(src, x - 1, y + 1, W, max_guide);
-      float a21 = guide_signal_at(src, x, y + 1, W, max_guide);
-      float a22 = guide_signal_at(src, x + 1, y + 1, W, max_guide);
-      float gx = -a00 + a02 - 2.f * a10 + 2.f * a12 - a20 + a22;
-      float gy = -a00 - 2.f * a01 - a02 + a20 + 2.f * a21 + a22;
-      mag = sqrtf(gx * gx + gy * gy);
-      local_max = smax(local_max, mag);
+  // a CTA walks several tiles, so the max-edge reduction costs one atomic
+  // per warp in total rather than one per tile
+  for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    const int x0 = (t % tiles_x) * PT_X, y0 = (t / tiles_x) * PT_Y;
+    __syncthreads();  // the previous tile's readers are done with s_g
+    for (int i = threadIdx.x; i < (PT_Y + 2) * (PT_X + 2); i += blockDim.x) {
+      const int r = i / (PT_X + 2), q = i % (PT_X + 2);
+      const int gy = min(max(y0 - 1 + r, 0), H - 1);
+      const int gx = min(max(x0 - 1 + q, 0), W - 1);
+      s_g[r][q] = guide_signal_at(src, gx, gy, W, max_guide);
     }
-    er[i] = mag;
+    __syncthreads();
+    const int tx = threadIdx.x % PT_X, ty = threadIdx.x / PT_X;
+    const int x = x0 + tx, y = y0 + ty;
+    if (x < W && y < H) {
+      const size_t i = (size_t)y * W + x;
+      const float* p = src + i * 3;
+      float r = p[0], g = p[1], b = p[2];
+      float gg = smax(g, 0.f);
+      lrg[i] = log_cr((smax(r, 0.f) + ratio_eps) / (gg + ratio_eps));
+      lbg[i] = log_cr((smax(b, 0.f) + ratio_eps) / (gg + ratio_eps));
+      float mag = 0.f;
+      if (y >= 1 && y < limit_y && x >= 1 && x < limit_x) {
+        const int cy = ty + 1, cx = tx + 1;
+        float a00 = s_g[cy - 1][cx - 1];
+        float a01 = s_g[cy - 1][cx];
+        float a02 = s_g[cy - 1][cx + 1];
+        float a10 = s_g[cy][cx - 1];
+        float a12 = s_g[cy][cx + 1];
+        float a20 = s_g[cy + 1][cx - 1];
+        float a21 = s_g[cy + 1][cx];
+        float a22 = s_g[cy + 1][cx + 1];
+        float gx = -a00 + a02 - 2.f * a10 + 2.f * a12 - a20 + a22;
+        float gy = -a00 - 2.f * a01 - a02 + a20 + 2.f * a21 + a22;
+        mag = sqrtf(gx * gx + gy * gy);
+        local_max = smax(local_max, mag);
+      }
+      er[i] = mag;
+    }
   }
   local_max = warp_max(local_max);
   if ((threadIdx.x & 31) == 0) atomic_max_float(&sc->max_edge, local_max);
@@ -390,10 +416,24 @@ __global__ void __launch_bounds__(256, 3) k_df_main(const float* src, float* dst
   const bool enable_green = k.green != 0;
   const float edge_threshold = k.edge_thr, chroma_threshold = k.chroma_thr, strength = k.strength;
   const float green_strength_scale = sclamp(k.green_scale, 0.f, 1.f);
+  // Pixels that provably keep their input: with green correction off, an
+  // edge weight of exactly zero (both edge factors at or below their lower
+  // smoothstep edges) makes every mask zero, and zero solo blurs make the
+  // solo masks zero, so the output is the input whatever the other planes
+  // hold.  Those pixels read 4 planes instead of 11 and skip the rest.
+  const float e0_edge = edge_threshold * 0.10f * inv_s;
+  const float e0_raw = 0.20f * inv_s;
+  const bool can_skip = !enable_green && edge_threshold > 0.f;  // smoothstep edges strictly ordered
   size_t n = (size_t)W * H;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const float s0 = src[i * 3 + 0], s1 = src[i * 3 + 1], s2 = src[i * 3 + 2];
     float d0 = s0, d1 = s1, d2 = s2;
+    if (can_skip && P.be[i] <= e0_edge && P.ber[i] <= e0_raw && P.srb[i] == 0.f && P.sbb[i] == 0.f) {
+      dst[i * 3 + 0] = d0;
+      dst[i * 3 + 1] = d1;
+      dst[i * 3 + 2] = d2;
+      continue;
+    }
     const float blur_guide = P.bg[i];
     const float blur_log_rg = P.blrg[i];
     const float blur_log_bg = P.blbg[i];
@@ -730,7 +770,9 @@ lre_status launch_defringe(Context* c, const float* in, float* out, size_t w, si
 
   k_df_init<<<1, 1, 0, c->stream>>>(sc);
   k_df_maxg<<<grid_for(n, 256, c->sm_count * 4), 256, 0, c->stream>>>(in, n, sc);
-  k_df_prep<<<gstream, 256, 0, c->stream>>>(in, W, H, sc, P.lrg, P.lbg, P.er);
+  const size_t prep_tiles = (size_t)((W + PT_X - 1) / PT_X) * ((H + PT_Y - 1) / PT_Y);
+  k_df_prep_tiled<<<(unsigned)std::min<size_t>(prep_tiles, (size_t)c->sm_count * 8), 256, 0, c->stream>>>(
+      in, W, H, sc, P.lrg, P.lbg, P.er);
   count_launch(c, 3);
   LRE_TRY(check_launch(c, "defringe prep"));
 

@@ -189,8 +189,7 @@ __global__ void __launch_bounds__(256) k_mc_stats(const float* __restrict__ in, 
       local_max = smax(local_max, sd);
     }
   }
-  local_max = warp_max(local_max);
-  if ((threadIdx.x & 31) == 0) atomic_max_float(d_max, local_max);
+  block_max_atomic(local_max, d_max);
 }
 
 __global__ void k_mc_apply(const float* in, float* out, const float* __restrict__ mean3,

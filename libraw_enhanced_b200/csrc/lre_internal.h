@@ -54,7 +54,7 @@ struct WsPlan {
 struct Tuning {
   int axial_tile = 32;      // guided-filter output tile edge: 32 or 16
   int axial_threads = 512;  // guided-filter CTA size: 512 or 256
-  int blur_tile = 32;       // defringe register-tiled blur output tile edge: 32 or 64
+  int blur_tile = 64;       // defringe register-tiled blur output tile edge: 64 or 32
 };
 
 struct Context {
