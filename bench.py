@@ -494,7 +494,7 @@ def run_batched(args, acc):
     b.close()
     # plain per-image path on the same images, same kernel shapes
     acc.set_stream(None)
-    acc.set_tuning(tuning["axial_tile"], tuning["axial_threads"], tuning["blur_tile"])
+    acc.set_tuning(tuning["axial_strip"], tuning["axial_rows"], tuning["blur_tile"])
     acc.develop(mos[0], params[0], out=outs[0])
     t0 = time.perf_counter()
     for m, p, o in zip(mos, params, outs):

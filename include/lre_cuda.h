@@ -253,8 +253,8 @@ lre_status lre_dev_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t 
 /* Kernel-shape choices that never change results, only speed. */
 typedef struct lre_tuning {
   int lanes;         /* batch/server: concurrent per-image pipelines (streams) */
-  int axial_tile;    /* guided-filter output tile edge: 32 or 16             */
-  int axial_threads; /* guided-filter CTA size: 512 or 256                    */
+  int axial_strip;   /* guided-filter strip width (columns per CTA): 128 or 64 */
+  int axial_rows;    /* guided-filter output rows per CTA: 128 or 64          */
   int blur_tile;     /* defringe blur output tile edge: 32 or 64              */
 } lre_tuning;
 lre_status lre_set_tuning(lre_ctx* ctx, const lre_tuning* t);

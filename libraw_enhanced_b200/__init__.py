@@ -318,14 +318,14 @@ class CudaAccelerator:
         self._check(self._lib.lre_dev_develop(self._h, _dptr(mosaic), _dptr(out), int(width), int(height), C.byref(params)))
 
     # ------------------------------------------------------------ tuning
-    def set_tuning(self, axial_tile=32, axial_threads=512, blur_tile=32) -> None:
-        t = _lib.Tuning(1, int(axial_tile), int(axial_threads), int(blur_tile))
+    def set_tuning(self, axial_strip=128, axial_rows=128, blur_tile=64) -> None:
+        t = _lib.Tuning(1, int(axial_strip), int(axial_rows), int(blur_tile))
         self._check(self._lib.lre_set_tuning(self._h, C.byref(t)))
 
     def get_tuning(self) -> dict:
         t = _lib.Tuning()
         self._check(self._lib.lre_get_tuning(self._h, C.byref(t)))
-        return {"axial_tile": t.axial_tile, "axial_threads": t.axial_threads, "blur_tile": t.blur_tile}
+        return {"axial_strip": t.axial_strip, "axial_rows": t.axial_rows, "blur_tile": t.blur_tile}
 
 
 def _out_for(h, w, params):
@@ -404,10 +404,10 @@ class Batch:
     def get_tuning(self) -> dict:
         t = _lib.Tuning()
         self._check(self._lib.lre_batch_get_tuning(self._h, C.byref(t)))
-        return {"lanes": t.lanes, "axial_tile": t.axial_tile, "axial_threads": t.axial_threads, "blur_tile": t.blur_tile}
+        return {"lanes": t.lanes, "axial_strip": t.axial_strip, "axial_rows": t.axial_rows, "blur_tile": t.blur_tile}
 
-    def set_tuning(self, lanes=3, axial_tile=32, axial_threads=512, blur_tile=32) -> None:
-        t = _lib.Tuning(int(lanes), int(axial_tile), int(axial_threads), int(blur_tile))
+    def set_tuning(self, lanes=3, axial_strip=128, axial_rows=128, blur_tile=64) -> None:
+        t = _lib.Tuning(int(lanes), int(axial_strip), int(axial_rows), int(blur_tile))
         self._check(self._lib.lre_batch_set_tuning(self._h, C.byref(t)))
 
 

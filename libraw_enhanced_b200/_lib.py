@@ -68,7 +68,7 @@ class DevelopParams(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("lanes", C.c_int), ("axial_tile", C.c_int), ("axial_threads", C.c_int), ("blur_tile", C.c_int)]
+    _fields_ = [("lanes", C.c_int), ("axial_strip", C.c_int), ("axial_rows", C.c_int), ("blur_tile", C.c_int)]
 
 
 class Image(C.Structure):

@@ -15,12 +15,13 @@
 //   * edge weight w = smoothstep(0.01, 0.06, boxmean_r(|central grad G|));
 //   * out = (X (1 - s w) + q s w) * norm, G passes through.
 //
-// B200 design: ONE fused kernel per image.  A CTA owns a T x T output tile,
-// stages the normalised (T+4r)^2 input region in shared memory once, and runs
-// both box-filter levels, the a/b solve, the edge gate and the blend out of
-// shared memory, so HBM sees 12 B/px in + 12 B/px out (the algorithmic
-// minimum) plus halo re-reads that hit L2.  The only other pass is the global
-// max(G) reduction that the normalisation needs before any tile can start.
+// B200 design: after the global max(G) reduction, two streaming passes over
+// column strips (k_ax_ab: guide statistics and the a/b solve for R and B;
+// k_ax_q: second box level, edge gate and blend), each pixel's window sums
+// computed once, with the a/b planes (16 B/px) passing through HBM.  The
+// older single fused tile kernel (k_axial_fused: both box levels out of
+// shared memory, the level-one statistics recomputed over each tile's halo)
+// remains for the allocation-free entry point at the end of this file.
 #include <mutex>
 
 #include "common.cuh"
@@ -384,13 +385,227 @@ cudaError_t axial_dispatch(int T, int NT, size_t w, size_t h, cudaStream_t s, co
   return axial_launch<16, 256>(grid, g.bytes, s, src, out, (int)w, (int)h, r, eps, strength, d_max);
 }
 
+// ---------------------------------------------------------------------------
+// Streaming two-pass form (the default path).  The image is cut into strips
+// of WS output columns and HS output rows; one warp walks a strip down its
+// rows.  The vertical window sum of every column of the strip (plus r halo
+// columns each side) lives in shared memory and slides: each row step adds
+// the row entering the window and subtracts the row leaving it.  Each lane
+// then forms the horizontal window sums of 4 adjacent output columns, sliding
+// across them.  Every pixel's statistics are computed once, all sums are in
+// double, and HBM carries the a/b planes between the two box levels.
+//   pass A: G, G^2, R, G R, B, G B -> a_R, b_R, a_B, b_B (float planes)
+//   pass B: a_R, b_R, a_B, b_B, |grad G| -> blended output
+// Window sums use the same truncated windows, area reciprocals and float /
+// double conversions as the fused kernel; only the summation order differs.
+constexpr int AXS_PER_LANE = 4;  // output columns per lane in the horizontal pass
+
+// Column j of a strip's shared-memory window sums, with one pad slot per 16
+// doubles: lanes reading 4 apart then hit 16 distinct 8-byte bank pairs.
+__device__ __forceinline__ int vidx(int j) { return j + (j >> 4); }
+template <int WS>
+__host__ __device__ constexpr int vs_len() { return (WS + 32) + (WS + 32) / 16 + 1; }
+
+// Quantities of pass A at (x, y) of the normalised image (zeros outside).
+struct AbQ {
+  __device__ static void load(const float* __restrict__ src, int W, int H, int x, int y, float inv_norm, double* q) {
+    float g = 0.f, rr = 0.f, b = 0.f;
+    if (x >= 0 && x < W && y >= 0 && y < H) {
+      const float* p = src + ((size_t)y * W + x) * 3;
+      rr = p[0] * inv_norm;
+      g = p[1] * inv_norm;
+      b = p[2] * inv_norm;
+    }
+    q[0] = (double)g;
+    q[1] = (double)(g * g);
+    q[2] = (double)rr;
+    q[3] = (double)(g * rr);
+    q[4] = (double)b;
+    q[5] = (double)(g * b);
+  }
+};
+
+template <int NQ, int WS, typename Loader>
+__device__ __forceinline__ void strip_update(double (*Vs)[vs_len<WS>()], int VC, int xv0, int y_add, int y_sub, Loader ld) {
+  for (int j = threadIdx.x; j < VC; j += 32) {
+    double qa[NQ], qs[NQ];
+    const int x = xv0 + j;
+    ld(x, y_add, qa);
+    ld(x, y_sub, qs);
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+      double v = Vs[q][vidx(j)];
+      v += qa[q];
+      v -= qs[q];
+      Vs[q][vidx(j)] = v;
+    }
+  }
+}
+
+// Horizontal window sums of the lane's 4 output columns: hs[q][k].
+template <int NQ, int WS>
+__device__ __forceinline__ void strip_hsum(double (*Vs)[vs_len<WS>()], int r, double hs[NQ][AXS_PER_LANE]) {
+  const int c0 = threadIdx.x * AXS_PER_LANE;
+#pragma unroll
+  for (int q = 0; q < NQ; q++) {
+    double s = 0.0;
+    for (int t = 0; t <= 2 * r; t++) s += Vs[q][vidx(c0 + t)];
+    hs[q][0] = s;
+#pragma unroll
+    for (int k = 1; k < AXS_PER_LANE; k++) {
+      s += Vs[q][vidx(c0 + k + 2 * r)];
+      s -= Vs[q][vidx(c0 + k - 1)];
+      hs[q][k] = s;
+    }
+  }
+}
+
+template <int WS>
+__global__ void __launch_bounds__(32) k_ax_ab(const float* __restrict__ src, int W, int H, int r, float eps, int HS,
+                                             const float* __restrict__ d_maxg, float* __restrict__ aR,
+                                             float* __restrict__ bR, float* __restrict__ aB, float* __restrict__ bB) {
+  constexpr int NQ = 6;
+  static_assert(WS == 32 * AXS_PER_LANE, "one warp covers the strip");
+  __shared__ double Vs[NQ][vs_len<WS>()];
+  const int VC = WS + 2 * r;
+  const float inv_norm = 1.f / fmaxf(*d_maxg, 1e-6f);
+  const int x0 = blockIdx.x * WS, y0 = blockIdx.y * HS;
+  const int xv0 = x0 - r;
+  const int y_end = min(y0 + HS, H);
+  auto ld = [&](int x, int y, double* q) { AbQ::load(src, W, H, x, y, inv_norm, q); };
+  for (int j = threadIdx.x; j < VC; j += 32)
+#pragma unroll
+    for (int q = 0; q < NQ; q++) Vs[q][vidx(j)] = 0.0;
+  // window of the first output row: rows [y0 - r, y0 + r] (out-of-image rows load zeros)
+  for (int iy = y0 - r; iy <= y0 + r; iy++) strip_update<NQ, WS>(Vs, VC, xv0, iy, -1, ld);
+  double inv_cx[AXS_PER_LANE];
+#pragma unroll
+  for (int k = 0; k < AXS_PER_LANE; k++) {
+    const int x = x0 + threadIdx.x * AXS_PER_LANE + k;
+    inv_cx[k] = x < W ? 1.0 / (double)win_count(x, r, W) : 0.0;
+  }
+  for (int y = y0; y < y_end; y++) {
+    if (y > y0) strip_update<NQ, WS>(Vs, VC, xv0, y + r, y - r - 1, ld);
+    __syncwarp();
+    double hs[NQ][AXS_PER_LANE];
+    strip_hsum<NQ, WS>(Vs, r, hs);
+    __syncwarp();  // the next update rewrites Vs
+    const double inv_cy = 1.0 / (double)win_count(y, r, H);
+#pragma unroll
+    for (int k = 0; k < AXS_PER_LANE; k++) {
+      const int x = x0 + threadIdx.x * AXS_PER_LANE + k;
+      if (x >= W) continue;
+      const double ia = inv_cx[k] * inv_cy;
+      const double mi = hs[0][k] * ia;
+      const double vi = hs[1][k] * ia - mi * mi;
+      const size_t o = (size_t)y * W + x;
+#pragma unroll
+      for (int ch = 0; ch < 2; ch++) {
+        const double mp = hs[2 + 2 * ch][k] * ia, mIp = hs[3 + 2 * ch][k] * ia;
+        const double cov = mIp - mi * mp;
+        const double a = cov / (vi + (double)eps);
+        const double b = mp - a * mi;
+        (ch == 0 ? aR : aB)[o] = (float)a;
+        (ch == 0 ? bR : bB)[o] = (float)b;
+      }
+    }
+  }
+}
+
+template <int WS>
+__global__ void __launch_bounds__(32) k_ax_q(const float* __restrict__ src, float* __restrict__ dst, int W, int H,
+                                            int r, float strength, int HS, const float* __restrict__ d_maxg,
+                                            const float* __restrict__ aR, const float* __restrict__ bR,
+                                            const float* __restrict__ aB, const float* __restrict__ bB) {
+  constexpr int NQ = 5;
+  static_assert(WS == 32 * AXS_PER_LANE, "one warp covers the strip");
+  __shared__ double Vs[NQ][vs_len<WS>()];
+  const int VC = WS + 2 * r;
+  const float norm_ref = fmaxf(*d_maxg, 1e-6f);
+  const float inv_norm = 1.f / norm_ref;
+  const int x0 = blockIdx.x * WS, y0 = blockIdx.y * HS;
+  const int xv0 = x0 - r;
+  const int y_end = min(y0 + HS, H);
+  auto ld = [&](int x, int y, double* q) {
+    float va = 0.f, vb = 0.f, vc = 0.f, vd = 0.f, e = 0.f;
+    if (x >= 0 && x < W && y >= 0 && y < H) {
+      const size_t i = (size_t)y * W + x;
+      va = aR[i];
+      vb = bR[i];
+      vc = aB[i];
+      vd = bB[i];
+      if (x >= 1 && x < W - 1 && y >= 1 && y < H - 1) {
+        const float gxv = src[(i + 1) * 3 + 1] * inv_norm - src[(i - 1) * 3 + 1] * inv_norm;
+        const float gyv = src[(i + W) * 3 + 1] * inv_norm - src[(i - W) * 3 + 1] * inv_norm;
+        e = sqrtf(gxv * gxv + gyv * gyv);
+      }
+    }
+    q[0] = (double)va;
+    q[1] = (double)vb;
+    q[2] = (double)vc;
+    q[3] = (double)vd;
+    q[4] = (double)e;
+  };
+  for (int j = threadIdx.x; j < VC; j += 32)
+#pragma unroll
+    for (int q = 0; q < NQ; q++) Vs[q][vidx(j)] = 0.0;
+  for (int iy = y0 - r; iy <= y0 + r; iy++) strip_update<NQ, WS>(Vs, VC, xv0, iy, -1, ld);
+  double inv_cx[AXS_PER_LANE];
+#pragma unroll
+  for (int k = 0; k < AXS_PER_LANE; k++) {
+    const int x = x0 + threadIdx.x * AXS_PER_LANE + k;
+    inv_cx[k] = x < W ? 1.0 / (double)win_count(x, r, W) : 0.0;
+  }
+  for (int y = y0; y < y_end; y++) {
+    if (y > y0) strip_update<NQ, WS>(Vs, VC, xv0, y + r, y - r - 1, ld);
+    __syncwarp();
+    double hs[NQ][AXS_PER_LANE];
+    strip_hsum<NQ, WS>(Vs, r, hs);
+    __syncwarp();
+    const double inv_cy = 1.0 / (double)win_count(y, r, H);
+#pragma unroll
+    for (int k = 0; k < AXS_PER_LANE; k++) {
+      const int x = x0 + threadIdx.x * AXS_PER_LANE + k;
+      if (x >= W) continue;
+      const double ia = inv_cx[k] * inv_cy;
+      const size_t o = ((size_t)y * W + x) * 3;
+      const float R = src[o + 0] * inv_norm;
+      const float G = src[o + 1];
+      const float I = G * inv_norm;
+      const float B = src[o + 2] * inv_norm;
+      const float qR = (float)((hs[0][k] * ia) * (double)I + hs[1][k] * ia);
+      const float qB = (float)((hs[2][k] * ia) * (double)I + hs[3][k] * ia);
+      const float tt = clampf(((float)(hs[4][k] * ia) - 0.01f) / 0.05f, 0.f, 1.f);
+      const float w = strength * (tt * tt * (3.f - 2.f * tt));
+      dst[o + 0] = (R * (1.f - w) + qR * w) * norm_ref;
+      dst[o + 1] = G;
+      dst[o + 2] = (B * (1.f - w) + qB * w) * norm_ref;
+    }
+  }
+}
+
+cudaError_t axial_stream(size_t w, size_t h, int HS, cudaStream_t s, const float* src, float* out, int r, float eps,
+                         float strength, const float* d_max, float* planes) {
+  constexpr int WS = 32 * AXS_PER_LANE;
+  const size_t n = w * h;
+  float* aR = planes;
+  float* bR = planes + n;
+  float* aB = planes + 2 * n;
+  float* bB = planes + 3 * n;
+  dim3 grid((unsigned)((w + WS - 1) / WS), (unsigned)((h + HS - 1) / HS));
+  k_ax_ab<WS><<<grid, 32, 0, s>>>(src, (int)w, (int)h, r, eps, HS, d_max, aR, bR, aB, bB);
+  k_ax_q<WS><<<grid, 32, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max, aR, bR, aB, bB);
+  return cudaPeekAtLastError();
+}
+
 }  // namespace
 
 size_t ws_bytes_axial(size_t w, size_t h, int radius) {
   (void)radius;
-  // out-of-place copy when the caller runs in place (tiles read halos of
-  // their neighbours' inputs).
-  return w * h * 3 * sizeof(float);
+  // the four a/b planes between the two passes, plus an out-of-place copy
+  // when the caller runs in place (pass B reads input rows below the rows it
+  // writes).
+  return ((w * h * 4 * sizeof(float) + 255) & ~size_t(255)) + w * h * 3 * sizeof(float) + 256;
 }
 
 lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, size_t h, int radius, float eps,
@@ -398,7 +613,8 @@ lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, si
   if (radius < 1) radius = 1;
   if (radius > 16) return fail(c, LRE_ERR_INVALID_ARGUMENT, "ca_axial_cleanup: radius > 16 is not supported");
   strength = fminf(fmaxf(strength, 0.f), 1.f);
-  const int T = pick_tile(radius, c->tune.axial_tile);
+  float* planes = reinterpret_cast<float*>(c->ws.take(w * h * 4 * sizeof(float)));
+  if (!planes) return fail(c, LRE_ERR_OUT_OF_MEMORY, "ca_axial_cleanup: workspace too small");
   const float* src = in;
   if (in == out) {
     float* tmp = reinterpret_cast<float*>(c->ws.take(w * h * 3 * sizeof(float)));
@@ -406,8 +622,9 @@ lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, si
     LRE_CUDA_TRY(c, cudaMemcpyAsync(tmp, in, w * h * 3 * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
     src = tmp;
   }
-  LRE_CUDA_TRY(c, axial_dispatch(T, c->tune.axial_threads, w, h, c->stream, src, out, radius, eps, strength, d_max_g));
-  count_launch(c);
+  const int HS = c->tune.axial_rows == 128 ? 128 : 64;
+  LRE_CUDA_TRY(c, axial_stream(w, h, HS, c->stream, src, out, radius, eps, strength, d_max_g, planes));
+  count_launch(c, 2);
   return check_launch(c, "ca_axial_cleanup");
 }
 

@@ -52,8 +52,8 @@ struct WsPlan {
 // Kernel-shape choices that do not change results (picked by the batch
 // autotuner, or set with lre_set_tuning).
 struct Tuning {
-  int axial_tile = 32;      // guided-filter output tile edge: 32 or 16
-  int axial_threads = 512;  // guided-filter CTA size: 512 or 256
+  int axial_strip = 128;    // guided-filter strip width (columns per CTA): 128 or 64
+  int axial_rows = 128;     // guided-filter output rows per CTA: 128 or 64
   int blur_tile = 64;       // defringe register-tiled blur output tile edge: 64 or 32
 };
 

@@ -30,6 +30,7 @@ size_t stage_ws(const lre_develop_params& p, size_t w, size_t h) {
   if (p.lateral_ca_correction)
     m = std::max(m, lre::ws_bytes_lateral(w, h, p.lateral_ca_cell_size, p.lateral_ca_pyramid_levels, true));
   if (p.defringe) m = std::max(m, lre::ws_bytes_defringe(w, h, p.defringe_radius));
+  if (p.axial_ca_correction) m = std::max(m, lre::ws_bytes_axial(w, h, p.axial_ca_radius));
   if (p.tone_mapping == 2) m = std::max(m, lre::ws_bytes_detail_tonemap(w, h));
   return m + 4096;
 }

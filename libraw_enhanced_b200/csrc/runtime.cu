@@ -349,7 +349,12 @@ lre_status autotune(Batch* b, const lre_image* im, size_t n, bool host_mode) {
     cudaFree(d_b);
   };
   cudaMemcpyAsync(d_mos, ref.mosaic, w * h * 4, host_mode ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, c->stream);
-  LRE_CUDA_TRY(c, c->ws.reserve(develop_ws_bytes(ref.params, w, h), c->stream));
+  {
+    lre_develop_params all = ref.params;  // room for every stage that is timed
+    all.defringe = 1;
+    all.axial_ca_correction = 1;
+    LRE_CUDA_TRY(c, c->ws.reserve(develop_ws_bytes(all, w, h), c->stream));
+  }
   c->ws.reset();
   lre_status st = launch_amaze(c, d_mos, 1, d_a, w, h, ref.params.filters == LRE_FILTERS_XTRANS ? 0x94949494u : ref.params.filters,
                                ref.params.cam_mul, ref.params.maximum_value);
@@ -362,21 +367,24 @@ lre_status autotune(Batch* b, const lre_image* im, size_t n, bool host_mode) {
   Tuning best = b->tune;
   // guided filter variants
   {
-    const int cand[4][2] = {{32, 512}, {32, 256}, {16, 256}, {16, 512}};
+    const int cand[4][2] = {{128, 128}, {128, 64}, {64, 128}, {64, 64}};
     float best_ms = 1e30f;
     float* dmax = c->d_scalars + 1;
     for (auto& v : cand) {
-      c->tune.axial_tile = v[0];
-      c->tune.axial_threads = v[1];
+      c->tune.axial_strip = v[0];
+      c->tune.axial_rows = v[1];
       float ms = time_stream(c->stream, [&]() -> lre_status {
+        const size_t mark = c->ws.used();
         LRE_TRY(launch_channel_max(c, d_a, w * h, 1, dmax, true));
-        return launch_axial_ca(c, d_a, d_b, w, h, p.axial_ca_radius, p.axial_ca_epsilon, p.axial_ca_strength, dmax);
+        lre_status s2 = launch_axial_ca(c, d_a, d_b, w, h, p.axial_ca_radius, p.axial_ca_epsilon, p.axial_ca_strength, dmax);
+        c->ws.rewind(mark);
+        return s2;
       }, 2, &st);
       if (st != LRE_OK) break;
       if (ms < best_ms) {
         best_ms = ms;
-        best.axial_tile = v[0];
-        best.axial_threads = v[1];
+        best.axial_strip = v[0];
+        best.axial_rows = v[1];
       }
     }
   }
@@ -623,11 +631,11 @@ extern "C" {
 lre_status lre_set_tuning(lre_ctx* ctx, const lre_tuning* t) {
   Context* c = reinterpret_cast<Context*>(ctx);
   if (!c || !t) return LRE_ERR_INVALID_ARGUMENT;
-  if ((t->axial_tile != 32 && t->axial_tile != 16) || (t->axial_threads != 512 && t->axial_threads != 256) ||
+  if ((t->axial_strip != 128 && t->axial_strip != 64) || (t->axial_rows != 128 && t->axial_rows != 64) ||
       (t->blur_tile != 32 && t->blur_tile != 64))
-    return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "set_tuning: axial_tile 32|16, axial_threads 512|256, blur_tile 32|64");
-  c->tune.axial_tile = t->axial_tile;
-  c->tune.axial_threads = t->axial_threads;
+    return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "set_tuning: axial_strip 128|64, axial_rows 128|64, blur_tile 32|64");
+  c->tune.axial_strip = t->axial_strip;
+  c->tune.axial_rows = t->axial_rows;
   c->tune.blur_tile = t->blur_tile;
   return LRE_OK;
 }
@@ -636,8 +644,8 @@ lre_status lre_get_tuning(const lre_ctx* ctx, lre_tuning* t) {
   const Context* c = reinterpret_cast<const Context*>(ctx);
   if (!c || !t) return LRE_ERR_INVALID_ARGUMENT;
   t->lanes = 1;
-  t->axial_tile = c->tune.axial_tile;
-  t->axial_threads = c->tune.axial_threads;
+  t->axial_strip = c->tune.axial_strip;
+  t->axial_rows = c->tune.axial_rows;
   t->blur_tile = c->tune.blur_tile;
   return LRE_OK;
 }
@@ -700,8 +708,8 @@ lre_status lre_batch_get_tuning(const lre_batch* bp, lre_tuning* t) {
   const Batch* b = reinterpret_cast<const Batch*>(bp);
   if (!b || !t) return LRE_ERR_INVALID_ARGUMENT;
   t->lanes = b->lanes;
-  t->axial_tile = b->tune.axial_tile;
-  t->axial_threads = b->tune.axial_threads;
+  t->axial_strip = b->tune.axial_strip;
+  t->axial_rows = b->tune.axial_rows;
   t->blur_tile = b->tune.blur_tile;
   return LRE_OK;
 }
@@ -709,13 +717,13 @@ lre_status lre_batch_get_tuning(const lre_batch* bp, lre_tuning* t) {
 lre_status lre_batch_set_tuning(lre_batch* bp, const lre_tuning* t) {
   Batch* b = reinterpret_cast<Batch*>(bp);
   if (!b || !t) return LRE_ERR_INVALID_ARGUMENT;
-  if ((t->axial_tile != 32 && t->axial_tile != 16) || (t->axial_threads != 512 && t->axial_threads != 256) ||
+  if ((t->axial_strip != 128 && t->axial_strip != 64) || (t->axial_rows != 128 && t->axial_rows != 64) ||
       (t->blur_tile != 32 && t->blur_tile != 64) || t->lanes < 1 || t->lanes > 8)
-    return b->fail_msg(LRE_ERR_INVALID_ARGUMENT, "batch_set_tuning: lanes 1..8, axial_tile 32|16, axial_threads 512|256, blur_tile 32|64");
+    return b->fail_msg(LRE_ERR_INVALID_ARGUMENT, "batch_set_tuning: lanes 1..8, axial_strip 128|64, axial_rows 128|64, blur_tile 32|64");
   cudaSetDevice(b->cfg.device);
   lre::drop_graph(b);
-  b->tune.axial_tile = t->axial_tile;
-  b->tune.axial_threads = t->axial_threads;
+  b->tune.axial_strip = t->axial_strip;
+  b->tune.axial_rows = t->axial_rows;
   b->tune.blur_tile = t->blur_tile;
   b->tuned = true;
   return lre::batch_set_lanes(b, t->lanes);

@@ -73,7 +73,7 @@ def test_batch_matches_plain(lre, acc, use_graph):
         assert st.launches > 0 and st.lanes >= 1
         assert st.graph == 0
         tune = b.get_tuning()
-        acc.set_tuning(tune["axial_tile"], tune["axial_threads"], tune["blur_tile"])
+        acc.set_tuning(tune["axial_strip"], tune["axial_rows"], tune["blur_tile"])
         for m, p, o in zip(ms, ps, outs):
             _compare(o, acc.develop(m, p))
         # page-locked buffers: captured once, then replayed
@@ -101,9 +101,9 @@ def test_batch_float_output_and_tuning_choices(lre, acc):
     ms, ps = _workload(lre, bits=32)
     b = lre.Batch(0, lanes=2, use_graph=False, autotune=False)
     try:
-        for tune in ({"lanes": 2, "axial_tile": 32, "axial_threads": 512, "blur_tile": 32},
-                     {"lanes": 3, "axial_tile": 16, "axial_threads": 256, "blur_tile": 64},
-                     {"lanes": 1, "axial_tile": 32, "axial_threads": 256, "blur_tile": 64}):
+        for tune in ({"lanes": 2, "axial_strip": 128, "axial_rows": 128, "blur_tile": 32},
+                     {"lanes": 3, "axial_strip": 64, "axial_rows": 64, "blur_tile": 64},
+                     {"lanes": 1, "axial_strip": 128, "axial_rows": 64, "blur_tile": 64}):
             b.set_tuning(**tune)
             assert b.get_tuning() == tune
             outs = b.run(ms, ps)
