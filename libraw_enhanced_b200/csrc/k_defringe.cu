@@ -342,41 +342,73 @@ constexpr int LT = 32;   // line-link output tile
 constexpr int LH = 14;   // max step along a line
 constexpr int LE = LT + 2 * LH;
 
+// Running max of a line's samples.  `along` starts at 0 and the samples are
+// finite or NaN: std::max(along, v) then equals fmaxf(along, v) (neither ever
+// yields NaN), so the single-instruction form is exact here.
+template <int TX, int TY, int STEPS>
+__device__ __forceinline__ float line_along(const float* s_ls, int c) {
+  float along = 0.f;
+#pragma unroll
+  for (int step = 1; step <= STEPS; step++) {
+    along = fmaxf(along, s_ls[c + (TY * LE + TX) * step]);
+    along = fmaxf(along, s_ls[c - (TY * LE + TX) * step]);
+  }
+  return along;
+}
+
+template <int TX, int TY, int STEPS>
+__device__ __forceinline__ void line_dir(const float* s_ls, const float* s_fs, int c, float& best) {
+  const float along = line_along<TX, TY, STEPS>(s_ls, c);
+  // along == 0 contributes 0 * thin (thin in [0, 1], or NaN which
+  // std::max ignores) to a running max that is already >= 0
+  if (along == 0.f) return;
+  constexpr int NX = -TY, NY = TX;  // across-direction normal
+  const float across = smax(s_fs[c + (NY * LE + NX) * 2], s_fs[c - (NY * LE + NX) * 2]);
+  const float thin = 1.f - ssmooth(along * 0.45f, along * 0.95f, across);
+  best = smax(best, along * thin);
+}
+
 __global__ void __launch_bounds__(256) k_df_line(const float* __restrict__ src, int W, int H, DfPlanes P, DfConst k) {
   __shared__ float s_ls[LE * LE];
   __shared__ float s_fs[LE * LE];
+  __shared__ int s_any;
   const int x0 = blockIdx.x * LT, y0 = blockIdx.y * LT;
+  if (threadIdx.x == 0) s_any = 0;
+  __syncthreads();
+  int any = 0;
   for (int i = threadIdx.x; i < LE * LE; i += blockDim.x) {
     int gy = min(max(y0 - LH + i / LE, 0), H - 1);
     int gx = min(max(x0 - LH + i % LE, 0), W - 1);
     size_t gi = (size_t)gy * W + gx;
     float f = P.fs[gi];
     s_fs[i] = f;
-    s_ls[i] = smax(f, P.bfs[gi] * 0.55f);
+    const float ls = smax(f, P.bfs[gi] * 0.55f);
+    s_ls[i] = ls;
+    any |= ls != 0.f;
   }
+  if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) s_any = 1;
   __syncthreads();
+  // a tile whose line sources are all zero has every `along` zero, so every
+  // line-linked support value is exactly 0
+  const bool tile_active = s_any != 0;
   const float sensitivity = sclamp(sqrtf(smax(k.strength, 1.0f)), 1.0f, 2.5f);
   const float inv_s = 1.0f / sensitivity;
-  const int dirs[8][2] = {{1, 0}, {0, 1}, {1, 1}, {1, -1}, {2, 1}, {1, 2}, {2, -1}, {1, -2}};
   for (int i = threadIdx.x; i < LT * LT; i += blockDim.x) {
     int ly = i / LT, lx = i % LT;
     int y = y0 + ly, x = x0 + lx;
     if (x >= W || y >= H) continue;
-    const int cx = lx + LH, cy = ly + LH;
+    const int c = (ly + LH) * LE + (lx + LH);
     float best = 0.f;
-#pragma unroll
-    for (int d = 0; d < 8; d++) {
-      const int tx = dirs[d][0], ty = dirs[d][1];
-      const int nx = -ty, ny = tx;
-      float along = 0.f;
-      const int max_step = d < 4 ? 14 : 6;
-      for (int step = 1; step <= max_step; step++) {
-        along = smax(along, s_ls[(cy + ty * step) * LE + (cx + tx * step)]);
-        along = smax(along, s_ls[(cy - ty * step) * LE + (cx - tx * step)]);
-      }
-      const float across = smax(s_fs[(cy + ny * 2) * LE + (cx + nx * 2)], s_fs[(cy - ny * 2) * LE + (cx - nx * 2)]);
-      const float thin = 1.f - ssmooth(along * 0.45f, along * 0.95f, across);
-      best = smax(best, along * thin);
+    if (tile_active) {
+      // directions and step counts of core/cpu_accelerator.cpp:4290-4318
+      line_dir<1, 0, 14>(s_ls, s_fs, c, best);
+      line_dir<0, 1, 14>(s_ls, s_fs, c, best);
+      line_dir<1, 1, 14>(s_ls, s_fs, c, best);
+      line_dir<1, -1, 14>(s_ls, s_fs, c, best);
+      line_dir<2, 1, 6>(s_ls, s_fs, c, best);
+      line_dir<1, 2, 6>(s_ls, s_fs, c, best);
+      line_dir<2, -1, 6>(s_ls, s_fs, c, best);
+      line_dir<1, -2, 6>(s_ls, s_fs, c, best);
     }
     const size_t gi = (size_t)y * W + x;
     P.lfs[gi] = best;
@@ -416,11 +448,13 @@ __global__ void __launch_bounds__(256, 3) k_df_main(const float* src, float* dst
   const bool enable_green = k.green != 0;
   const float edge_threshold = k.edge_thr, chroma_threshold = k.chroma_thr, strength = k.strength;
   const float green_strength_scale = sclamp(k.green_scale, 0.f, 1.f);
-  // Pixels that provably keep their input: with green correction off, an
-  // edge weight of exactly zero (both edge factors at or below their lower
-  // smoothstep edges) makes every mask zero, and zero solo blurs make the
-  // solo masks zero, so the output is the input whatever the other planes
-  // hold.  Those pixels read 4 planes instead of 11 and skip the rest.
+  // Pixels that provably keep their input: with green correction off, either
+  // edge factor at or below its lower smoothstep edge zeroes both edge
+  // weights (the other factor is finite, or NaN, and a NaN mask never passes
+  // the cutoff), so no ratio/direct correction applies; zero solo blurs make
+  // the solo masks zero.  The output is then the input whatever the other
+  // planes hold, so those pixels read 4 planes instead of 11 and skip the
+  // rest.
   const float e0_edge = edge_threshold * 0.10f * inv_s;
   const float e0_raw = 0.20f * inv_s;
   const bool can_skip = !enable_green && edge_threshold > 0.f;  // smoothstep edges strictly ordered
@@ -428,7 +462,7 @@ __global__ void __launch_bounds__(256, 3) k_df_main(const float* src, float* dst
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const float s0 = src[i * 3 + 0], s1 = src[i * 3 + 1], s2 = src[i * 3 + 2];
     float d0 = s0, d1 = s1, d2 = s2;
-    if (can_skip && P.be[i] <= e0_edge && P.ber[i] <= e0_raw && P.srb[i] == 0.f && P.sbb[i] == 0.f) {
+    if (can_skip && (P.be[i] <= e0_edge || P.ber[i] <= e0_raw) && P.srb[i] == 0.f && P.sbb[i] == 0.f) {
       dst[i * 3 + 0] = d0;
       dst[i * 3 + 1] = d1;
       dst[i * 3 + 2] = d2;
