@@ -403,6 +403,8 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }
+        if world == 1 and not args.no_xtrans:
+            line["xtrans"] = run_xtrans(args, acc, stream)
         if world == 1 and not args.no_batch:
             line["batched"] = run_batched(args, acc)
         if world == 1 and not args.no_serve:
@@ -520,6 +522,55 @@ def run_batched(args, acc):
         "d2h_bytes_per_step": int(sum(h * w * 6 for _, h, w, _, _ in specs)),
         "workload": "32 Bayer images (sizes/CFA/WB by seeds 100..131), AMaZE->defringe->axial CA, u16 out; "
                     "host page-locked buffers in/out, timed per whole batch",
+    }
+
+
+def run_xtrans(args, acc, stream):
+    """The X-Trans workload: a 6240x4160 mosaic (standard 6x6 CFA) with radial
+    lateral CA injected (R x1.0008, B x0.9992), 3-pass X-Trans demosaic ->
+    pyramidal LK lateral CA (cell 96, 3 levels, 3 iterations, max shift 6,
+    min confidence 0.02), float32 RGB out; device-resident, CUDA events on
+    the library's stream."""
+    import torch
+
+    import libraw_enhanced_b200 as lre
+    from libraw_enhanced_b200 import scenes
+
+    h, w = 4160, 6240
+    d_mos = scenes.xtrans_lateral_ca_torch(3, h, w)
+    d_out = torch.empty((h, w, 3), dtype=torch.float32, device=d_mos.device)
+    d_tmp = torch.empty_like(d_out)
+    acc.set_stream(stream.cuda_stream)
+    p = lre.develop_params(cfa=scenes.XTRANS_STD, cam_mul=(1.8, 1.0, 1.6, 1.0), xtrans_passes=3,
+                           lateral_ca_correction=1, lateral_ca_cell_size=96, lateral_ca_pyramid_levels=3,
+                           lateral_ca_max_iterations=3, lateral_ca_max_shift=6.0, lateral_ca_min_confidence=0.02)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    reps = max(3, min(args.steps, 10))
+    ms = timed(lambda: acc.dev_develop(d_mos, d_out, w, h, p), reps)
+    st = {
+        "xtrans_3pass": timed(lambda: acc.dev_demosaic_xtrans(d_mos, d_tmp, w, h, scenes.XTRANS_STD, 1.0, 3), 3),
+        "lateral_ca": timed(lambda: acc.dev_ca_register_lateral(d_tmp, d_out, w, h, 96, 3, 6.0, 0.02, 3), 3),
+    }
+    mp = h * w / 1e6
+    return {
+        "value": round(mp / (ms / 1e3), 2),
+        "unit": "MP/s",
+        "ms_per_image": round(ms, 3),
+        "stage_ms": {k: round(v, 3) for k, v in st.items()},
+        "workload": "6240x4160 X-Trans (radial lateral CA injected): 3-pass demosaic -> pyramidal LK lateral CA, "
+                    "f32 RGB out, device-resident",
     }
 
 
@@ -656,6 +707,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the 32-image batched develop")
     ap.add_argument("--no-serve", action="store_true", help="skip the request-server sweep")
+    ap.add_argument("--no-xtrans", action="store_true", help="skip the X-Trans + lateral CA workload")
     ap.add_argument("--size", default=None, help="WxH of a reduced case (profiling); default 8736x5856")
     args = ap.parse_args()
     if args.size:

@@ -29,6 +29,8 @@ namespace {
 constexpr int XTS = 114;
 constexpr int NDIR = 8;
 constexpr int XT_THREADS = 256;
+constexpr int kXtCtasPerSm = 4;
+constexpr int kXtMaxCtas = 148 * kXtCtasPerSm;
 
 struct XtParams {
   char xt[6][6];
@@ -213,14 +215,29 @@ __global__ void k_xtrans_1pass(XtArgs A) {
 }
 
 // --------------------------------------------------------- 3-pass
-__global__ void __launch_bounds__(XT_THREADS) k_xtrans_3pass(XtArgs A) {
+__global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArgs Ain) {
   const int ts = XTS;
   const int tid = threadIdx.x, nth = blockDim.x;
+  // The pattern tables are indexed at run time; read from the kernel's
+  // parameter block that would force a local-memory copy of it per thread,
+  // so one copy goes to shared memory (constant-offset parameter loads).
+  __shared__ XtArgs sA;
+  {
+    constexpr int NW = (int)(sizeof(XtArgs) / 4);
+    const int* from = reinterpret_cast<const int*>(&Ain);
+    int* to = reinterpret_cast<int*>(&sA);
+#pragma unroll
+    for (int k = 0; k < NW; k++)
+      if (k % XT_THREADS == tid) to[k] = from[k];
+  }
+  __syncthreads();
+  const XtArgs& A = sA;
   const XtParams& P = A.P;
   XtSlab S = make_xt_slab(A.scratch + (size_t)blockIdx.x * kXtSlabBytes);
   __shared__ int s_tile;
   const int W = A.W, H = A.H;
   const int dirv[4] = {1, ts, ts + 1, ts - 1};
+  bool zeroed_once = false;
 
   for (;;) {
     if (tid == 0) s_tile = atomicAdd(A.tile_counter, 1);
@@ -233,11 +250,17 @@ __global__ void __launch_bounds__(XT_THREADS) k_xtrans_3pass(XtArgs A) {
     const int mrow_g = min(top + ts, H - 3);  // global row bound of the computations
     const int mcol_g = min(left + ts, W - 3);
 
-    // fresh scratch (zeros)
-    {
+    // Fresh scratch (zeros) for tiles on the image border: only their
+    // outputs read positions the tile never computes (the homogeneity maps
+    // of the first/last tile rows and columns); an interior tile writes
+    // every position before reading it, so its slab needs no clearing.
+    const bool border_tile = tile / A.n_left == 0 || tile / A.n_left == A.n_top - 1 || tile % A.n_left == 0 ||
+                             tile % A.n_left == A.n_left - 1;
+    if (border_tile || !zeroed_once) {
       float4* z = reinterpret_cast<float4*>(S.rgb);
       const size_t n4 = kXtSlabBytes / 16;
       for (size_t i = tid; i < n4; i += nth) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      zeroed_once = true;
     }
     __syncthreads();
     float* rgb = S.rgb;
@@ -614,7 +637,7 @@ XtParams make_xt_params(const char* xtrans, int width) {
 size_t ws_bytes_xtrans(size_t w, size_t h, int passes) {
   (void)w;
   (void)h;
-  return passes == 1 ? 0 : 148u * kXtSlabBytes + 4096;
+  return passes == 1 ? 0 : (size_t)kXtMaxCtas * kXtSlabBytes + 4096;
 }
 
 lre_status launch_xtrans(Context* c, const float* raw, int cstride, float* rgb, size_t w, size_t h, const char* xtrans,
@@ -646,7 +669,9 @@ lre_status launch_xtrans(Context* c, const float* raw, int cstride, float* rgb, 
   A.n_left = n_left;
   const int tiles = n_top * n_left;
   if (tiles > 0) {
-    int nblk = std::min(tiles, c->sm_count);
+    // several tiles in flight per SM: the row scans keep only ~114 threads
+    // of a CTA busy, so more CTAs hide the slab's memory latency
+    int nblk = std::min(std::min(tiles, c->sm_count * kXtCtasPerSm), kXtMaxCtas);
     A.scratch = reinterpret_cast<unsigned char*>(c->ws.take((size_t)nblk * kXtSlabBytes));
     A.tile_counter = reinterpret_cast<int*>(c->ws.take(256));
     if (!A.scratch || !A.tile_counter) return fail(c, LRE_ERR_OUT_OF_MEMORY, "demosaic_xtrans_3pass: workspace too small");

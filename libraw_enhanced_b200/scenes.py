@@ -285,3 +285,35 @@ def mosaic_upscaled_torch(seed: int, h: int, w: int, cfa, wb, base=(512, 768), d
     x.clamp_min_(0)
     gains = torch.tensor(list(wb), dtype=torch.float32, device=device)[ii]
     return (x * gains).float().contiguous()
+
+
+def xtrans_lateral_ca_torch(seed: int = 3, h: int = 4160, w: int = 6240, wb=(1.8, 1.0, 1.6, 1.0),
+                            r_scale=1.0008, b_scale=0.9992, base=(1024, 1536), device="cuda"):
+    """The X-Trans lateral-CA workload generated on the GPU: the seeded scene
+    at `base` resolution upscaled bilinearly, R and B scaled radially about
+    the image centre (bilinear, clamp to edge), mosaiced through the standard
+    6x6 X-Trans CFA with Poisson-Gaussian noise and WB.  float32 CUDA (h, w)."""
+    import torch
+    import torch.nn.functional as F
+
+    small = torch.from_numpy(scene_rgb(base[0], base[1], seed)).to(device)
+    big = F.interpolate(small.permute(2, 0, 1)[None], size=(h, w), mode="bilinear", align_corners=False)[0]
+    cy, cx = (h - 1) / 2.0, (w - 1) / 2.0
+    yy = torch.arange(h, device=device, dtype=torch.float32)[:, None]
+    xx = torch.arange(w, device=device, dtype=torch.float32)[None, :]
+    for c, s in ((0, r_scale), (2, b_scale)):
+        sy = (cy + (yy - cy) / s).expand(h, w)
+        sx = (cx + (xx - cx) / s).expand(h, w)
+        grid = torch.stack([sx / (w - 1) * 2 - 1, sy / (h - 1) * 2 - 1], dim=-1)[None]
+        big[c] = F.grid_sample(big[c][None, None], grid, mode="bilinear", padding_mode="border",
+                               align_corners=True)[0, 0]
+    idx = torch.from_numpy(cfa_map(6, 6, XTRANS_STD)).to(device)
+    ii = idx.repeat((h + 5) // 6, (w + 5) // 6)[:h, :w]
+    x = torch.gather(big, 0, ii[None]).squeeze(0).clamp_min_(0)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed + 7919)
+    x = torch.poisson(x * 4000.0, generator=g) / 4000.0
+    x += torch.randn(x.shape, generator=g, device=device) * 0.002
+    x.clamp_min_(0)
+    gains = torch.tensor(list(wb), dtype=torch.float32, device=device)[ii]
+    return (x * gains).float().contiguous()
