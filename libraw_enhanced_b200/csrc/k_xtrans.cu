@@ -28,8 +28,8 @@ namespace {
 
 constexpr int XTS = 114;
 constexpr int NDIR = 8;
-constexpr int XT_THREADS = 256;
-constexpr int kXtCtasPerSm = 4;
+constexpr int XT_THREADS = 128;
+constexpr int kXtCtasPerSm = 8;
 constexpr int kXtMaxCtas = 148 * kXtCtasPerSm;
 
 struct XtParams {
