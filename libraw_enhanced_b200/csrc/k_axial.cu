@@ -394,8 +394,8 @@ cudaError_t axial_dispatch(int T, int NT, size_t w, size_t h, cudaStream_t s, co
 // then forms the horizontal window sums of 4 adjacent output columns, sliding
 // across them.  Every pixel's statistics are computed once, all sums are in
 // double, and HBM carries the a/b planes between the two box levels.
-//   pass A: G, G^2, R, G R, B, G B -> a_R, b_R, a_B, b_B (float planes)
-//   pass B: a_R, b_R, a_B, b_B, |grad G| -> blended output
+//   pass A: G, G^2, R, G R, B, G B -> a_R, b_R, a_B, b_B, |grad G| (float planes)
+//   pass B: box means of those five -> blended output
 // Window sums use the same truncated windows, area reciprocals and float /
 // double conversions as the fused kernel; only the summation order differs.
 constexpr int AXS_PER_LANE = 4;  // output columns per lane in the horizontal pass
@@ -463,7 +463,8 @@ __device__ __forceinline__ void strip_hsum(double (*Vs)[vs_len<WS>()], int r, do
 template <int WS>
 __global__ void __launch_bounds__(32) k_ax_ab(const float* __restrict__ src, int W, int H, int r, float eps, int HS,
                                              const float* __restrict__ d_maxg, float* __restrict__ aR,
-                                             float* __restrict__ bR, float* __restrict__ aB, float* __restrict__ bB) {
+                                             float* __restrict__ bR, float* __restrict__ aB, float* __restrict__ bB,
+                                             float* __restrict__ er) {
   constexpr int NQ = 6;
   static_assert(WS == 32 * AXS_PER_LANE, "one warp covers the strip");
   __shared__ double Vs[NQ][vs_len<WS>()];
@@ -499,6 +500,14 @@ __global__ void __launch_bounds__(32) k_ax_ab(const float* __restrict__ src, int
       const double mi = hs[0][k] * ia;
       const double vi = hs[1][k] * ia - mi * mi;
       const size_t o = (size_t)y * W + x;
+      // |central gradient of G| (interior pixels), boxed by pass B
+      float e = 0.f;
+      if (x >= 1 && x < W - 1 && y >= 1 && y < H - 1) {
+        const float gxv = src[(o + 1) * 3 + 1] * inv_norm - src[(o - 1) * 3 + 1] * inv_norm;
+        const float gyv = src[(o + W) * 3 + 1] * inv_norm - src[(o - W) * 3 + 1] * inv_norm;
+        e = sqrtf(gxv * gxv + gyv * gyv);
+      }
+      er[o] = e;
 #pragma unroll
       for (int ch = 0; ch < 2; ch++) {
         const double mp = hs[2 + 2 * ch][k] * ia, mIp = hs[3 + 2 * ch][k] * ia;
@@ -516,7 +525,8 @@ template <int WS>
 __global__ void __launch_bounds__(32) k_ax_q(const float* __restrict__ src, float* __restrict__ dst, int W, int H,
                                             int r, float strength, int HS, const float* __restrict__ d_maxg,
                                             const float* __restrict__ aR, const float* __restrict__ bR,
-                                            const float* __restrict__ aB, const float* __restrict__ bB) {
+                                            const float* __restrict__ aB, const float* __restrict__ bB,
+                                            const float* __restrict__ er) {
   constexpr int NQ = 5;
   static_assert(WS == 32 * AXS_PER_LANE, "one warp covers the strip");
   __shared__ double Vs[NQ][vs_len<WS>()];
@@ -534,11 +544,7 @@ __global__ void __launch_bounds__(32) k_ax_q(const float* __restrict__ src, floa
       vb = bR[i];
       vc = aB[i];
       vd = bB[i];
-      if (x >= 1 && x < W - 1 && y >= 1 && y < H - 1) {
-        const float gxv = src[(i + 1) * 3 + 1] * inv_norm - src[(i - 1) * 3 + 1] * inv_norm;
-        const float gyv = src[(i + W) * 3 + 1] * inv_norm - src[(i - W) * 3 + 1] * inv_norm;
-        e = sqrtf(gxv * gxv + gyv * gyv);
-      }
+      e = er[i];
     }
     q[0] = (double)va;
     q[1] = (double)vb;
@@ -592,9 +598,10 @@ cudaError_t axial_stream(size_t w, size_t h, int HS, cudaStream_t s, const float
   float* bR = planes + n;
   float* aB = planes + 2 * n;
   float* bB = planes + 3 * n;
+  float* er = planes + 4 * n;
   dim3 grid((unsigned)((w + WS - 1) / WS), (unsigned)((h + HS - 1) / HS));
-  k_ax_ab<WS><<<grid, 32, 0, s>>>(src, (int)w, (int)h, r, eps, HS, d_max, aR, bR, aB, bB);
-  k_ax_q<WS><<<grid, 32, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max, aR, bR, aB, bB);
+  k_ax_ab<WS><<<grid, 32, 0, s>>>(src, (int)w, (int)h, r, eps, HS, d_max, aR, bR, aB, bB, er);
+  k_ax_q<WS><<<grid, 32, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max, aR, bR, aB, bB, er);
   return cudaPeekAtLastError();
 }
 
@@ -602,10 +609,10 @@ cudaError_t axial_stream(size_t w, size_t h, int HS, cudaStream_t s, const float
 
 size_t ws_bytes_axial(size_t w, size_t h, int radius) {
   (void)radius;
-  // the four a/b planes between the two passes, plus an out-of-place copy
+  // the four a/b planes and the edge plane between the two passes, plus an out-of-place copy
   // when the caller runs in place (pass B reads input rows below the rows it
   // writes).
-  return ((w * h * 4 * sizeof(float) + 255) & ~size_t(255)) + w * h * 3 * sizeof(float) + 256;
+  return ((w * h * 5 * sizeof(float) + 255) & ~size_t(255)) + w * h * 3 * sizeof(float) + 256;
 }
 
 lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, size_t h, int radius, float eps,
@@ -613,7 +620,7 @@ lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, si
   if (radius < 1) radius = 1;
   if (radius > 16) return fail(c, LRE_ERR_INVALID_ARGUMENT, "ca_axial_cleanup: radius > 16 is not supported");
   strength = fminf(fmaxf(strength, 0.f), 1.f);
-  float* planes = reinterpret_cast<float*>(c->ws.take(w * h * 4 * sizeof(float)));
+  float* planes = reinterpret_cast<float*>(c->ws.take(w * h * 5 * sizeof(float)));
   if (!planes) return fail(c, LRE_ERR_OUT_OF_MEMORY, "ca_axial_cleanup: workspace too small");
   const float* src = in;
   if (in == out) {
