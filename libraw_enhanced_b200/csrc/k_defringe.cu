@@ -218,7 +218,8 @@ __global__ void __launch_bounds__(256) k_df_blur(BlurJob job, GaussTaps taps, in
 // or 4 vertical outputs from operands held in registers.  Tap order and
 // clamping are those of k_df_blur.
 template <int KS, int TB>
-__global__ void __launch_bounds__(256) k_df_blur_fast(BlurJob job, GaussTaps taps, int W, int H, const DfScalars* sc) {
+__device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTaps& taps, int W, int H,
+                                               const DfScalars* sc) {
   constexpr int E = TB + 2 * KS;
   constexpr int LD = E + 1;  // odd row stride: conflict-light row reads
   extern __shared__ __align__(16) float sm_fast[];
@@ -274,6 +275,11 @@ __global__ void __launch_bounds__(256) k_df_blur_fast(BlurJob job, GaussTaps tap
   }
 }
 
+template <int KS, int TB>
+__global__ void __launch_bounds__(256) k_df_blur_fast(BlurJob job, GaussTaps taps, int W, int H, const DfScalars* sc) {
+  blur_fast_body<KS, TB>(job, taps, W, H, sc);
+}
+
 template <int TB>
 lre_status run_blur_fast(Context* c, const BlurJob& job, const GaussTaps& taps, int W, int H, const DfScalars* sc) {
   constexpr int E = TB + 2 * 10;
@@ -291,50 +297,87 @@ struct DfConst {
   int green;
 };
 
+// Fringe-support seed of pixel i (core/cpu_accelerator.cpp:4158-4205).
+__device__ __forceinline__ float support_at(const float* __restrict__ src, size_t i, const DfPlanes& P, const DfConst& k,
+                                            float inv_s, bool enable_green) {
+  const float rg = P.lrg[i];
+  const float bgr = P.lbg[i];
+  const float dr = rg - P.blrg[i];
+  const float db = bgr - P.blbg[i];
+  const float* s = src + i * 3;
+  const float r0 = smax(s[0], 0.f);
+  const float g0 = smax(s[1], 0.f);
+  const float b0 = smax(s[2], 0.f);
+  const float blur_guide = P.bg[i];
+  const float purple_excess = smin(smax(0.f, dr), smax(0.f, db));
+  const float denom_support = smax(blur_guide, 0.05f);
+  const float g_over_min_support = smax(0.f, g0 - smin(r0, b0)) / denom_support;
+  const float green_dom_support = ssmooth(0.010f, 0.060f, g_over_min_support);
+  const float green_excess = smax(smax(0.f, -dr), smax(0.f, -db)) * green_dom_support;
+  const bool is_purple = purple_excess >= green_excess;
+  const float excess_support = is_purple ? purple_excess : green_excess;
+  const float min_dir = is_purple ? smax(0.f, smin(rg, bgr)) : smax(0.f, smin(-rg, -bgr));
+  const float max_dir = is_purple ? smax(1e-4f, smax(rg, bgr)) : smax(1e-4f, smax(-rg, -bgr));
+  const float balance = min_dir / max_dir;
+  const float c_edge = ssmooth(k.edge_thr * 0.35f * inv_s, k.edge_thr * 1.50f * inv_s, P.be[i]) *
+                       ssmooth(0.55f * inv_s, 1.35f * inv_s, P.ber[i]);
+  const float c_bright = ssmooth(0.24f * inv_s, 0.52f * inv_s, blur_guide);
+  const float c_chroma = ssmooth(k.chroma_thr * 0.45f * inv_s, k.chroma_thr * 1.60f * inv_s, excess_support);
+  const float red_strength = smax(0.f, r0 - smax(g0, b0)) / smax(r0, 1e-4f);
+  const float red_blue_balance = b0 / smax(r0, 1e-4f);
+  const float blue_lift = smax(0.f, b0 - g0) / smax(r0 - g0, 1e-4f);
+  const float red_purple = smax(ssmooth(0.55f, 0.78f, red_blue_balance), ssmooth(0.16f, 0.34f, blue_lift));
+  const float red_purple_hue_signal = ssmooth(0.50f, 0.72f, red_blue_balance) * ssmooth(0.24f, 0.42f, blue_lift);
+  const float balanced_hue = ssmooth(0.06f * inv_s, 0.22f * inv_s, min_dir) * ssmooth(0.35f, 0.75f, balance);
+  const float red_purple_hue = is_purple ? smin(1.f, red_purple_hue_signal * 1.50f) *
+                                               ssmooth(0.035f * inv_s, 0.16f * inv_s, min_dir) *
+                                               ssmooth(0.18f, 0.58f, balance)
+                                         : 0.f;
+  const float c_hue = smax(balanced_hue, red_purple_hue);
+  const float natural_guard = 1.f - ssmooth(0.08f, 0.25f, red_strength) * (1.f - red_purple);
+  const float green_enable = (enable_green || is_purple) ? 1.f : 0.f;
+  return c_edge * c_bright * c_hue * c_chroma * natural_guard * green_enable;
+}
+
+// Blur of the five first-stage planes with K3 fused after it: once a tile's
+// blurred planes are written, the same CTA computes the fringe-support seed
+// of the tile's pixels while those values are still in L2.
+template <int KS, int TB>
+__global__ void __launch_bounds__(256) k_df_blur_support(BlurJob job, GaussTaps taps, int W, int H,
+                                                         const DfScalars* sc, const float* __restrict__ src,
+                                                         DfPlanes P, DfConst k) {
+  blur_fast_body<KS, TB>(job, taps, W, H, sc);  // ends with a CTA barrier
+  const float sensitivity = sclamp(sqrtf(smax(k.strength, 1.0f)), 1.0f, 2.5f);
+  const float inv_s = 1.0f / sensitivity;
+  const bool enable_green = k.green != 0;
+  const int x0 = blockIdx.x * TB, y0 = blockIdx.y * TB;
+  for (int i = threadIdx.x; i < TB * TB; i += blockDim.x) {
+    const int gx = x0 + i % TB, gy = y0 + i / TB;
+    if (gx >= W || gy >= H) continue;
+    const size_t gi = (size_t)gy * W + gx;
+    P.fs[gi] = support_at(src, gi, P, k, inv_s, enable_green);
+  }
+}
+
+template <int TB>
+lre_status run_blur_support(Context* c, const BlurJob& job, const GaussTaps& taps, int W, int H, const DfScalars* sc,
+                            const float* src, const DfPlanes& P, const DfConst& k) {
+  constexpr int E = TB + 2 * 10;
+  const size_t smem = ((size_t)E * (E + 1) + (size_t)E * TB) * sizeof(float);
+  LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_df_blur_support<10, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid((W + TB - 1) / TB, (H + TB - 1) / TB);
+  k_df_blur_support<10, TB><<<grid, 256, smem, c->stream>>>(job, taps, W, H, sc, src, P, k);
+  count_launch(c);
+  return check_launch(c, "defringe blur + support");
+}
+
 __global__ void k_df_support(const float* __restrict__ src, int W, int H, DfPlanes P, DfConst k) {
   const float sensitivity = sclamp(sqrtf(smax(k.strength, 1.0f)), 1.0f, 2.5f);
   const float inv_s = 1.0f / sensitivity;
   const bool enable_green = k.green != 0;
   size_t n = (size_t)W * H;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const float rg = P.lrg[i];
-    const float bgr = P.lbg[i];
-    const float dr = rg - P.blrg[i];
-    const float db = bgr - P.blbg[i];
-    const float* s = src + i * 3;
-    const float r0 = smax(s[0], 0.f);
-    const float g0 = smax(s[1], 0.f);
-    const float b0 = smax(s[2], 0.f);
-    const float blur_guide = P.bg[i];
-    const float purple_excess = smin(smax(0.f, dr), smax(0.f, db));
-    const float denom_support = smax(blur_guide, 0.05f);
-    const float g_over_min_support = smax(0.f, g0 - smin(r0, b0)) / denom_support;
-    const float green_dom_support = ssmooth(0.010f, 0.060f, g_over_min_support);
-    const float green_excess = smax(smax(0.f, -dr), smax(0.f, -db)) * green_dom_support;
-    const bool is_purple = purple_excess >= green_excess;
-    const float excess_support = is_purple ? purple_excess : green_excess;
-    const float min_dir = is_purple ? smax(0.f, smin(rg, bgr)) : smax(0.f, smin(-rg, -bgr));
-    const float max_dir = is_purple ? smax(1e-4f, smax(rg, bgr)) : smax(1e-4f, smax(-rg, -bgr));
-    const float balance = min_dir / max_dir;
-    const float c_edge = ssmooth(k.edge_thr * 0.35f * inv_s, k.edge_thr * 1.50f * inv_s, P.be[i]) *
-                         ssmooth(0.55f * inv_s, 1.35f * inv_s, P.ber[i]);
-    const float c_bright = ssmooth(0.24f * inv_s, 0.52f * inv_s, blur_guide);
-    const float c_chroma = ssmooth(k.chroma_thr * 0.45f * inv_s, k.chroma_thr * 1.60f * inv_s, excess_support);
-    const float red_strength = smax(0.f, r0 - smax(g0, b0)) / smax(r0, 1e-4f);
-    const float red_blue_balance = b0 / smax(r0, 1e-4f);
-    const float blue_lift = smax(0.f, b0 - g0) / smax(r0 - g0, 1e-4f);
-    const float red_purple = smax(ssmooth(0.55f, 0.78f, red_blue_balance), ssmooth(0.16f, 0.34f, blue_lift));
-    const float red_purple_hue_signal = ssmooth(0.50f, 0.72f, red_blue_balance) * ssmooth(0.24f, 0.42f, blue_lift);
-    const float balanced_hue = ssmooth(0.06f * inv_s, 0.22f * inv_s, min_dir) * ssmooth(0.35f, 0.75f, balance);
-    const float red_purple_hue = is_purple ? smin(1.f, red_purple_hue_signal * 1.50f) *
-                                                 ssmooth(0.035f * inv_s, 0.16f * inv_s, min_dir) *
-                                                 ssmooth(0.18f, 0.58f, balance)
-                                           : 0.f;
-    const float c_hue = smax(balanced_hue, red_purple_hue);
-    const float natural_guard = 1.f - ssmooth(0.08f, 0.25f, red_strength) * (1.f - red_purple);
-    const float green_enable = (enable_green || is_purple) ? 1.f : 0.f;
-    P.fs[i] = c_edge * c_bright * c_hue * c_chroma * natural_guard * green_enable;
-  }
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    P.fs[i] = support_at(src, i, P, k, inv_s, enable_green);
 }
 
 // ---------------------------------------------------------------- K5
@@ -817,11 +860,15 @@ lre_status launch_defringe(Context* c, const float* in, float* out, size_t w, si
   j1.in[2] = P.lbg; j1.mode[2] = BS_PLANE;           j1.out[2] = P.blbg;
   j1.in[3] = P.er;  j1.mode[3] = BS_PLANE_EDGE_NORM; j1.out[3] = P.be;
   j1.in[4] = P.er;  j1.mode[4] = BS_PLANE;           j1.out[4] = P.ber;
-  LRE_TRY(run_blur(c, j1, taps, W, H, sc));
-
-  k_df_support<<<gstream, 256, 0, c->stream>>>(in, W, H, P, k);
-  count_launch(c);
-  LRE_TRY(check_launch(c, "defringe support"));
+  if (taps.ks == 10) {  // radius 10: the register-tiled blur with K3 fused
+    LRE_TRY(c->tune.blur_tile == 64 ? run_blur_support<64>(c, j1, taps, W, H, sc, in, P, k)
+                                    : run_blur_support<32>(c, j1, taps, W, H, sc, in, P, k));
+  } else {
+    LRE_TRY(run_blur(c, j1, taps, W, H, sc));
+    k_df_support<<<gstream, 256, 0, c->stream>>>(in, W, H, P, k);
+    count_launch(c);
+    LRE_TRY(check_launch(c, "defringe support"));
+  }
 
   BlurJob j2{};
   j2.np = 1;
