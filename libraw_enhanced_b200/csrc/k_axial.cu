@@ -629,7 +629,13 @@ lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, si
     LRE_CUDA_TRY(c, cudaMemcpyAsync(tmp, in, w * h * 3 * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
     src = tmp;
   }
-  const int HS = c->tune.axial_rows == 128 ? 128 : 64;
+  // Strip height: enough one-warp strips for ~24 resident warps per SM (the
+  // passes are load-latency bound), but at least 16 rows so the 2r + 1 row
+  // prologue of a strip stays small; capped by the tuning choice.
+  const size_t strips_x = (w + 127) / 128;
+  const size_t want = (size_t)c->sm_count * 24;
+  int HS = c->tune.axial_rows == 128 ? 128 : 64;
+  while (HS > 16 && strips_x * ((h + HS - 1) / HS) < want) HS /= 2;
   LRE_CUDA_TRY(c, axial_stream(w, h, HS, c->stream, src, out, radius, eps, strength, d_max_g, planes));
   count_launch(c, 2);
   return check_launch(c, "ca_axial_cleanup");
