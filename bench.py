@@ -41,6 +41,12 @@ WB = (2.0, 1.0, 1.5, 1.0)
 METRIC = "develop MP/s on 1 B200 (51 MP Bayer: AMaZE->defringe->axial CA->tone map)"
 # algorithmic bytes per output pixel of each stage (float32 RGB = 12 B/px)
 STAGE_BYTES = {"amaze": 16.0, "defringe": 24.0, "axial": 24.0, "tone": 24.0}
+# From one ncu capture of k_amaze at 4096x3072 (profiles/amaze_axial_12mp_full.md):
+# DRAM read+write bytes and executed warp-instructions per output pixel.
+AMAZE_DRAM_BYTES_PER_PX = (109.713152e6 + 900.116224e6) / (4096 * 3072)
+AMAZE_WARP_INST_PER_PX = 883750708 / (4096 * 3072)
+# issue roofline: 148 SMs x 4 schedulers x 1.965 GHz, one warp-instruction per cycle each
+ISSUE_PEAK_G = 148 * 4 * 1.965
 
 
 def load_peaks():
@@ -361,19 +367,30 @@ def run_ours(args):
 
     if rank == 0:
         peak, peak_kind = load_peaks()
-        dom = max(stage_ms, key=stage_ms.get)
-        algo_bytes = STAGE_BYTES[dom] * H * W
-        achieved = algo_bytes / (stage_ms[dom] / 1e3) / 1e9
+        # dominant single kernel: k_amaze (the AMaZE stage is that kernel
+        # plus a 10 us border fill)
+        amaze_ms = stage_ms["amaze"]
+        px = H * W
+        achieved = STAGE_BYTES["amaze"] * px / (amaze_ms / 1e3) / 1e9
+        warp_inst = AMAZE_WARP_INST_PER_PX * px / (amaze_ms / 1e3)
         roof = {
             "bound": "hbm",
-            "stage": dom,
+            "kernel": "k_amaze",
             "achieved": round(achieved, 1),
             "peak": peak,
             "peak_kind": peak_kind,
             "unit": "GB/s",
             "frac": round(achieved / peak, 4),
-            "traffic": None,
-            "algorithmic_bytes_per_px": STAGE_BYTES[dom],
+            "traffic": int(AMAZE_DRAM_BYTES_PER_PX * px),
+            "traffic_source": "ncu dram__bytes_read+write of k_amaze at 4096x3072, scaled by pixel count",
+            "algorithmic_bytes_per_px": STAGE_BYTES["amaze"],
+            "issue": {
+                "bound": "issue",
+                "achieved": round(warp_inst / 1e9, 1),
+                "peak": ISSUE_PEAK_G,
+                "unit": "G warp-inst/s",
+                "frac": round(warp_inst / 1e9 / ISSUE_PEAK_G, 4),
+            },
             "stage_ms": {k: round(v, 3) for k, v in stage_ms.items()},
         }
         line = {
