@@ -249,6 +249,50 @@ lre_status lre_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t widt
 lre_status lre_dev_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t width,
                            size_t height, const lre_develop_params* params);
 
+/* ------------------------------------------------------ on-device ingest */
+/* The LibRaw-side frame description the raw ingest reads (imgdata.sizes and
+ * imgdata.color fields, plus the pipeline's WB and adjust_maximum inputs). */
+typedef struct lre_raw_frame {
+  size_t raw_width, raw_height;   /* raw_image geometry (sizes.raw_width/height)      */
+  size_t raw_pitch;               /* bytes per Bayer raw_image row (sizes.raw_pitch)  */
+  size_t top_margin, left_margin; /* sizes.top_margin / left_margin                   */
+  size_t width, height;           /* visible frame (sizes.width / height)             */
+  int shrink;                     /* 1: half-size frame (iwidth = (width + 1) / 2)     */
+  uint32_t filters;               /* Bayer filters word or LRE_FILTERS_XTRANS         */
+  char xtrans[36];                /* 6x6 X-Trans pattern (filters == X-Trans)          */
+  unsigned cblack[6 + 36];        /* color.cblack: [0..3], [4],[5] pattern size, [6..] */
+  unsigned black;                 /* color.black                                       */
+  unsigned maximum;               /* color.maximum                                     */
+  int green_matching;             /* 1: apply_green_matching (Bayer only)              */
+  float wb[4];                    /* effective WB multipliers (scale_colors)           */
+  float adjust_maximum_thr;       /* params.adjust_maximum_thr; 0: keep `maximum`       */
+  float data_maximum;             /* color.data_maximum; 0: scanned on the device       */
+} lre_raw_frame;
+
+/* raw2image (core/libraw_wrapper.cpp:2299-2438, copy_bayer_image standard
+ * path and copy_xtrans_image): the uint16 raw_image into zero-initialised
+ * uint16[4] pixels (ImageBuffer), each sample in its CFA channel, a Bayer
+ * colour-3 sample also in channel 1; half-size frames keep the last sample
+ * of each 2x2 cell per channel, as the reference's scan order does. */
+lre_status lre_raw2image(lre_ctx* ctx, const uint16_t* raw_image, const lre_raw_frame* frame,
+                         uint16_t* image4);
+/* apply_green_matching (core/libraw_wrapper.cpp:496-585), in place on
+ * uint16[4] pixels; no-op for X-Trans. */
+lre_status lre_green_matching(lre_ctx* ctx, uint16_t* raw4, size_t width, size_t height,
+                              uint32_t filters, unsigned maximum);
+/* process_raw_to_rgb from the decoded raw_image to the developed image
+ * (core/libraw_wrapper.cpp:1477-1853 order): raw2image, black level, green
+ * matching, white balance, adjust_maximum, then the develop chain of
+ * `params` (its filters/xtrans/maximum_value are taken from the frame and
+ * the adopted maximum).  The frame crosses PCIe as 16-bit samples.
+ * *maximum_used (may be NULL) receives the maximum handed to the demosaic. */
+lre_status lre_develop_raw(lre_ctx* ctx, const uint16_t* raw_image, const lre_raw_frame* frame,
+                           void* out, const lre_develop_params* params, float* maximum_used);
+/* Same on device buffers; synchronises the context stream once when the
+ * maximum has to be scanned. */
+lre_status lre_dev_develop_raw(lre_ctx* ctx, const uint16_t* raw_image, const lre_raw_frame* frame,
+                               void* out, const lre_develop_params* params, float* maximum_used);
+
 /* ---------------------------------------------------------------- tuning */
 /* Kernel-shape choices that never change results, only speed. */
 typedef struct lre_tuning {

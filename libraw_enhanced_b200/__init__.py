@@ -47,6 +47,7 @@ __all__ = [
     "Batch",
     "Server",
     "develop_params",
+    "raw_frame",
 ]
 
 # LibRaw `filters` words of the four Bayer layouts.
@@ -317,6 +318,31 @@ class CudaAccelerator:
     def dev_develop(self, mosaic, out, width, height, params: DevelopParams):
         self._check(self._lib.lre_dev_develop(self._h, _dptr(mosaic), _dptr(out), int(width), int(height), C.byref(params)))
 
+    # ------------------------------------------------------------ raw ingest
+    def raw2image(self, raw_image, frame):
+        """raw_image: (raw_height, raw_pitch // 2) uint16 (X-Trans: raw_width)."""
+        r = np.ascontiguousarray(raw_image, dtype=np.uint16)
+        s = 1 if frame.shrink else 0
+        out = np.zeros(((frame.height + s) >> s, (frame.width + s) >> s, 4), np.uint16)
+        self._check(self._lib.lre_raw2image(self._h, _ptr(r), C.byref(frame), _ptr(out)))
+        return out
+
+    def green_matching(self, raw4, filters: int, maximum: int):
+        a = np.ascontiguousarray(raw4, dtype=np.uint16).copy()
+        self._check(self._lib.lre_green_matching(self._h, _ptr(a), a.shape[1], a.shape[0], int(filters), int(maximum)))
+        return a
+
+    def develop_raw(self, raw_image, frame, params: DevelopParams, out=None):
+        """process_raw_to_rgb from the 16-bit raw_image: returns (rgb, maximum_used)."""
+        r = np.ascontiguousarray(raw_image, dtype=np.uint16)
+        s = 1 if frame.shrink else 0
+        h, w = (frame.height + s) >> s, (frame.width + s) >> s
+        if out is None:
+            out = np.empty((h, w, 3), np.float32 if params.output_bits == 32 else np.uint16)
+        m = C.c_float()
+        self._check(self._lib.lre_develop_raw(self._h, _ptr(r), C.byref(frame), _ptr(out), C.byref(params), C.byref(m)))
+        return out, m.value
+
     # ------------------------------------------------------------ tuning
     def set_tuning(self, axial_strip=128, axial_rows=128, blur_tile=64) -> None:
         t = _lib.Tuning(1, int(axial_strip), int(axial_rows), int(blur_tile))
@@ -470,6 +496,31 @@ class Server:
         a, b = C.c_size_t(), C.c_size_t()
         self._check(self._lib.lre_server_memory(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+
+def raw_frame(raw_width, raw_height, width, height, filters, raw_pitch=None, top_margin=0, left_margin=0,
+              shrink=0, xtrans=None, cblack=(), black=0, maximum=65535, green_matching=0, wb=(1.0, 1.0, 1.0, 1.0),
+              adjust_maximum_thr=0.0, data_maximum=0.0) -> "_lib.RawFrame":
+    """A LibRaw-style frame description for the raw ingest entry points."""
+    f = _lib.RawFrame()
+    f.raw_width, f.raw_height = int(raw_width), int(raw_height)
+    f.raw_pitch = int(raw_pitch if raw_pitch is not None else 2 * raw_width)
+    f.top_margin, f.left_margin = int(top_margin), int(left_margin)
+    f.width, f.height = int(width), int(height)
+    f.shrink = int(shrink)
+    f.filters = int(filters)
+    if xtrans is not None:
+        x = np.asarray(xtrans, dtype=np.int8).reshape(36)
+        C.memmove(C.addressof(f) + _lib.RawFrame.xtrans.offset, x.ctypes.data, 36)
+    for i, v in enumerate(cblack):
+        f.cblack[i] = int(v)
+    f.black, f.maximum = int(black), int(maximum)
+    f.green_matching = int(green_matching)
+    for i, v in enumerate(wb):
+        f.wb[i] = float(v)
+    f.adjust_maximum_thr = float(adjust_maximum_thr)
+    f.data_maximum = float(data_maximum)
+    return f
 
 
 def develop_params(**kw) -> DevelopParams:

@@ -67,6 +67,28 @@ class DevelopParams(C.Structure):
     ]
 
 
+class RawFrame(C.Structure):
+    _fields_ = [
+        ("raw_width", C.c_size_t),
+        ("raw_height", C.c_size_t),
+        ("raw_pitch", C.c_size_t),
+        ("top_margin", C.c_size_t),
+        ("left_margin", C.c_size_t),
+        ("width", C.c_size_t),
+        ("height", C.c_size_t),
+        ("shrink", C.c_int),
+        ("filters", C.c_uint32),
+        ("xtrans", C.c_char * 36),
+        ("cblack", C.c_uint * 42),
+        ("black", C.c_uint),
+        ("maximum", C.c_uint),
+        ("green_matching", C.c_int),
+        ("wb", C.c_float * 4),
+        ("adjust_maximum_thr", C.c_float),
+        ("data_maximum", C.c_float),
+    ]
+
+
 class Tuning(C.Structure):
     _fields_ = [("lanes", C.c_int), ("axial_strip", C.c_int), ("axial_rows", C.c_int), ("blur_tile", C.c_int)]
 
@@ -160,6 +182,10 @@ SIGNATURES = {
     "lre_develop_params_default": (None, [C.POINTER(DevelopParams)]),
     "lre_develop": (_st, [_p, _p, _p, _sz, _sz, C.POINTER(DevelopParams)]),
     "lre_dev_develop": (_st, [_p, _p, _p, _sz, _sz, C.POINTER(DevelopParams)]),
+    "lre_raw2image": (_st, [_p, _p, C.POINTER(RawFrame), _p]),
+    "lre_green_matching": (_st, [_p, _p, _sz, _sz, C.c_uint32, C.c_uint]),
+    "lre_develop_raw": (_st, [_p, _p, C.POINTER(RawFrame), _p, C.POINTER(DevelopParams), C.POINTER(_f)]),
+    "lre_dev_develop_raw": (_st, [_p, _p, C.POINTER(RawFrame), _p, C.POINTER(DevelopParams), C.POINTER(_f)]),
     "lre_set_tuning": (_st, [_p, C.POINTER(Tuning)]),
     "lre_get_tuning": (_st, [_p, C.POINTER(Tuning)]),
     "lre_batch_create": (_st, [C.POINTER(BatchConfig), C.POINTER(_p)]),

@@ -156,3 +156,15 @@ size_t develop_ws_bytes(const lre_develop_params& p, size_t w, size_t h);
 lre_status develop_device(Context* c, const float* mosaic, void* out, size_t w, size_t h,
                           const lre_develop_params& p);
 }  // namespace lre
+
+namespace lre {
+// On-device raw ingest (k_ingest.cu).
+size_t raw_image_elems(const lre_raw_frame& f);
+lre_status launch_raw2image(Context* c, const uint16_t* raw, const lre_raw_frame& f, uint16_t* image4);
+lre_status launch_green_matching(Context* c, uint16_t* raw4, const uint16_t* copy, size_t w, size_t h,
+                                 uint32_t filters, unsigned maximum);
+lre_status launch_wb_dense(Context* c, const uint16_t* raw4, float* dense, size_t w, size_t h, const float wb[4],
+                           uint32_t filters, const char* xtrans);
+lre_status launch_cfa_max_dense(Context* c, const float* dense, size_t w, size_t h, uint32_t filters,
+                                const char* xtrans, float* d_out);
+}  // namespace lre

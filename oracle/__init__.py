@@ -76,6 +76,8 @@ _PORT_SIGS = {
     "port_fcol_bayer": (C.c_uint, [C.c_uint, C.c_uint, C.c_uint32]),
     "port_fcol_xtrans": (C.c_uint, [C.c_uint, C.c_uint, _p]),
     "port_black_level": (None, [_p, _sz, _sz, _p, C.c_uint, C.c_uint]),
+    "port_raw2image": (None, [_p, _sz, _sz, _sz, _sz, _sz, _sz, _sz, C.c_int, C.c_uint32, _p, _p]),
+    "port_green_matching": (None, [_p, _sz, _sz, C.c_uint32, C.c_int]),
     "port_white_balance": (None, [_p, _p, _sz, _sz, _p, C.c_uint32, _p]),
     "port_adjust_maximum": (_f, [_p, _sz, _sz, C.c_uint32, _f, C.POINTER(_f), _f]),
     "port_tone_mapping": (None, [_p, _p, _sz, _f]),
@@ -208,6 +210,23 @@ def black_level(raw4, cblack, black, maximum):
     cb = np.zeros(6 + 4104, dtype=np.uint32)
     cb[: len(cblack)] = np.asarray(cblack, dtype=np.uint32)
     port().port_black_level(_ptr(a), a.shape[1], a.shape[0], _ptr(cb), int(black), int(maximum))
+    return a
+
+
+def raw2image(raw, raw_pitch, top_margin, left_margin, width, height, filters, xtrans_pattern=None, shrink=0):
+    """raw: (raw_height, raw_width) uint16 (Bayer rows raw_pitch bytes apart)."""
+    raw = np.ascontiguousarray(raw, dtype=np.uint16)
+    rh, rw = raw.shape
+    iw, ih = (width + shrink) >> shrink, (height + shrink) >> shrink
+    out = np.zeros((ih, iw, 4), np.uint16)
+    port().port_raw2image(_ptr(raw), rw, rh, int(raw_pitch), int(top_margin), int(left_margin), int(width),
+                          int(height), int(shrink), int(filters), _ptr(_xt(xtrans_pattern)), _ptr(out))
+    return out
+
+
+def green_matching(raw4, filters, maximum):
+    a = np.ascontiguousarray(raw4, dtype=np.uint16).copy()
+    port().port_green_matching(_ptr(a), a.shape[1], a.shape[0], int(filters), int(maximum))
     return a
 
 

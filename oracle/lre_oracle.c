@@ -293,3 +293,78 @@ void port_border_interpolate(float* rgb, size_t w, size_t h, uint32_t filters, s
         if (c != f && sum[c + 4] > 0) rgb[(row * w + col) * 3 + c] = sum[c] / sum[c + 4];
     }
 }
+
+/*
+ * core/libraw_wrapper.cpp:2299-2438 (copy_bayer_image standard path and
+ * copy_xtrans_image): raw_image (uint16, raw_width x raw_height, Bayer rows
+ * raw_pitch bytes apart, X-Trans rows raw_width pixels apart) into the
+ * zero-initialised image4 (iwidth x iheight x 4), each sample into its CFA
+ * channel; a Bayer colour-3 sample is also copied into channel 1.  With
+ * shrink = 1 (half size) the four samples of a 2x2 cell land in one pixel in
+ * row-major order, later samples overwriting earlier ones.
+ */
+void port_raw2image(const uint16_t* raw, size_t raw_width, size_t raw_height, size_t raw_pitch,
+                    size_t top_margin, size_t left_margin, size_t width, size_t height, int shrink,
+                    uint32_t filters, const char xtrans[36], uint16_t* image4) {
+  size_t iwidth = (width + shrink) >> shrink, iheight = (height + shrink) >> shrink;
+  memset(image4, 0, iwidth * iheight * 4 * sizeof(uint16_t));
+  int is_xtrans = filters == 9;
+  for (size_t row = 0; row < height && row < raw_height - top_margin; row++)
+    for (size_t col = 0; col < width && col < raw_width - left_margin; col++) {
+      size_t src_row = row + top_margin, src_col = col + left_margin;
+      size_t src_idx = is_xtrans ? src_row * raw_width + src_col : src_row * (raw_pitch / 2) + src_col;
+      size_t dst_row = row >> shrink, dst_col = col >> shrink;
+      if (dst_row >= iheight || dst_col >= iwidth) continue;
+      size_t dst = dst_row * iwidth + dst_col;
+      uint16_t val = raw[src_idx];
+      if (is_xtrans) {
+        image4[dst * 4 + port_fcol_xtrans((unsigned)row, (unsigned)col, xtrans)] = val;
+      } else {
+        unsigned c = port_fcol_bayer_native((unsigned)row, (unsigned)col, filters);
+        image4[dst * 4 + c] = val;
+        if (c == 3) image4[dst * 4 + 1] = val;
+      }
+    }
+}
+
+/*
+ * core/libraw_wrapper.cpp:496-585 (apply_green_matching): at the G2
+ * positions of an RGGB layout (rows 3, 5, ..., columns 2, 4, ...), in flat,
+ * unsaturated areas, scale channel 3 by the ratio of the surrounding G1 and
+ * G2 means.  Reads a copy of the image, writes the image.  No-op for X-Trans.
+ */
+void port_green_matching(uint16_t* img4, size_t w, size_t h, uint32_t filters, int maximum) {
+  if (filters == 9) return;
+  const int margin = 3;
+  const float thr = 0.01f;
+  const int width = (int)w, height = (int)h;
+  uint16_t* img = (uint16_t*)malloc(w * h * 4 * sizeof(uint16_t));
+  if (!img) return;
+  memcpy(img, img4, w * h * 4 * sizeof(uint16_t));
+  for (int j = 1 + 2; j < height - margin; j += 2)
+    for (int i = 0 + 2; i < width - margin; i += 2) {
+      if (j - 1 < 0 || j + 1 >= height || i - 1 < 0 || i + 1 >= width || j - 2 < 0 || j + 2 >= height || i - 2 < 0 ||
+          i + 2 >= width)
+        continue;
+      int o1_1 = img[((j - 1) * width + i - 1) * 4 + 1];
+      int o1_2 = img[((j - 1) * width + i + 1) * 4 + 1];
+      int o1_3 = img[((j + 1) * width + i - 1) * 4 + 1];
+      int o1_4 = img[((j + 1) * width + i + 1) * 4 + 1];
+      int o2_1 = img[((j - 2) * width + i) * 4 + 3];
+      int o2_2 = img[((j + 2) * width + i) * 4 + 3];
+      int o2_3 = img[(j * width + i - 2) * 4 + 3];
+      int o2_4 = img[(j * width + i + 2) * 4 + 3];
+      double m1 = (o1_1 + o1_2 + o1_3 + o1_4) / 4.0;
+      double m2 = (o2_1 + o2_2 + o2_3 + o2_4) / 4.0;
+      double c1 = (abs(o1_1 - o1_2) + abs(o1_1 - o1_3) + abs(o1_1 - o1_4) + abs(o1_2 - o1_3) + abs(o1_3 - o1_4) +
+                   abs(o1_2 - o1_4)) / 6.0;
+      double c2 = (abs(o2_1 - o2_2) + abs(o2_1 - o2_3) + abs(o2_1 - o2_4) + abs(o2_2 - o2_3) + abs(o2_3 - o2_4) +
+                   abs(o2_2 - o2_4)) / 6.0;
+      if ((img[(j * width + i) * 4 + 3] < maximum * 0.95) && (c1 < maximum * thr) && (c2 < maximum * thr) &&
+          (m2 > 0.1)) {
+        float correction = img4[(j * width + i) * 4 + 3] * m1 / m2;
+        img4[(j * width + i) * 4 + 3] = correction > maximum ? (uint16_t)maximum : (uint16_t)correction;
+      }
+    }
+  free(img);
+}
