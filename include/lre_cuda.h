@@ -249,6 +249,42 @@ lre_status lre_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t widt
 lre_status lre_dev_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t width,
                            size_t height, const lre_develop_params* params);
 
+/* GPUAccelerator::demosaic_bayer_linear (core/gpu_accelerator.h:29-32;
+ * core/cpu_accelerator.cpp:74-156): bilinear interpolation of the missing
+ * colours, then the 1-px border interpolation.  Sparse (H,W,3) raw in. */
+lre_status lre_demosaic_bayer_linear(lre_ctx* ctx, const float* raw_rgb, float* rgb, size_t width,
+                                     size_t height, uint32_t filters, float maximum_value);
+/* Same on a dense device mosaic. */
+lre_status lre_dev_demosaic_bayer_linear(lre_ctx* ctx, const float* raw, float* rgb, size_t width,
+                                         size_t height, uint32_t filters, float maximum_value);
+
+/* ------------------------------------------------------ output end */
+/* GPUAccelerator::convert_color_space (core/gpu_accelerator.h:66-69;
+ * core/cpu_accelerator.cpp:2874-2897): out = M[:, :3] * in + M[:, 3] with
+ * the row-major 3x4 matrix `transform`. */
+lre_status lre_convert_color_space(lre_ctx* ctx, const float* in, float* out, size_t width,
+                                   size_t height, const float transform[12]);
+/* GPUAccelerator::gamma_correct (core/gpu_accelerator.h:70-72;
+ * core/cpu_accelerator.cpp:2903-2978): the output colour space's encoding
+ * (1/7 sRGB, 2/3 power 2.222, 4 power 1.8, 8 Rec.2020, otherwise power
+ * `gamma_power` with linear slope `gamma_slope`). */
+lre_status lre_gamma_correct(lre_ctx* ctx, const float* in, float* out, size_t width, size_t height,
+                             float gamma_power, float gamma_slope, int output_color_space);
+lre_status lre_dev_convert_color_space(lre_ctx* ctx, const float* in, float* out, size_t width,
+                                       size_t height, const float transform[12]);
+lre_status lre_dev_gamma_correct(lre_ctx* ctx, const float* in, float* out, size_t width,
+                                 size_t height, float gamma_power, float gamma_slope,
+                                 int output_color_space);
+/* The two above fused with ProcessedImageData.to_numpy's quantisation
+ * (core/python_bindings.cpp:235-257): one pass from linear camera RGB to
+ * 8-bit, 16-bit (or float, bits = 32) output RGB. */
+lre_status lre_output_epilogue(lre_ctx* ctx, const float* in, void* out, size_t width, size_t height,
+                               const float transform[12], float gamma_power, float gamma_slope,
+                               int output_color_space, int bits);
+lre_status lre_dev_output_epilogue(lre_ctx* ctx, const float* in, void* out, size_t width,
+                                   size_t height, const float transform[12], float gamma_power,
+                                   float gamma_slope, int output_color_space, int bits);
+
 /* ------------------------------------------------------ on-device ingest */
 /* The LibRaw-side frame description the raw ingest reads (imgdata.sizes and
  * imgdata.color fields, plus the pipeline's WB and adjust_maximum inputs). */

@@ -166,6 +166,13 @@ class CudaAccelerator:
         )
         return out
 
+    def demosaic_bayer_linear(self, raw_rgb, filters: int, maximum_value: float = 1.0):
+        raw = _rgb(raw_rgb, "demosaic_bayer_linear")
+        out = np.empty_like(raw)
+        self._check(self._lib.lre_demosaic_bayer_linear(self._h, _ptr(raw), _ptr(out), raw.shape[1], raw.shape[0],
+                                                        int(filters), float(maximum_value)))
+        return out
+
     def demosaic_xtrans_1pass(self, raw_rgb, xtrans, color_matrix=None, maximum_value: float = 1.0):
         return self._xtrans(raw_rgb, xtrans, color_matrix, maximum_value, 1)
 
@@ -317,6 +324,33 @@ class CudaAccelerator:
 
     def dev_develop(self, mosaic, out, width, height, params: DevelopParams):
         self._check(self._lib.lre_dev_develop(self._h, _dptr(mosaic), _dptr(out), int(width), int(height), C.byref(params)))
+
+    # ------------------------------------------------------------ output end
+    def convert_color_space(self, image, transform):
+        """GPUAccelerator.convert_color_space: 3x4 row-major matrix."""
+        img = _rgb(image, "convert_color_space")
+        t = np.ascontiguousarray(transform, dtype=np.float32).reshape(12)
+        out = np.empty_like(img)
+        self._check(self._lib.lre_convert_color_space(self._h, _ptr(img), _ptr(out), img.shape[1], img.shape[0], _ptr(t)))
+        return out
+
+    def gamma_correct(self, image, gamma_power=0.0, gamma_slope=0.0, output_color_space=1):
+        img = _rgb(image, "gamma_correct")
+        out = np.empty_like(img)
+        self._check(self._lib.lre_gamma_correct(self._h, _ptr(img), _ptr(out), img.shape[1], img.shape[0],
+                                                float(gamma_power), float(gamma_slope), int(output_color_space)))
+        return out
+
+    def output_epilogue(self, image, transform, gamma_power=0.0, gamma_slope=0.0, output_color_space=1, bits=16):
+        """Colour space + gamma + to_numpy quantisation in one pass."""
+        img = _rgb(image, "output_epilogue")
+        t = np.ascontiguousarray(transform, dtype=np.float32).reshape(12)
+        dt = {8: np.uint8, 16: np.uint16, 32: np.float32}[int(bits)]
+        out = np.empty(img.shape, dt)
+        self._check(self._lib.lre_output_epilogue(self._h, _ptr(img), _ptr(out), img.shape[1], img.shape[0], _ptr(t),
+                                                  float(gamma_power), float(gamma_slope), int(output_color_space),
+                                                  int(bits)))
+        return out
 
     # ------------------------------------------------------------ raw ingest
     def raw2image(self, raw_image, frame):

@@ -182,6 +182,14 @@ SIGNATURES = {
     "lre_develop_params_default": (None, [C.POINTER(DevelopParams)]),
     "lre_develop": (_st, [_p, _p, _p, _sz, _sz, C.POINTER(DevelopParams)]),
     "lre_dev_develop": (_st, [_p, _p, _p, _sz, _sz, C.POINTER(DevelopParams)]),
+    "lre_demosaic_bayer_linear": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _f]),
+    "lre_dev_demosaic_bayer_linear": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _f]),
+    "lre_convert_color_space": (_st, [_p, _p, _p, _sz, _sz, _p]),
+    "lre_gamma_correct": (_st, [_p, _p, _p, _sz, _sz, _f, _f, _i]),
+    "lre_dev_convert_color_space": (_st, [_p, _p, _p, _sz, _sz, _p]),
+    "lre_dev_gamma_correct": (_st, [_p, _p, _p, _sz, _sz, _f, _f, _i]),
+    "lre_output_epilogue": (_st, [_p, _p, _p, _sz, _sz, _p, _f, _f, _i, _i]),
+    "lre_dev_output_epilogue": (_st, [_p, _p, _p, _sz, _sz, _p, _f, _f, _i, _i]),
     "lre_raw2image": (_st, [_p, _p, C.POINTER(RawFrame), _p]),
     "lre_green_matching": (_st, [_p, _p, _sz, _sz, C.c_uint32, C.c_uint]),
     "lre_develop_raw": (_st, [_p, _p, C.POINTER(RawFrame), _p, C.POINTER(DevelopParams), C.POINTER(_f)]),

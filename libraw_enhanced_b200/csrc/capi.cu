@@ -191,6 +191,39 @@ lre_status lre_dev_demosaic_bayer_amaze(lre_ctx* ctx, const float* raw, float* r
   return lre::launch_amaze(c, raw, 1, rgb, w, h, filters, cam_mul, maximum_value);
 }
 
+lre_status lre_dev_demosaic_bayer_linear(lre_ctx* ctx, const float* raw, float* rgb, size_t w, size_t h,
+                                         uint32_t filters, float maximum_value) {
+  Context* c = C(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  LRE_TRY(check_img(c, raw, rgb, w, h, "demosaic_bayer_linear"));
+  if (filters == LRE_FILTERS_XTRANS || filters < 1000)
+    return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "demosaic_bayer_linear: not a Bayer filters word");
+  cudaSetDevice(c->device);
+  LRE_TRY(lre::check_injection(c));
+  return lre::launch_bayer_linear(c, raw, 1, rgb, w, h, filters, maximum_value);
+}
+
+lre_status lre_demosaic_bayer_linear(lre_ctx* ctx, const float* raw_rgb, float* rgb, size_t w, size_t h,
+                                     uint32_t filters, float maximum_value) {
+  Context* c = C(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  LRE_TRY(check_img(c, raw_rgb, rgb, w, h, "demosaic_bayer_linear"));
+  if (filters == LRE_FILTERS_XTRANS || filters < 1000)
+    return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "demosaic_bayer_linear: not a Bayer filters word");
+  std::lock_guard<std::mutex> lk(c->mu);
+  LRE_TRY(begin(c, 0));
+  const size_t bytes = w * h * 3 * sizeof(float);
+  LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, bytes));
+  LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, bytes));
+  float* din = reinterpret_cast<float*>(c->d_in);
+  float* dout = reinterpret_cast<float*>(c->d_out);
+  LRE_CUDA_TRY(c, cudaMemcpyAsync(din, raw_rgb, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::launch_bayer_linear(c, din, 3, dout, w, h, filters, maximum_value));
+  LRE_CUDA_TRY(c, cudaMemcpyAsync(rgb, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return LRE_OK;
+}
+
 lre_status lre_demosaic_bayer_amaze(lre_ctx* ctx, const float* raw_rgb, float* rgb, size_t w, size_t h,
                                     uint32_t filters, const float cam_mul[4], float maximum_value) {
   Context* c = C(ctx);
@@ -355,6 +388,44 @@ lre_status lre_quantize_u16(lre_ctx* ctx, const float* in, uint16_t* out, size_t
 }
 lre_status lre_quantize_u8(lre_ctx* ctx, const float* in, uint8_t* out, size_t n) {
   return quantize_host(ctx, in, out, n, 8);
+}
+
+
+lre_status lre_convert_color_space(lre_ctx* ctx, const float* in, float* out, size_t w, size_t h,
+                                   const float transform[12]) {
+  Context* c = C(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  if (!in || !out || !transform || w == 0 || h == 0)
+    return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "convert_color_space: bad arguments");
+  return host_rgb_stage(c, in, out, w, h, 0, [&](float* d) { return lre::launch_color_space(c, d, d, w * h, transform); });
+}
+
+lre_status lre_gamma_correct(lre_ctx* ctx, const float* in, float* out, size_t w, size_t h, float gamma_power,
+                             float gamma_slope, int output_color_space) {
+  Context* c = C(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  if (!in || !out || w == 0 || h == 0) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "gamma_correct: bad arguments");
+  return host_rgb_stage(c, in, out, w, h, 0, [&](float* d) {
+    return lre::launch_gamma(c, d, d, w * h, gamma_power, gamma_slope, output_color_space);
+  });
+}
+
+lre_status lre_dev_convert_color_space(lre_ctx* ctx, const float* in, float* out, size_t w, size_t h,
+                                       const float transform[12]) {
+  Context* c = C(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  if (!in || !out || !transform) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "convert_color_space: null argument");
+  cudaSetDevice(c->device);
+  return lre::launch_color_space(c, in, out, w * h, transform);
+}
+
+lre_status lre_dev_gamma_correct(lre_ctx* ctx, const float* in, float* out, size_t w, size_t h, float gamma_power,
+                                 float gamma_slope, int output_color_space) {
+  Context* c = C(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  if (!in || !out) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "gamma_correct: null argument");
+  cudaSetDevice(c->device);
+  return lre::launch_gamma(c, in, out, w * h, gamma_power, gamma_slope, output_color_space);
 }
 
 }  // extern "C"

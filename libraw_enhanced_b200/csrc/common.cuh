@@ -83,5 +83,6 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 // downstream match the CPU far more often than with single-precision logf.
 __device__ __forceinline__ float log_cr(float x) { return (float)log((double)x); }
 __device__ __forceinline__ float exp_cr(float x) { return (float)exp((double)x); }
+__device__ __forceinline__ float pow_cr(float x, float y) { return (float)pow((double)x, (double)y); }
 
 }  // namespace lre

@@ -938,11 +938,16 @@ lre_status launch_amaze(Context* c, const float* raw, int cstride, float* rgb, s
   LRE_CUDA_TRY(c, cudaMemsetAsync(A.tile_counter, 0, sizeof(int), c->stream));
   LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_amaze, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
   k_amaze<<<nblk, AMZ_THREADS, kSmemBytes, c->stream>>>(A);
-  const int band = 4;
-  const long long nb = 2LL * band * (long long)w + 2LL * band * (long long)(h > 8 ? h - 8 : 0);
+  count_launch(c);
+  LRE_TRY(check_launch(c, "demosaic_bayer_amaze"));
+  return launch_border_interp(c, rgb, w, h, filters, 4);
+}
+
+lre_status launch_border_interp(Context* c, float* rgb, size_t w, size_t h, uint32_t filters, int band) {
+  const long long nb = 2LL * band * (long long)w + 2LL * band * (long long)(h > (size_t)(2 * band) ? h - 2 * band : 0);
   k_border_interp<<<grid_for((size_t)nb, 256, c->sm_count * 2), 256, 0, c->stream>>>(rgb, (int)w, (int)h, filters, band);
-  count_launch(c, 2);
-  return check_launch(c, "demosaic_bayer_amaze");
+  count_launch(c);
+  return check_launch(c, "border_interpolate");
 }
 
 }  // namespace lre

@@ -168,3 +168,20 @@ lre_status launch_wb_dense(Context* c, const uint16_t* raw4, float* dense, size_
 lre_status launch_cfa_max_dense(Context* c, const float* dense, size_t w, size_t h, uint32_t filters,
                                 const char* xtrans, float* d_out);
 }  // namespace lre
+
+namespace lre {
+// Output end of the pipeline (k_output.cu).
+lre_status launch_color_space(Context* c, const float* in, float* out, size_t n_px, const float transform[12]);
+lre_status launch_gamma(Context* c, const float* in, float* out, size_t n_px, float gamma_power, float gamma_slope,
+                        int color_space);
+lre_status launch_output_epilogue(Context* c, const float* in, void* out, size_t n_px, const float transform[12],
+                                  float gamma_power, float gamma_slope, int color_space, int bits);
+}  // namespace lre
+
+namespace lre {
+// LibRaw border interpolation of the `band`-px frame (k_amaze.cu) and the
+// bilinear Bayer demosaic (k_linear.cu).
+lre_status launch_border_interp(Context* c, float* rgb, size_t w, size_t h, uint32_t filters, int band);
+lre_status launch_bayer_linear(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
+                               uint32_t filters, float maximum_value);
+}  // namespace lre

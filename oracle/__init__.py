@@ -61,9 +61,12 @@ _REF_SIGS = {
     "ref_num_threads": (C.c_int, []),
     "ref_set_num_threads": (None, [C.c_int]),
     "ref_demosaic_bayer_amaze": (C.c_int, [_p, _p, _sz, _sz, C.c_uint32, _p, _f]),
+    "ref_demosaic_bayer_linear": (C.c_int, [_p, _p, _sz, _sz, C.c_uint32, _f]),
     "ref_demosaic_xtrans": (C.c_int, [_p, _p, _sz, _sz, _p, _p, _f, C.c_int]),
     "ref_apply_white_balance": (C.c_int, [_p, _p, _sz, _sz, _p, C.c_uint32, _p]),
     "ref_tone_mapping": (C.c_int, [_p, _p, _sz, _sz, _f]),
+    "ref_convert_color_space": (C.c_int, [_p, _p, _sz, _sz, _p]),
+    "ref_gamma_correct": (C.c_int, [_p, _p, _sz, _sz, _f, _f, C.c_int]),
     "ref_enhance_micro_contrast": (C.c_int, [_p, _p, _sz, _sz, _f, _f, _f, _p]),
     "ref_defringe": (C.c_int, [_p, _p, _sz, _sz, _f, _f, _f, _f, C.c_int, _f]),
     "ref_ca_register_lateral": (C.c_int, [_p, _p, _sz, _sz, C.c_int, C.c_int, _f, _f, C.c_int]),
@@ -136,6 +139,14 @@ def amaze(raw_sparse, filters, cam_mul=(2.0, 1.0, 1.5, 1.0), maximum=1.0):
     return out
 
 
+def bayer_linear(raw_sparse, filters, maximum=1.0):
+    raw = _img(raw_sparse)
+    h, w, _ = raw.shape
+    out = np.zeros_like(raw)
+    assert ref().ref_demosaic_bayer_linear(_ptr(raw), _ptr(out), w, h, int(filters), float(maximum))
+    return out
+
+
 def xtrans(raw_sparse, xtrans_pattern, passes=3, maximum=1.0, color_matrix=None):
     raw = _img(raw_sparse)
     h, w, _ = raw.shape
@@ -200,6 +211,22 @@ def axial_ca(img, radius=6, eps=1e-4, strength=0.3):
     a = _img(img)
     out = np.empty_like(a)
     assert ref().ref_ca_axial_cleanup(_ptr(a), _ptr(out), a.shape[1], a.shape[0], int(radius), float(eps), float(strength))
+    return out
+
+
+def convert_color_space(img, transform):
+    a = _img(img)
+    out = np.empty_like(a)
+    t = np.ascontiguousarray(transform, dtype=np.float32).reshape(12)
+    assert ref().ref_convert_color_space(_ptr(a), _ptr(out), a.shape[1], a.shape[0], _ptr(t))
+    return out
+
+
+def gamma_correct(img, gamma_power=0.0, gamma_slope=0.0, color_space=1):
+    a = _img(img)
+    out = np.empty_like(a)
+    assert ref().ref_gamma_correct(_ptr(a), _ptr(out), a.shape[1], a.shape[0], float(gamma_power), float(gamma_slope),
+                                   int(color_space))
     return out
 
 

@@ -95,6 +95,14 @@ int ref_demosaic_bayer_amaze(const float* raw, float* rgb, size_t w, size_t h, u
   return accel().demosaic_bayer_amaze(in, out, filters, cm, maximum_value) ? 1 : 0;
 }
 
+/* core/cpu_accelerator.cpp:74-156 (bilinear Bayer demosaic + border(1)) */
+int ref_demosaic_bayer_linear(const float* raw, float* rgb, size_t w, size_t h, uint32_t filters,
+                              float maximum_value) {
+  MuteCout m;
+  ImageBufferFloat in = fbuf(raw, w, h), out = fbuf(rgb, w, h);
+  return accel().demosaic_bayer_linear(in, out, filters, maximum_value) ? 1 : 0;
+}
+
 /* core/cpu_accelerator.cpp:2767-2784 (X-Trans 1-pass / 3-pass) */
 int ref_demosaic_xtrans(const float* raw, float* rgb, size_t w, size_t h, const char xtrans[36],
                         const float color_matrix[12], float maximum_value, int passes) {
@@ -129,6 +137,23 @@ int ref_tone_mapping(const float* in, float* out, size_t w, size_t h, float afte
   MuteCout m;
   ImageBufferFloat a = fbuf(in, w, h), b = fbuf(out, w, h);
   return accel().tone_mapping(a, b, after_scale) ? 1 : 0;
+}
+
+/* core/cpu_accelerator.cpp:2874-2897 (convert_color_space, 3x4 matrix) */
+int ref_convert_color_space(const float* in, float* out, size_t w, size_t h, const float transform[12]) {
+  MuteCout m;
+  ImageBufferFloat a = fbuf(in, w, h), b = fbuf(out, w, h);
+  float t[3][4];
+  for (int i = 0; i < 12; i++) t[i / 4][i % 4] = transform[i];
+  return accel().convert_color_space(a, b, t) ? 1 : 0;
+}
+
+/* core/cpu_accelerator.cpp:2903-2978 (gamma_correct) */
+int ref_gamma_correct(const float* in, float* out, size_t w, size_t h, float gamma_power, float gamma_slope,
+                      int output_color_space) {
+  MuteCout m;
+  ImageBufferFloat a = fbuf(in, w, h), b = fbuf(out, w, h);
+  return accel().gamma_correct(a, b, gamma_power, gamma_slope, output_color_space) ? 1 : 0;
 }
 
 /* core/cpu_accelerator.cpp:3130-3319 (micro-contrast) */
