@@ -72,6 +72,11 @@ class CudaAccelerator {
   const std::string& last_error() const { return err_; }
   lre_ctx* context() const { return ctx_; }
 
+  bool demosaic_bayer_linear(const ImageBufferFloat& raw, ImageBufferFloat& rgb, uint32_t filters,
+                             float maximum_value) {
+    if (!same(raw, rgb)) return bad("demosaic_bayer_linear: buffer size mismatch");
+    return ok(lre_demosaic_bayer_linear(ctx_, f(raw), f(rgb), raw.width, raw.height, filters, maximum_value));
+  }
   bool demosaic_bayer_amaze(const ImageBufferFloat& raw, ImageBufferFloat& rgb, uint32_t filters,
                             const float (&cam_mul)[4], float maximum_value) {
     if (!same(raw, rgb)) return bad("demosaic_bayer_amaze: mismatched buffers");
@@ -95,6 +100,15 @@ class CudaAccelerator {
       return bad("apply_white_balance: invalid buffers");
     return ok(lre_apply_white_balance(ctx_, &raw.image[0][0], &rgb.image[0][0], raw.width, raw.height, wb, filters,
                                       xtrans ? &xtrans[0][0] : nullptr));
+  }
+  bool convert_color_space(const ImageBufferFloat& in, ImageBufferFloat& out, const float transform[3][4]) {
+    if (!same(in, out)) return bad("convert_color_space: buffer size mismatch");
+    return ok(lre_convert_color_space(ctx_, f(in), f(out), in.width, in.height, &transform[0][0]));
+  }
+  bool gamma_correct(const ImageBufferFloat& in, ImageBufferFloat& out, float gamma_power, float gamma_slope,
+                     int output_color_space) {
+    if (!same(in, out)) return bad("gamma_correct: buffer size mismatch");
+    return ok(lre_gamma_correct(ctx_, f(in), f(out), in.width, in.height, gamma_power, gamma_slope, output_color_space));
   }
   bool tone_mapping(const ImageBufferFloat& in, ImageBufferFloat& out, float after_scale) {
     if (!same(in, out)) return bad("tone_mapping: mismatched buffers");
