@@ -554,7 +554,7 @@ def run_xtrans(args, acc, stream):
     import libraw_enhanced_b200 as lre
     from libraw_enhanced_b200 import scenes
 
-    h, w = 4160, 6240
+    w, h = (int(v) for v in args.xtrans_size.lower().split("x"))
     d_mos = scenes.xtrans_lateral_ca_torch(3, h, w)
     d_out = torch.empty((h, w, 3), dtype=torch.float32, device=d_mos.device)
     d_tmp = torch.empty_like(d_out)
@@ -587,7 +587,7 @@ def run_xtrans(args, acc, stream):
         "unit": "MP/s",
         "ms_per_image": round(ms, 3),
         "stage_ms": {k: round(v, 3) for k, v in st.items()},
-        "workload": "6240x4160 X-Trans (radial lateral CA injected): 3-pass demosaic -> pyramidal LK lateral CA, "
+        "workload": f"{w}x{h} X-Trans (radial lateral CA injected): 3-pass demosaic -> pyramidal LK lateral CA, "
                     "f32 RGB out, device-resident",
     }
 
@@ -726,6 +726,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the 32-image batched develop")
     ap.add_argument("--no-serve", action="store_true", help="skip the request-server sweep")
     ap.add_argument("--no-xtrans", action="store_true", help="skip the X-Trans + lateral CA workload")
+    ap.add_argument("--xtrans-size", default="6240x4160", help="WxH of the X-Trans workload (reduced cases: profiling)")
     ap.add_argument("--size", default=None, help="WxH of a reduced case (profiling); default 8736x5856")
     args = ap.parse_args()
     if args.size:

@@ -252,8 +252,9 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
 
     // Fresh scratch (zeros) for tiles on the image border: only their
     // outputs read positions the tile never computes (the homogeneity maps
-    // of the first/last tile rows and columns); an interior tile writes
-    // every position before reading it, so its slab needs no clearing.
+    // of the first/last tile rows and columns).  Interior tiles clear only
+    // direction plane 0, as the reference does for every tile; they write
+    // every other position before reading it.
     const bool border_tile = tile / A.n_left == 0 || tile / A.n_left == A.n_top - 1 || tile % A.n_left == 0 ||
                              tile % A.n_left == A.n_left - 1;
     if (border_tile || !zeroed_once) {
@@ -261,6 +262,10 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
       const size_t n4 = kXtSlabBytes / 16;
       for (size_t i = tid; i < n4; i += nth) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
       zeroed_once = true;
+    } else {
+      // direction plane 0 is cleared for every tile (:2058)
+      float4* z = reinterpret_cast<float4*>(S.rgb);
+      for (int i = tid; i < XTS * XTS * 3 / 4; i += nth) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
     float* rgb = S.rgb;
@@ -308,12 +313,23 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
       RGB(0, lr, lc)[xfc(P, row, col)] = xraw(A, row, col);
     }
     __syncthreads();
-    // copy direction 0 to 1..3, all but the last float (:2067-2069)
-    for (int i = tid; i < ts * ts * 3 - 1; i += nth) {
-      const float v = rgb[i];
-      rgb[(size_t)1 * ts * ts * 3 + i] = v;
-      rgb[(size_t)2 * ts * ts * 3 + i] = v;
-      rgb[(size_t)3 * ts * ts * 3 + i] = v;
+    // copy direction 0 to 1..3, all but the last float (:2067-2069); the
+    // planes are 16-byte aligned (ts*ts*3 floats apart), so 4 floats a step
+    {
+      constexpr int NF = XTS * XTS * 3 - 1;
+      const float4* s4 = reinterpret_cast<const float4*>(rgb);
+      for (int i = tid; i < NF / 4; i += nth) {
+        const float4 v = s4[i];
+        reinterpret_cast<float4*>(rgb + (size_t)1 * XTS * XTS * 3)[i] = v;
+        reinterpret_cast<float4*>(rgb + (size_t)2 * XTS * XTS * 3)[i] = v;
+        reinterpret_cast<float4*>(rgb + (size_t)3 * XTS * XTS * 3)[i] = v;
+      }
+      for (int i = (NF / 4) * 4 + tid; i < NF; i += nth) {
+        const float v = rgb[i];
+        rgb[(size_t)1 * XTS * XTS * 3 + i] = v;
+        rgb[(size_t)2 * XTS * XTS * 3 + i] = v;
+        rgb[(size_t)3 * XTS * XTS * 3 + i] = v;
+      }
     }
     __syncthreads();
     // (b) green in 4 directions (:2071-2127), one row per thread
@@ -357,8 +373,11 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
     for (int pass = 0; pass < 3; pass++) {
       if (pass == 1) {
         // copy directions 0..3 into 4..7, all but the last float (:2131-2136)
-        const size_t n = (size_t)4 * ts * ts * 3 - 1;
-        for (size_t i = tid; i < n; i += nth) S.rgb[(size_t)4 * ts * ts * 3 + i] = S.rgb[i];
+        constexpr int NF = 4 * XTS * XTS * 3 - 1;
+        const float4* s4 = reinterpret_cast<const float4*>(S.rgb);
+        float4* d4 = reinterpret_cast<float4*>(S.rgb + (size_t)4 * XTS * XTS * 3);
+        for (int i = tid; i < NF / 4; i += nth) d4[i] = s4[i];
+        for (int i = (NF / 4) * 4 + tid; i < NF; i += nth) S.rgb[(size_t)4 * XTS * XTS * 3 + i] = S.rgb[i];
         __syncthreads();
         rgb = S.rgb + (size_t)4 * ts * ts * 3;
       }
@@ -406,9 +425,17 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
       {
         const int sgstartcol = (left - P.sgcol + 4) / 3 * 3 + P.sgcol;
         const int row0 = (top - P.sgrow + 4) / 3 * 3 + P.sgrow;
-        for (int row = row0 + 3 * tid; row < mrow_g - 2; row += 3 * nth) {
+        // One solitary green per thread: along a row the scan toggles h once
+        // per site (its inner loops toggle it an even number of times), so
+        // the k-th site starts from h0 ^ 2 (k & 1); sites are independent.
+        const int nrow = row0 < mrow_g - 2 ? (mrow_g - 2 - row0 + 2) / 3 : 0;
+        const int ncol = sgstartcol < mcol_g - 2 ? (mcol_g - 2 - sgstartcol + 2) / 3 : 0;
+        for (int item = tid; item < nrow * ncol; item += nth) {
+          const int row = row0 + 3 * (item / ncol), k = item % ncol;
+          const int col = sgstartcol + 3 * k;
           float color[3][6];
-          for (int col = sgstartcol, h = xfc(P, row, col + 1); col < mcol_g - 2; col += 3, h ^= 2) {
+          {
+            int h = xfc(P, row, sgstartcol + 1) ^ ((k & 1) << 1);
             float* rix = RGB(0, row - top, col - left);
             float diff[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             for (int i = 1, d = 0; d < 6; d++, i ^= ts ^ 1, h ^= 2) {
