@@ -215,6 +215,7 @@ __global__ void k_xtrans_1pass(XtArgs A) {
 }
 
 // --------------------------------------------------------- 3-pass
+template <bool SITES>
 __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArgs Ain) {
   const int ts = XTS;
   const int tid = threadIdx.x, nth = blockDim.x;
@@ -332,14 +333,18 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
       }
     }
     __syncthreads();
-    // (b) green in 4 directions (:2071-2127), one row per thread
-    for (int row = top + tid; row < mrow_g; row += nth) {
-      int leftstart = left;
-      for (; leftstart < mcol_g; leftstart++)
-        if (!xisgreen(P, row, leftstart)) break;
-      int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1 + (xfc(P, row, leftstart + 1) & 1));
-      const float2* g = S.gmm + (size_t)(row - top) * (ts / 2);
-      auto colors = [&](int col, const short* hex, float* color) {
+    // (b) green in 4 directions (:2071-2127).  The reference scans each row
+    // from its first non-green site; for the X-Trans layouts the scan visits
+    // every non-green site, with hexagon allhex0[row % 3][col % 3] and
+    // directions swapped pairwise on rows with one green per period, and
+    // sites only read the mosaic, so they are computed independently.
+    if (SITES) {
+      const int ncols = mcol_g - left;
+      for (int i = tid; i < (mrow_g - top) * ncols; i += nth) {
+        const int row = top + i / ncols, col = left + i % ncols;
+        if (xisgreen(P, row, col)) continue;
+        const short* hex = P.allhex0[row % 3][col % 3];
+        float color[4];
         color[0] = 0.6796875f * (xraw_hex(A, row, col, hex[1]) + xraw_hex(A, row, col, hex[0])) -
                    0.1796875f * (xraw_hex(A, row, col, 2 * hex[1]) + xraw_hex(A, row, col, 2 * hex[0]));
         color[1] = 0.87109375f * xraw_hex(A, row, col, hex[3]) + xraw_hex(A, row, col, hex[2]) * 0.12890625f +
@@ -348,27 +353,50 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
           color[2 + c] = 0.640625f * xraw_hex(A, row, col, hex[4 + c]) + 0.359375f * xraw_hex(A, row, col, -2 * hex[4 + c]) +
                          0.12890625f * (2.f * xraw_hex(A, row, col, 0) - xraw_hex(A, row, col, 3 * hex[4 + c]) -
                                         xraw_hex(A, row, col, -3 * hex[4 + c]));
-      };
-      if (coloffset == 3) {
-        const short* hex = P.allhex0[row % 3][leftstart % 3];
-        for (int col = leftstart; col < mcol_g; col += coloffset) {
-          float color[4];
-          colors(col, hex, color);
-          const float2 mmv = g[(col - left) >> 1];
-          for (int c = 0; c < 4; c++) RGB(c, row - top, col - left)[1] = LIMf(color[c], mmv.x, mmv.y);
-        }
-      } else {
-        const short* hexmod[2] = {P.allhex0[row % 3][leftstart % 3], P.allhex0[row % 3][(leftstart + coloffset) % 3]};
-        for (int col = leftstart, hexindex = 0; col < mcol_g; col += coloffset, coloffset ^= 3, hexindex ^= 1) {
-          const short* hex = hexmod[hexindex];
-          float color[4];
-          colors(col, hex, color);
-          const float2 mmv = g[(col - left) >> 1];
-          for (int c = 0; c < 4; c++) RGB(c ^ 1, row - top, col - left)[1] = LIMf(color[c], mmv.x, mmv.y);
+        const float2 mmv = S.gmm[(size_t)(row - top) * (ts / 2) + ((col - left) >> 1)];
+        const int swap = P.right_shift[row % 3] == 1 ? 0 : 1;
+        for (int c = 0; c < 4; c++) RGB(c ^ swap, row - top, col - left)[1] = LIMf(color[c], mmv.x, mmv.y);
+      }
+      __syncthreads();
+    } else {
+      // (b) green in 4 directions (:2071-2127), one row per thread
+      for (int row = top + tid; row < mrow_g; row += nth) {
+        int leftstart = left;
+        for (; leftstart < mcol_g; leftstart++)
+          if (!xisgreen(P, row, leftstart)) break;
+        int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1 + (xfc(P, row, leftstart + 1) & 1));
+        const float2* g = S.gmm + (size_t)(row - top) * (ts / 2);
+        auto colors = [&](int col, const short* hex, float* color) {
+          color[0] = 0.6796875f * (xraw_hex(A, row, col, hex[1]) + xraw_hex(A, row, col, hex[0])) -
+                     0.1796875f * (xraw_hex(A, row, col, 2 * hex[1]) + xraw_hex(A, row, col, 2 * hex[0]));
+          color[1] = 0.87109375f * xraw_hex(A, row, col, hex[3]) + xraw_hex(A, row, col, hex[2]) * 0.12890625f +
+                     0.359375f * (xraw_hex(A, row, col, 0) - xraw_hex(A, row, col, -hex[2]));
+          for (int c = 0; c < 2; c++)
+            color[2 + c] = 0.640625f * xraw_hex(A, row, col, hex[4 + c]) + 0.359375f * xraw_hex(A, row, col, -2 * hex[4 + c]) +
+                           0.12890625f * (2.f * xraw_hex(A, row, col, 0) - xraw_hex(A, row, col, 3 * hex[4 + c]) -
+                                          xraw_hex(A, row, col, -3 * hex[4 + c]));
+        };
+        if (coloffset == 3) {
+          const short* hex = P.allhex0[row % 3][leftstart % 3];
+          for (int col = leftstart; col < mcol_g; col += coloffset) {
+            float color[4];
+            colors(col, hex, color);
+            const float2 mmv = g[(col - left) >> 1];
+            for (int c = 0; c < 4; c++) RGB(c, row - top, col - left)[1] = LIMf(color[c], mmv.x, mmv.y);
+          }
+        } else {
+          const short* hexmod[2] = {P.allhex0[row % 3][leftstart % 3], P.allhex0[row % 3][(leftstart + coloffset) % 3]};
+          for (int col = leftstart, hexindex = 0; col < mcol_g; col += coloffset, coloffset ^= 3, hexindex ^= 1) {
+            const short* hex = hexmod[hexindex];
+            float color[4];
+            colors(col, hex, color);
+            const float2 mmv = g[(col - left) >> 1];
+            for (int c = 0; c < 4; c++) RGB(c ^ 1, row - top, col - left)[1] = LIMf(color[c], mmv.x, mmv.y);
+          }
         }
       }
+      __syncthreads();
     }
-    __syncthreads();
 
     for (int pass = 0; pass < 3; pass++) {
       if (pass == 1) {
@@ -457,37 +485,88 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
         }
       }
       __syncthreads();
-      // (e) red for blue pixels and vice versa (:2224-2264)
-      for (int row = top + 3 + tid; row < mrow_g - 3; row += nth) {
-        int leftstart = left + 3;
-        for (; leftstart < mcol_g - 1; leftstart++)
-          if (!xisgreen(P, row, leftstart)) break;
-        int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1);
-        const int c = ((row - P.sgrow) % 3) ? ts : 1;
-        const int h = 3 * (c ^ ts ^ 1);
-        auto body = [&](int col, int f) {
+      // (e) red for blue pixels and vice versa (:2224-2264): every non-green
+      // site from the scan start, writing its other colour f = 2 - own; it
+      // reads greens and its neighbours' native colours only.
+      if (SITES) {
+        const int r0e = top + 3, c0e = left + 3;
+        const int ncols = mcol_g - 3 - c0e;
+        for (int i = tid; i < (mrow_g - 3 - r0e) * (ncols > 0 ? ncols : 0); i += nth) {
+          const int row = r0e + i / ncols, col = c0e + i % ncols;
+          if (xisgreen(P, row, col)) continue;
+          const int c = ((row - P.sgrow) % 3) ? ts : 1;
+          const int h = 3 * (c ^ ts ^ 1);
+          const int f = 2 - xfc(P, row, col);
           float* rix = RGB(0, row - top, col - left);
           for (int d = 0; d < 4; d++, rix += (size_t)ts * ts * 3) {
-            const int i = d > 1 || ((d ^ c) & 1) ||
-                                  ((fabsf(rix[1] - rix[c * 3 + 1]) + fabsf(rix[1] - rix[-c * 3 + 1])) <
-                                   2.f * (fabsf(rix[1] - rix[h * 3 + 1]) + fabsf(rix[1] - rix[-h * 3 + 1])))
-                              ? c
-                              : h;
-            rix[f] = rix[1] + 0.5f * (rix[i * 3 + f] + rix[-i * 3 + f] - rix[i * 3 + 1] - rix[-i * 3 + 1]);
+            const int ii = d > 1 || ((d ^ c) & 1) ||
+                                   ((fabsf(rix[1] - rix[c * 3 + 1]) + fabsf(rix[1] - rix[-c * 3 + 1])) <
+                                    2.f * (fabsf(rix[1] - rix[h * 3 + 1]) + fabsf(rix[1] - rix[-h * 3 + 1])))
+                               ? c
+                               : h;
+            rix[f] = rix[1] + 0.5f * (rix[ii * 3 + f] + rix[-ii * 3 + f] - rix[ii * 3 + 1] - rix[-ii * 3 + 1]);
           }
-        };
-        if (coloffset == 3) {
-          int f = 2 - xfc(P, row, leftstart);
-          for (int col = leftstart; col < mcol_g - 3; col += coloffset, f ^= 2) body(col, f);
-        } else {
-          coloffset = xfc(P, row, leftstart + 1) == 1 ? 2 : 1;
-          int f = 2 - xfc(P, row, leftstart);
-          for (int col = leftstart; col < mcol_g - 3; col += coloffset, coloffset ^= 3, f = f ^ (coloffset & 2)) body(col, f);
         }
+        __syncthreads();
+      } else {
+        for (int row = top + 3 + tid; row < mrow_g - 3; row += nth) {
+          int leftstart = left + 3;
+          for (; leftstart < mcol_g - 1; leftstart++)
+            if (!xisgreen(P, row, leftstart)) break;
+          int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1);
+          const int c = ((row - P.sgrow) % 3) ? ts : 1;
+          const int h = 3 * (c ^ ts ^ 1);
+          auto body = [&](int col, int f) {
+            float* rix = RGB(0, row - top, col - left);
+            for (int d = 0; d < 4; d++, rix += (size_t)ts * ts * 3) {
+              const int i = d > 1 || ((d ^ c) & 1) ||
+                                    ((fabsf(rix[1] - rix[c * 3 + 1]) + fabsf(rix[1] - rix[-c * 3 + 1])) <
+                                     2.f * (fabsf(rix[1] - rix[h * 3 + 1]) + fabsf(rix[1] - rix[-h * 3 + 1])))
+                                ? c
+                                : h;
+              rix[f] = rix[1] + 0.5f * (rix[i * 3 + f] + rix[-i * 3 + f] - rix[i * 3 + 1] - rix[-i * 3 + 1]);
+            }
+          };
+          if (coloffset == 3) {
+            int f = 2 - xfc(P, row, leftstart);
+            for (int col = leftstart; col < mcol_g - 3; col += coloffset, f ^= 2) body(col, f);
+          } else {
+            coloffset = xfc(P, row, leftstart + 1) == 1 ? 2 : 1;
+            int f = 2 - xfc(P, row, leftstart);
+            for (int col = leftstart; col < mcol_g - 3; col += coloffset, coloffset ^= 3, f = f ^ (coloffset & 2)) body(col, f);
+          }
+        }
+        __syncthreads();
       }
-      __syncthreads();
-      // (f) R and B for 2x2 green blocks (:2266-2310)
-      {
+      // (f) R and B for 2x2 green blocks (:2266-2310): the scan visits the
+      // greens off the solitary-green row and column classes, hexagon
+      // allhex1[row % 3][col % 3]; each writes only its own R and B.
+      if (SITES) {
+        int topstart = top + 2;
+        for (; topstart < mrow_g - 2; topstart++)
+          if ((topstart - P.sgrow) % 3) break;
+        int leftstart = left + 2;
+        for (; leftstart < mcol_g - 2; leftstart++)
+          if ((leftstart - P.sgcol) % 3) break;
+        const int ncols = mcol_g - 2 - leftstart;
+        const int nrows = mrow_g - 2 - topstart;
+        for (int i = tid; i < (nrows > 0 ? nrows : 0) * (ncols > 0 ? ncols : 0); i += nth) {
+          const int row = topstart + i / ncols, col = leftstart + i % ncols;
+          if (!((row - P.sgrow) % 3) || !((col - P.sgcol) % 3)) continue;
+          float* rix = RGB(0, row - top, col - left);
+          const short* hex = P.allhex1[row % 3][col % 3];
+          for (int d = 0; d < NDIR; d += 2, rix += (size_t)ts * ts * 3) {
+            const int o0 = hex[d] * 3, o1 = hex[d + 1] * 3;
+            if (hex[d] + hex[d + 1]) {
+              const float g = 3 * rix[1] - 2 * rix[o0 + 1] - rix[o1 + 1];
+              for (int c = 0; c < 4; c += 2) rix[c] = (g + 2 * rix[o0 + c] + rix[o1 + c]) * 0.33333333f;
+            } else {
+              const float g = 2 * rix[1] - rix[o0 + 1] - rix[o1 + 1];
+              for (int c = 0; c < 4; c += 2) rix[c] = (g + rix[o0 + c] + rix[o1 + c]) * 0.5f;
+            }
+          }
+        }
+      } else {
         int topstart = top + 2;
         for (; topstart < mrow_g - 2; topstart++)
           if ((topstart - P.sgrow) % 3) break;
@@ -516,8 +595,7 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
         }
       }
       __syncthreads();
-    }
-    rgb = S.rgb;
+    }    rgb = S.rgb;
     int mrow = mrow_g - top;
     int mcol = mcol_g - left;
 
@@ -659,6 +737,58 @@ XtParams make_xt_params(const char* xtrans, int width) {
   return P;
 }
 
+// Whether the reference's row scans of phases (b), (e) and (f) reduce to
+// "every site of the class" for this pattern (true for the X-Trans layouts
+// and their shifts), so the site-parallel kernel variant applies.  Checked
+// by replaying the scans over every tile-origin residue.
+bool xt_sites_ok(const XtParams& P) {
+  auto isg = [&](int r, int c) { return P.xt[((r % 3) + 3) % 3][((c % 3) + 3) % 3] & 1; };
+  auto fc = [&](int r, int c) { return (int)P.xt[(r + 6) % 6][(c + 6) % 6]; };
+  for (int t0 = 0; t0 < 6; t0++)
+    for (int l0 = 0; l0 < 6; l0++) {
+      const int top = 6 + t0, left = 6 + l0, mrow = top + 30, mcol = left + 30;
+      for (int row = top; row < mrow; row++) {
+        // (b): visits from the first non-green site
+        int ls = left;
+        while (ls < mcol && isg(row, ls)) ls++;
+        int co = P.right_shift[row % 3] == 1 ? 3 : 1 + (fc(row, ls + 1) & 1);
+        int expect = ls;
+        for (int col = ls; col < mcol; col += co, co = (co == 3) ? 3 : (co ^ 3)) {
+          while (expect < mcol && isg(row, expect)) expect++;
+          if (col != expect) return false;
+          expect++;
+        }
+        while (expect < mcol && isg(row, expect)) expect++;
+        if (expect < mcol) return false;
+        // (e): the written colour is 2 - own colour at every visit
+        ls = left;
+        while (ls < mcol - 1 && isg(row, ls)) ls++;
+        int f = 2 - fc(row, ls);
+        if (P.right_shift[row % 3] == 1) {
+          for (int col = ls; col < mcol; col += 3, f ^= 2)
+            if (isg(row, col) || f != 2 - fc(row, col)) return false;
+        } else {
+          co = fc(row, ls + 1) == 1 ? 2 : 1;
+          for (int col = ls; col < mcol; col += co, co ^= 3, f ^= (co & 2))
+            if (isg(row, col) || f != 2 - fc(row, col)) return false;
+        }
+      }
+      // (f): visited columns are those off the solitary-green column class
+      int ts_ = top;
+      while (ts_ < mrow && !((ts_ - P.sgrow + 6) % 3)) ts_++;
+      int lsf = left;
+      while (lsf < mcol && !((lsf - P.sgcol + 6) % 3)) lsf++;
+      const int cos = 2 - (fc(ts_, lsf + 1) & 1);
+      for (int col = lsf, co = cos; col < mcol; col += co, co ^= 3)
+        if (!((col - P.sgcol + 6) % 3)) return false;
+      int visits = 0, expect_n = 0;
+      for (int col = lsf, co = cos; col < mcol; col += co, co ^= 3) visits++;
+      for (int col = lsf; col < mcol; col++) expect_n += ((col - P.sgcol + 6) % 3) != 0;
+      if (visits != expect_n) return false;
+    }
+  return true;
+}
+
 }  // namespace
 
 size_t ws_bytes_xtrans(size_t w, size_t h, int passes) {
@@ -703,7 +833,10 @@ lre_status launch_xtrans(Context* c, const float* raw, int cstride, float* rgb, 
     A.tile_counter = reinterpret_cast<int*>(c->ws.take(256));
     if (!A.scratch || !A.tile_counter) return fail(c, LRE_ERR_OUT_OF_MEMORY, "demosaic_xtrans_3pass: workspace too small");
     LRE_CUDA_TRY(c, cudaMemsetAsync(A.tile_counter, 0, sizeof(int), c->stream));
-    k_xtrans_3pass<<<nblk, XT_THREADS, 0, c->stream>>>(A);
+    if (xt_sites_ok(A.P))
+      k_xtrans_3pass<true><<<nblk, XT_THREADS, 0, c->stream>>>(A);
+    else
+      k_xtrans_3pass<false><<<nblk, XT_THREADS, 0, c->stream>>>(A);
     count_launch(c);
   }
   k_xtrans_border<<<grid_for(16 * (w + h), 256, c->sm_count * 2), 256, 0, c->stream>>>(A, 8);
