@@ -101,6 +101,15 @@ __device__ __forceinline__ float xraw_hex(const XtArgs& A, int row, int col, int
   return v / A.maximum;
 }
 
+// n / d by a multiply-high, exact while n * d < 2^32 (every loop here); the
+// per-site loops map a flat index to (row, column) every iteration.
+struct XDiv {
+  unsigned m;
+  int d;
+  __device__ explicit XDiv(int d_) : m(d_ > 1 ? 0xFFFFFFFFu / (unsigned)d_ + 1u : 0u), d(d_) {}
+  __device__ __forceinline__ int div(int n) const { return (int)__umulhi((unsigned)n, m) + (d == 1 ? n : 0); }
+};
+
 // std::max(low, std::min(val, high)) -- LIM of core/metal/shader_common.h.
 __device__ __forceinline__ float LIMf(float val, float low, float high) {
   float m = (high < val) ? high : val;
@@ -308,8 +317,9 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
       }
     }
     // native samples into direction 0 (:2055-2061)
+    const XDiv fdn(mcol_g - left);
     for (int i = tid; i < (mrow_g - top) * (mcol_g - left); i += nth) {
-      const int lr = i / (mcol_g - left), lc = i % (mcol_g - left);
+      const int lr = fdn.div(i), lc = i - lr * (mcol_g - left);
       const int row = top + lr, col = left + lc;
       RGB(0, lr, lc)[xfc(P, row, col)] = xraw(A, row, col);
     }
@@ -340,8 +350,9 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
     // sites only read the mosaic, so they are computed independently.
     if (SITES) {
       const int ncols = mcol_g - left;
+      const XDiv fdb(ncols);
       for (int i = tid; i < (mrow_g - top) * ncols; i += nth) {
-        const int row = top + i / ncols, col = left + i % ncols;
+        const int q_ = fdb.div(i), row = top + q_, col = left + i - q_ * ncols;
         if (xisgreen(P, row, col)) continue;
         const short* hex = P.allhex0[row % 3][col % 3];
         float color[4];
@@ -491,8 +502,9 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
       if (SITES) {
         const int r0e = top + 3, c0e = left + 3;
         const int ncols = mcol_g - 3 - c0e;
+        const XDiv fde(ncols > 0 ? ncols : 1);
         for (int i = tid; i < (mrow_g - 3 - r0e) * (ncols > 0 ? ncols : 0); i += nth) {
-          const int row = r0e + i / ncols, col = c0e + i % ncols;
+          const int q_ = fde.div(i), row = r0e + q_, col = c0e + i - q_ * ncols;
           if (xisgreen(P, row, col)) continue;
           const int c = ((row - P.sgrow) % 3) ? ts : 1;
           const int h = 3 * (c ^ ts ^ 1);
@@ -550,8 +562,9 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
           if ((leftstart - P.sgcol) % 3) break;
         const int ncols = mcol_g - 2 - leftstart;
         const int nrows = mrow_g - 2 - topstart;
+        const XDiv fdf(ncols > 0 ? ncols : 1);
         for (int i = tid; i < (nrows > 0 ? nrows : 0) * (ncols > 0 ? ncols : 0); i += nth) {
-          const int row = topstart + i / ncols, col = leftstart + i % ncols;
+          const int q_ = fdf.div(i), row = topstart + q_, col = leftstart + i - q_ * ncols;
           if (!((row - P.sgrow) % 3) || !((col - P.sgcol) % 3)) continue;
           float* rix = RGB(0, row - top, col - left);
           const short* hex = P.allhex1[row % 3][col % 3];
@@ -603,10 +616,12 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
     {
       const int dn = XTS - 10;
       const int rows = mrow - 10, cols = mcol - 10;
+      const XDiv fdrc(rows * cols), fdcl(cols);
       for (int i = tid; i < NDIR * rows * cols; i += nth) {
-        const int d = i / (rows * cols);
-        const int rem = i % (rows * cols);
-        const int row = 5 + rem / cols, col = 5 + rem % cols;
+        const int d = fdrc.div(i);
+        const int rem = i - d * (rows * cols);
+        const int q_ = fdcl.div(rem);
+        const int row = 5 + q_, col = 5 + rem - q_ * cols;
         int f = dirv[d & 3];
         f = f == 1 ? 1 : f - 8;
         // yuv buffer offset f (width ts-8) -> tile offset
@@ -630,8 +645,9 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
     {
       const int dn = XTS - 10;
       const int rows = mrow - 12, cols = mcol - 12;
+      const XDiv fdh(cols);
       for (int i = tid; i < rows * cols; i += nth) {
-        const int row = 6 + i / cols, col = 6 + i % cols;
+        const int q_ = fdh.div(i), row = 6 + q_, col = 6 + i - q_ * cols;
         auto D = [&](int d, int r, int c) { return S.drv[((size_t)d * dn + (r - 5)) * dn + (c - 5)]; };
         float tr = D(0, row, col) < D(1, row, col) ? D(0, row, col) : D(1, row, col);
         for (int d = 2; d < NDIR; d++) tr = (D(d, row, col) < tr ? D(d, row, col) : tr);
@@ -647,17 +663,31 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
     __syncthreads();
     if (H - top < ts + 4) mrow = H - top + 2;
     if (W - left < ts + 4) mcol = W - left + 2;
-    // (j) 5x5 homogeneity sums and their max (:2504-2612)
+    // (j) 5x5 homogeneity sums and their max (:2504-2612).  Integer sums
+    // (at most 25 * 9 = 225, no wrap), so they are formed separably: row
+    // 5-sums first, into the derivative planes' memory (dead after (h)).
     const int r0 = min(top, 8), c0 = min(left, 8);
+    unsigned char* hs5 = reinterpret_cast<unsigned char*>(S.drv);  // [NDIR][ts][ts]
+    {
+      const int rows = mrow - 8 - r0 + 4, cols = mcol - 8 - c0;
+      const XDiv fdr(rows * cols), fdc(cols);
+      for (int i = tid; i < NDIR * rows * cols; i += nth) {
+        const int d = fdr.div(i), rem = i - d * (rows * cols);
+        const int q_ = fdc.div(rem), row = r0 - 2 + q_, col = c0 + rem - q_ * cols;
+        const unsigned char* hp = S.homo + ((size_t)d * ts + row) * ts + col;
+        hs5[((size_t)d * ts + row) * ts + col] = (unsigned char)(hp[-2] + hp[-1] + hp[0] + hp[1] + hp[2]);
+      }
+    }
+    __syncthreads();
     {
       const int rows = mrow - 8 - r0, cols = mcol - 8 - c0;
+      const XDiv fdj(cols);
       for (int i = tid; i < rows * cols; i += nth) {
-        const int row = r0 + i / cols, col = c0 + i % cols;
+        const int q_ = fdj.div(i), row = r0 + q_, col = c0 + i - q_ * cols;
         unsigned char maxval = 0;
         for (int d = 0; d < NDIR; d++) {
           int s = 0;
-          for (int v = -2; v <= 2; v++)
-            for (int h = -2; h <= 2; h++) s += S.homo[((size_t)d * ts + row + v) * ts + col + h];
+          for (int v = -2; v <= 2; v++) s += hs5[((size_t)d * ts + row + v) * ts + col];
           const unsigned char hs = (unsigned char)s;
           S.homosum[((size_t)d * ts + row) * ts + col] = hs;
           if (d == 0 || maxval < hs) maxval = hs;
@@ -670,8 +700,9 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
     // (l) average the most homogeneous directions (:2614-2650)
     {
       const int rows = mrow - 8 - r0, cols = mcol - 8 - c0;
+      const XDiv fdj(cols);
       for (int i = tid; i < rows * cols; i += nth) {
-        const int row = r0 + i / cols, col = c0 + i % cols;
+        const int q_ = fdj.div(i), row = r0 + q_, col = c0 + i - q_ * cols;
         unsigned char hm[8];
         for (int d = 0; d < 4; d++) hm[d] = S.homosum[((size_t)d * ts + row) * ts + col];
         for (int d = 4; d < NDIR; d++) {
