@@ -398,7 +398,8 @@ cudaError_t axial_dispatch(int T, int NT, size_t w, size_t h, cudaStream_t s, co
 //   pass B: box means of those five -> blended output
 // Window sums use the same truncated windows, area reciprocals and float /
 // double conversions as the fused kernel; only the summation order differs.
-constexpr int AXS_PER_LANE = 4;  // output columns per lane in the horizontal pass
+// A strip is WS = 32 * PL columns: each lane forms the horizontal sums of PL
+// adjacent output columns (PL = 4 or 2).
 
 // Column j of a strip's shared-memory window sums, with one pad slot per 16
 // doubles: lanes reading 4 apart then hit 16 distinct 8-byte bank pairs.
@@ -444,15 +445,16 @@ __device__ __forceinline__ void strip_update(double (*Vs)[vs_len<WS>()], int VC,
 
 // Horizontal window sums of the lane's 4 output columns: hs[q][k].
 template <int NQ, int WS>
-__device__ __forceinline__ void strip_hsum(double (*Vs)[vs_len<WS>()], int r, double hs[NQ][AXS_PER_LANE]) {
-  const int c0 = threadIdx.x * AXS_PER_LANE;
+__device__ __forceinline__ void strip_hsum(double (*Vs)[vs_len<WS>()], int r, double hs[NQ][WS / 32]) {
+  constexpr int PL = WS / 32;
+  const int c0 = threadIdx.x * PL;
 #pragma unroll
   for (int q = 0; q < NQ; q++) {
     double s = 0.0;
     for (int t = 0; t <= 2 * r; t++) s += Vs[q][vidx(c0 + t)];
     hs[q][0] = s;
 #pragma unroll
-    for (int k = 1; k < AXS_PER_LANE; k++) {
+    for (int k = 1; k < PL; k++) {
       s += Vs[q][vidx(c0 + k + 2 * r)];
       s -= Vs[q][vidx(c0 + k - 1)];
       hs[q][k] = s;
@@ -466,7 +468,7 @@ __global__ void __launch_bounds__(32) k_ax_ab(const float* __restrict__ src, int
                                              float* __restrict__ bR, float* __restrict__ aB, float* __restrict__ bB,
                                              float* __restrict__ er) {
   constexpr int NQ = 6;
-  static_assert(WS == 32 * AXS_PER_LANE, "one warp covers the strip");
+  constexpr int PL = WS / 32;
   __shared__ double Vs[NQ][vs_len<WS>()];
   const int VC = WS + 2 * r;
   const float inv_norm = 1.f / fmaxf(*d_maxg, 1e-6f);
@@ -479,22 +481,22 @@ __global__ void __launch_bounds__(32) k_ax_ab(const float* __restrict__ src, int
     for (int q = 0; q < NQ; q++) Vs[q][vidx(j)] = 0.0;
   // window of the first output row: rows [y0 - r, y0 + r] (out-of-image rows load zeros)
   for (int iy = y0 - r; iy <= y0 + r; iy++) strip_update<NQ, WS>(Vs, VC, xv0, iy, -1, ld);
-  double inv_cx[AXS_PER_LANE];
+  double inv_cx[PL];
 #pragma unroll
-  for (int k = 0; k < AXS_PER_LANE; k++) {
-    const int x = x0 + threadIdx.x * AXS_PER_LANE + k;
+  for (int k = 0; k < PL; k++) {
+    const int x = x0 + threadIdx.x * PL + k;
     inv_cx[k] = x < W ? 1.0 / (double)win_count(x, r, W) : 0.0;
   }
   for (int y = y0; y < y_end; y++) {
     if (y > y0) strip_update<NQ, WS>(Vs, VC, xv0, y + r, y - r - 1, ld);
     __syncwarp();
-    double hs[NQ][AXS_PER_LANE];
+    double hs[NQ][PL];
     strip_hsum<NQ, WS>(Vs, r, hs);
     __syncwarp();  // the next update rewrites Vs
     const double inv_cy = 1.0 / (double)win_count(y, r, H);
 #pragma unroll
-    for (int k = 0; k < AXS_PER_LANE; k++) {
-      const int x = x0 + threadIdx.x * AXS_PER_LANE + k;
+    for (int k = 0; k < PL; k++) {
+      const int x = x0 + threadIdx.x * PL + k;
       if (x >= W) continue;
       const double ia = inv_cx[k] * inv_cy;
       const double mi = hs[0][k] * ia;
@@ -528,7 +530,7 @@ __global__ void __launch_bounds__(32) k_ax_q(const float* __restrict__ src, floa
                                             const float* __restrict__ aB, const float* __restrict__ bB,
                                             const float* __restrict__ er) {
   constexpr int NQ = 5;
-  static_assert(WS == 32 * AXS_PER_LANE, "one warp covers the strip");
+  constexpr int PL = WS / 32;
   __shared__ double Vs[NQ][vs_len<WS>()];
   const int VC = WS + 2 * r;
   const float norm_ref = fmaxf(*d_maxg, 1e-6f);
@@ -556,22 +558,22 @@ __global__ void __launch_bounds__(32) k_ax_q(const float* __restrict__ src, floa
 #pragma unroll
     for (int q = 0; q < NQ; q++) Vs[q][vidx(j)] = 0.0;
   for (int iy = y0 - r; iy <= y0 + r; iy++) strip_update<NQ, WS>(Vs, VC, xv0, iy, -1, ld);
-  double inv_cx[AXS_PER_LANE];
+  double inv_cx[PL];
 #pragma unroll
-  for (int k = 0; k < AXS_PER_LANE; k++) {
-    const int x = x0 + threadIdx.x * AXS_PER_LANE + k;
+  for (int k = 0; k < PL; k++) {
+    const int x = x0 + threadIdx.x * PL + k;
     inv_cx[k] = x < W ? 1.0 / (double)win_count(x, r, W) : 0.0;
   }
   for (int y = y0; y < y_end; y++) {
     if (y > y0) strip_update<NQ, WS>(Vs, VC, xv0, y + r, y - r - 1, ld);
     __syncwarp();
-    double hs[NQ][AXS_PER_LANE];
+    double hs[NQ][PL];
     strip_hsum<NQ, WS>(Vs, r, hs);
     __syncwarp();
     const double inv_cy = 1.0 / (double)win_count(y, r, H);
 #pragma unroll
-    for (int k = 0; k < AXS_PER_LANE; k++) {
-      const int x = x0 + threadIdx.x * AXS_PER_LANE + k;
+    for (int k = 0; k < PL; k++) {
+      const int x = x0 + threadIdx.x * PL + k;
       if (x >= W) continue;
       const double ia = inv_cx[k] * inv_cy;
       const size_t o = ((size_t)y * W + x) * 3;
@@ -590,9 +592,9 @@ __global__ void __launch_bounds__(32) k_ax_q(const float* __restrict__ src, floa
   }
 }
 
+template <int WS>
 cudaError_t axial_stream(size_t w, size_t h, int HS, cudaStream_t s, const float* src, float* out, int r, float eps,
                          float strength, const float* d_max, float* planes) {
-  constexpr int WS = 32 * AXS_PER_LANE;
   const size_t n = w * h;
   float* aR = planes;
   float* bR = planes + n;
@@ -629,14 +631,17 @@ lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, si
     LRE_CUDA_TRY(c, cudaMemcpyAsync(tmp, in, w * h * 3 * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
     src = tmp;
   }
-  // Strip height: enough one-warp strips for ~24 resident warps per SM (the
+  // Strip width 128 (4 columns per lane) or 64 (2 per lane); strip height:
+  // enough one-warp strips for ~24 resident warps per SM (the
   // passes are load-latency bound), but at least 16 rows so the 2r + 1 row
   // prologue of a strip stays small; capped by the tuning choice.
-  const size_t strips_x = (w + 127) / 128;
+  const int WS = c->tune.axial_strip == 64 ? 64 : 128;
+  const size_t strips_x = (w + WS - 1) / WS;
   const size_t want = (size_t)c->sm_count * 24;
   int HS = c->tune.axial_rows == 128 ? 128 : 64;
   while (HS > 16 && strips_x * ((h + HS - 1) / HS) < want) HS /= 2;
-  LRE_CUDA_TRY(c, axial_stream(w, h, HS, c->stream, src, out, radius, eps, strength, d_max_g, planes));
+  LRE_CUDA_TRY(c, WS == 64 ? axial_stream<64>(w, h, HS, c->stream, src, out, radius, eps, strength, d_max_g, planes)
+                           : axial_stream<128>(w, h, HS, c->stream, src, out, radius, eps, strength, d_max_g, planes));
   count_launch(c, 2);
   return check_launch(c, "ca_axial_cleanup");
 }
