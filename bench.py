@@ -41,7 +41,7 @@ WB = (2.0, 1.0, 1.5, 1.0)
 METRIC = "develop MP/s on 1 B200 (51 MP Bayer: AMaZE->defringe->axial CA->tone map)"
 # algorithmic bytes per output pixel of each stage (float32 RGB = 12 B/px)
 STAGE_BYTES = {"amaze": 16.0, "defringe": 24.0, "axial": 24.0, "tone": 24.0}
-# From one ncu capture of k_amaze at 4096x3072 (profiles/amaze_axial_12mp_full.md):
+# From one ncu capture of k_amaze at 4096x3072 (profiles/develop_12mp_full.md):
 # DRAM read+write bytes and executed warp-instructions per output pixel.
 AMAZE_DRAM_BYTES_PER_PX = (109.713152e6 + 900.116224e6) / (4096 * 3072)
 AMAZE_WARP_INST_PER_PX = 883750708 / (4096 * 3072)
