@@ -258,6 +258,24 @@ lre_status lre_demosaic_bayer_linear(lre_ctx* ctx, const float* raw_rgb, float* 
 lre_status lre_dev_demosaic_bayer_linear(lre_ctx* ctx, const float* raw, float* rgb, size_t width,
                                          size_t height, uint32_t filters, float maximum_value);
 
+/* Accelerator::demosaic_bayer_dcb (core/accelerator.h:273-277, defaults
+ * iterations = 1, dcb_enhance = true; the reference GPU path has no DCB and
+ * falls back to the CPU, core/accelerator.cpp:180-199) and its CPU body
+ * CPUAccelerator::demosaic_bayer_dcb (core/cpu_accelerator.cpp:1043-1137):
+ * 8-neighbour seed, DCB_Processor::run_dcb(iterations, dcb_enhance), /max,
+ * 3-px border interpolation.  Results equal the reference run with one
+ * OpenMP thread (its row-parallel in-place passes are order-dependent).
+ * Needs a 2x2 Bayer layout (RGGB, BGGR, GRBG, GBRG); returns
+ * LRE_ERR_INVALID_ARGUMENT for other filters words.  Sparse (H,W,3) raw in. */
+lre_status lre_demosaic_bayer_dcb(lre_ctx* ctx, const float* raw_rgb, float* rgb, size_t width,
+                                  size_t height, uint32_t filters, float maximum_value, int iterations,
+                                  int dcb_enhance);
+/* Same on a dense device mosaic; returns after the stream has drained (the
+ * sweeps' completion flag is read back). */
+lre_status lre_dev_demosaic_bayer_dcb(lre_ctx* ctx, const float* raw, float* rgb, size_t width,
+                                      size_t height, uint32_t filters, float maximum_value, int iterations,
+                                      int dcb_enhance);
+
 /* ------------------------------------------------------ output end */
 /* GPUAccelerator::convert_color_space (core/gpu_accelerator.h:66-69;
  * core/cpu_accelerator.cpp:2874-2897): out = M[:, :3] * in + M[:, 3] with

@@ -184,4 +184,9 @@ namespace lre {
 lre_status launch_border_interp(Context* c, float* rgb, size_t w, size_t h, uint32_t filters, int band);
 lre_status launch_bayer_linear(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
                                uint32_t filters, float maximum_value);
+// DCB Bayer demosaic (k_dcb.cu).  Synchronises the stream at the end to read
+// the sweeps' error flag.
+size_t ws_bytes_dcb(size_t w, size_t h);
+lre_status launch_dcb(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
+                      uint32_t filters, float maximum_value, int iterations, bool enhance);
 }  // namespace lre

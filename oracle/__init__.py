@@ -62,6 +62,7 @@ _REF_SIGS = {
     "ref_set_num_threads": (None, [C.c_int]),
     "ref_demosaic_bayer_amaze": (C.c_int, [_p, _p, _sz, _sz, C.c_uint32, _p, _f]),
     "ref_demosaic_bayer_linear": (C.c_int, [_p, _p, _sz, _sz, C.c_uint32, _f]),
+    "ref_demosaic_bayer_dcb": (C.c_int, [_p, _p, _sz, _sz, C.c_uint32, _f, C.c_int, C.c_int]),
     "ref_demosaic_xtrans": (C.c_int, [_p, _p, _sz, _sz, _p, _p, _f, C.c_int]),
     "ref_apply_white_balance": (C.c_int, [_p, _p, _sz, _sz, _p, C.c_uint32, _p]),
     "ref_tone_mapping": (C.c_int, [_p, _p, _sz, _sz, _f]),
@@ -144,6 +145,26 @@ def bayer_linear(raw_sparse, filters, maximum=1.0):
     h, w, _ = raw.shape
     out = np.zeros_like(raw)
     assert ref().ref_demosaic_bayer_linear(_ptr(raw), _ptr(out), w, h, int(filters), float(maximum))
+    return out
+
+
+def bayer_dcb(raw_sparse, filters, maximum=1.0, iterations=1, enhance=True, threads=1):
+    """The reference's DCB demosaic (core/cpu_accelerator.cpp:1043-1137).
+
+    ``threads=1`` (the default) gives the sequential result of DCB's in-place
+    passes; with more OpenMP threads the reference's row-parallel nyquist, pp
+    and color_full loops read rows that other threads are rewriting, so rows
+    at each thread's chunk boundary depend on timing."""
+    raw = _img(raw_sparse)
+    h, w, _ = raw.shape
+    out = np.zeros_like(raw)
+    saved = num_threads()
+    set_threads(threads)
+    try:
+        assert ref().ref_demosaic_bayer_dcb(_ptr(raw), _ptr(out), w, h, int(filters), float(maximum),
+                                            int(iterations), int(bool(enhance)))
+    finally:
+        set_threads(saved)
     return out
 
 

@@ -103,6 +103,19 @@ int ref_demosaic_bayer_linear(const float* raw, float* rgb, size_t w, size_t h, 
   return accel().demosaic_bayer_linear(in, out, filters, maximum_value) ? 1 : 0;
 }
 
+/* core/cpu_accelerator.cpp:1043-1137 (DCB demosaic: sparse + 8-neighbour
+ * bilinear seed, DCB_Processor::run_dcb at :998-1035, /maximum,
+ * border_interpolate(3)).  Several of DCB's in-place passes are OpenMP
+ * row-parallel loops whose rows read rows the same loop rewrites (nyquist,
+ * pp, the last color_full loop); their defined result is the sequential one,
+ * so tests call this with ref_set_num_threads(1). */
+int ref_demosaic_bayer_dcb(const float* raw, float* rgb, size_t w, size_t h, uint32_t filters,
+                           float maximum_value, int iterations, int dcb_enhance) {
+  MuteCout m;
+  ImageBufferFloat in = fbuf(raw, w, h), out = fbuf(rgb, w, h);
+  return accel().demosaic_bayer_dcb(in, out, filters, maximum_value, iterations, dcb_enhance != 0) ? 1 : 0;
+}
+
 /* core/cpu_accelerator.cpp:2767-2784 (X-Trans 1-pass / 3-pass) */
 int ref_demosaic_xtrans(const float* raw, float* rgb, size_t w, size_t h, const char xtrans[36],
                         const float color_matrix[12], float maximum_value, int passes) {

@@ -116,3 +116,23 @@ def test_restatement_reproduces_golden(gold):
     )
     assert np.array_equal(oracle.black_level(gold["raw4"], [510, 512, 514, 511, 0, 0], 0, 16000), gold["black_chan"])
     assert np.array_equal(oracle.port_white_balance(gold["raw4"], (2.1, 1.0, 1.7, 1.02), scenes.FILTERS["GRBG"]), gold["wb_grbg"])
+
+
+def test_reference_dcb_flat_field_and_thread_dependence():
+    """The reference DCB (core/cpu_accelerator.cpp:1043-1137) keeps a flat
+    field flat; single-threaded it is deterministic.  (With several OpenMP
+    threads its in-place row-parallel passes read rows other threads are
+    rewriting, which is why parity is taken against one thread.)"""
+    import numpy as np
+    from libraw_enhanced_b200 import scenes
+
+    if not oracle.ref_available():
+        pytest.skip("reference not built")
+    f = scenes.FILTERS["RGGB"]
+    flat = scenes.sparse_rgb(np.full((40, 72), 700.0, np.float32), "RGGB")
+    out = oracle.bayer_dcb(flat, f, 4095.0)
+    assert np.array_equal(out, np.full_like(out, np.float32(700.0) / np.float32(4095.0)))
+    sp = scenes.sparse_rgb(scenes.bayer_scene(64, 96, 3) * np.float32(4095.0), "RGGB")
+    a = oracle.bayer_dcb(sp, f, 4095.0, threads=1)
+    b = oracle.bayer_dcb(sp, f, 4095.0, threads=1)
+    assert np.array_equal(a, b) and np.isfinite(a).all()
