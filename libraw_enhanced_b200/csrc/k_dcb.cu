@@ -379,6 +379,32 @@ __global__ void k_dcb_output(const float* __restrict__ R, const float* __restric
   }
 }
 
+// Terms of dcb_nyquist that do not change during the pass: the site's own
+// sample and (S + N + W + E) / 4 of the same colour two sites away.
+__global__ void k_dcb_nyq_terms(const float* __restrict__ R, const float* __restrict__ B, float* __restrict__ A,
+                                float* __restrict__ Q, Geo g) {
+  DCB_FOR_PIXELS(g) {
+    const unsigned f = g.fc(r, c);
+    if (f == 1 || r < 2 || r >= g.H - 2 || c < 2 || c >= g.W - 2) continue;
+    const size_t i = g.at(r, c), v = 2 * (size_t)g.W;
+    const float* X = f == 0 ? R : B;
+    A[i] = X[i];
+    Q[i] = (X[i + v] + X[i - v] + X[i - 2] + X[i + 2]) / 4.0f;
+  }
+}
+
+// dcb_pp's green term G - mean8(G), in the reference's summation order.
+__global__ void k_dcb_pp_terms(const float* __restrict__ G, float* __restrict__ K, Geo g) {
+  DCB_FOR_PIXELS(g) {
+    if (r < 2 || r >= g.H - 2 || c < 2 || c >= g.W - 2) continue;
+    const size_t i = g.at(r, c), u = g.W;
+    const float g1 = (G[i - 1] + G[i + 1] + G[i - u] + G[i + u] + G[i - u - 1] + G[i + u + 1] + G[i - u + 1] +
+                      G[i + u - 1]) /
+                     8.0f;
+    K[i] = G[i] - g1;
+  }
+}
+
 // ------------------------------------------------------------------ sweeps
 
 struct SweepArgs {
@@ -390,48 +416,52 @@ struct SweepArgs {
   int* progress;  // per band: columns < progress[b] of band b are final in HBM
 };
 
-template <int NP, int HALO, int SKEW>
+// The sweep's shared-memory ring, addressed through the __shared__ symbol
+// itself so every access compiles to a shared-memory instruction.
+extern __shared__ float sweep_smem[];
+
+template <int NP, int HALO, int PAD>
 struct Ring {
   static constexpr int ROWS = 32 + 2 * HALO;
-  static constexpr int PITCH = kRing + SKEW + 1;  // lane l hits bank (l + const) % 32
+  static constexpr int PITCH = kRing + PAD;
   static constexpr int PLANE = ROWS * PITCH;
   static constexpr size_t BYTES = (size_t)NP * PLANE * sizeof(float);
-  float* sm;
   int rbase;
   __device__ __forceinline__ float& operator()(int p, int r, int c) const {
-    return sm[p * PLANE + (r - rbase) * PITCH + (c & (kRing - 1))];
+    return sweep_smem[p * PLANE + (r - rbase) * PITCH + (c & (kRing - 1))];
   }
 };
 
-// dcb_nyquist (:836-848): state G; inputs R, B.
+// Each sweep op names its planes per warp: NS state planes first, then
+// inputs.  NCH = 2 runs two independent channels (R and B) as separate
+// warps; PAIR = 2 gives two adjacent rows the same column when a row only
+// depends on rows two above it.
+
+// dcb_nyquist (:836-848): state G; inputs the site's own sample A and the
+// quarter-sum Q of the four same-colour samples two sites away (k_dcb_nyq_terms;
+// R and B do not change across the nyquist passes).  A site reads rows r +- 2
+// only, so rows r and r + 1 advance together.
 struct OpNyquist {
-  static constexpr int NS = 1, NP = 3, HALO = 2, SKEW = 1;
+  static constexpr int NS = 1, NP = 3, HALO = 2, SKEW = 1, PAIR = 2, NCH = 1;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo& g) {
-    const unsigned f = g.fc(r, c);
-    if (f == 1) return;
-    const int X = f == 0 ? 1 : 2;
-    t(0, r, c) = dclip((t(0, r + 2, c) + t(0, r - 2, c) + t(0, r, c - 2) + t(0, r, c + 2)) / 4.0f + t(X, r, c) -
-                           (t(X, r + 2, c) + t(X, r - 2, c) + t(X, r, c - 2) + t(X, r, c + 2)) / 4.0f,
+    if (g.fc(r, c) == 1) return;
+    t(0, r, c) = dclip((t(0, r + 2, c) + t(0, r - 2, c) + t(0, r, c - 2) + t(0, r, c + 2)) / 4.0f + t(1, r, c) -
+                           t(2, r, c),
                        g.maxv);
   }
 };
 
-// dcb_pp (:820-834): state R, B; input G.
+// dcb_pp (:820-834), one channel (R or B) per warp: state the channel;
+// input K = G - mean8(G) (k_dcb_pp_terms; green does not change in the pass).
 struct OpPP {
-  static constexpr int NS = 2, NP = 3, HALO = 1, SKEW = 2;
-  template <class T>
-  __device__ static float avg8(const T& t, int p, int r, int c) {
-    return (t(p, r, c - 1) + t(p, r, c + 1) + t(p, r - 1, c) + t(p, r + 1, c) + t(p, r - 1, c - 1) +
-            t(p, r + 1, c + 1) + t(p, r - 1, c + 1) + t(p, r + 1, c - 1)) /
-           8.0f;
-  }
+  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 2;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo& g) {
-    const float r1 = avg8(t, 0, r, c), g1 = avg8(t, 2, r, c), b1 = avg8(t, 1, r, c);
-    const float gc = t(2, r, c);
-    t(0, r, c) = dclip(r1 + (gc - g1), g.maxv);
-    t(1, r, c) = dclip(b1 + (gc - g1), g.maxv);
+    const float x1 = (t(0, r, c - 1) + t(0, r, c + 1) + t(0, r - 1, c) + t(0, r + 1, c) + t(0, r - 1, c - 1) +
+                      t(0, r + 1, c + 1) + t(0, r - 1, c + 1) + t(0, r + 1, c - 1)) /
+                     8.0f;
+    t(0, r, c) = dclip(x1 + t(1, r, c), g.maxv);
   }
 };
 
@@ -446,7 +476,7 @@ __device__ __forceinline__ void clamp8(const T& t, int p, int r, int c, float v)
 
 // dcb_refinement's closing clamp (:992-994): state G; input the pre-clamp value.
 struct OpRefine {
-  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2;
+  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 1;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo& g) {
     if (g.fc(r, c) == 1) return;
@@ -454,15 +484,22 @@ struct OpRefine {
   }
 };
 
-// dcb_color_full's last loop (:898-913): state R, B; inputs CLIP(chroma + G).
+// dcb_color_full's last loop (:898-913), one channel per warp: state R or B;
+// input that channel's CLIP(chroma + G).
 struct OpColorFull {
-  static constexpr int NS = 2, NP = 4, HALO = 1, SKEW = 2;
+  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 2;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo&) {
-    clamp8(t, 0, r, c, t(2, r, c));
-    clamp8(t, 1, r, c, t(3, r, c));
+    clamp8(t, 0, r, c, t(1, r, c));
   }
 };
+
+// Row padding so the 32 lanes of a step hit 32 different banks: lane l
+// reads row l + k at column t - SKEW * (l / PAIR), so with PAIR = 1 a pitch
+// of SKEW + 1 (mod 32) gives bank l + const; with PAIR = 2 (SKEW = 1) a
+// pitch of 16 (mod 32) gives bank 16 * (l & 1) - l / 2 + const.
+template <class Op>
+using RingOf = Ring<Op::NP, Op::HALO, (Op::PAIR == 2 ? 16 : Op::SKEW + 1)>;
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -475,78 +512,168 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
+__device__ __forceinline__ void cp_async4(float* s, const float* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Steps per group.  Each group first makes the columns it needs resident
+// (copies issued one group earlier), then issues the copies for the next
+// group, then runs its GS steps while those copies are in flight.
+constexpr int kGroup = 16;
+
 template <class Op>
 __global__ void __launch_bounds__(32) k_dcb_sweep(SweepArgs a) {
-  using R = Ring<Op::NP, Op::HALO, Op::SKEW>;
-  constexpr int HALO = Op::HALO, SKEW = Op::SKEW;
-  extern __shared__ float sweep_smem[];
-  const int lane = threadIdx.x;
-  int band = 0;
-  if (lane == 0) band = atomicAdd(a.ticket, 1);
-  band = __shfl_sync(0xffffffffu, band, 0);
+  using R = RingOf<Op>;
+  constexpr int HALO = Op::HALO, NS = Op::NS, NP = Op::NP, NCH = Op::NCH, GS = kGroup;
+  constexpr int SPAN = Op::SKEW * (31 / Op::PAIR);  // column lag of lane 31 behind lane 0
+  const int lane = threadIdx.x, lc = lane & 15, lr = lane >> 4;
+  int ticket = 0;
+  if (lane == 0) ticket = atomicAdd(a.ticket, 1);
+  ticket = __shfl_sync(0xffffffffu, ticket, 0);
+  // Tickets go out in CTA start order; ticket k is band k / NCH, channel
+  // k % NCH, and waits only for ticket k - NCH (same channel, band above).
+  const int band = ticket / NCH, ch = ticket % NCH;
+  // Per-warp plane pointers (with NCH = 2 the argument holds
+  // {state ch0, state ch1, input ch0, input ch1}).
+  const float* src[NP];
+  float* dst[NS];
+#pragma unroll
+  for (int p = 0; p < NP; p++) {
+    if (NCH == 1) src[p] = a.plane[p];
+    else src[p] = p < NS ? (ch ? a.plane[1] : a.plane[0]) : (ch ? a.plane[3] : a.plane[2]);
+  }
+#pragma unroll
+  for (int p = 0; p < NS; p++) dst[p] = NCH == 1 ? a.plane[p] : (ch ? a.plane[1] : a.plane[0]);
   const int r0 = a.r_lo + band * 32;
   const int W = a.g.W, H = a.g.H;
-  const R t{sweep_smem, r0 - HALO};
+  const R t{r0 - HALO};
   const int st_r0 = max(r0 - HALO, 0), st_r1 = min(r0 + 31 + HALO, H - 1);
   const int out_r1 = min(r0 + 31, a.r_hi);
-  const int t_end = a.c_hi + SKEW * 31;
-  int staged = a.c_lo - HALO, flushed = a.c_lo;
+  const int t_end = a.c_hi + SPAN;
+  const int c_stop = a.c_hi + HALO + 1;  // staging never reaches past this column
+  int flushed = a.c_lo;
   bool waiting = band > 0;
 
-  auto flush = [&](int hi) {
-    if (hi <= flushed) return;
-    for (int p = 0; p < Op::NS; p++)
-      for (int r = r0; r <= out_r1; r++)
-        for (int c = flushed + lane; c < hi; c += 32) __stcg(a.plane[p] + (size_t)r * W + c, t(p, r, c));
-    flushed = hi;
-    __threadfence();
-    __syncwarp();
-    if (lane == 0) st_release(a.progress + band, hi > a.c_hi ? INT_MAX : hi);
+  // Rows above r0 belong to the band above: its state planes are read only
+  // after that band has flushed the columns, and with L2-coherent loads.
+  auto upper = [&](int p, int r) { return band > 0 && p < NS && r < r0; };
+
+  // Progress of the band above as last observed by lane 0 (acquire loads;
+  // the warp barrier after the wait orders every lane's later loads).
+  int above = 0;
+  auto wait_above = [&](int need) {
+    if (!waiting) return;
+    int ok = 1;
+    if (lane == 0 && above < need) {
+      const long long start = clock64();
+      while ((above = ld_acquire(a.progress + ticket - NCH)) < need) {
+        __nanosleep(32);
+        if (clock64() - start > kWaitCycles) {
+          atomicExch(a.err, 1);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    if (!__shfl_sync(0xffffffffu, ok, 0)) waiting = false;
   };
 
-  for (int t0 = a.c_lo; t0 <= t_end; t0 += 32) {
-    flush(min(t0 - SKEW * 31, a.c_hi + 1));
-    const int st_hi = min(t0 + 32 + HALO, a.c_hi + HALO + 1);
-    if (st_hi > staged) {
-      if (waiting) {
-        const int need = min(st_hi, a.c_hi + 1);
-        int ok = 1;
-        if (lane == 0) {
-          const long long start = clock64();
-          while (ld_acquire(a.progress + band - 1) < need) {
-            __nanosleep(64);
-            if (clock64() - start > kWaitCycles) {
-              atomicExch(a.err, 1);
-              ok = 0;
-              break;
-            }
-          }
-          __threadfence();
-        }
-        if (!__shfl_sync(0xffffffffu, ok, 0)) waiting = false;
-      }
-      for (int p = 0; p < Op::NP; p++)
-        for (int r = st_r0; r <= st_r1; r++)
-          for (int c = staged + lane; c < st_hi; c += 32) t(p, r, c) = __ldcg(a.plane[p] + (size_t)r * W + c);
-      staged = st_hi;
-    }
+  // Flushing stores the final columns; publishing (a release by lane 0 after
+  // a warp barrier, so it covers every lane's stores) happens after the
+  // group's steps, by which time the stores have drained.
+  int published = a.c_lo;
+  auto flush = [&](int hi) {
+    if (hi <= flushed) return;
+#pragma unroll
+    for (int p = 0; p < NS; p++)
+      for (int c = flushed + lc; c < hi; c += 16)
+        for (int r = r0 + lr; r <= out_r1; r += 2) __stcg(dst[p] + (size_t)r * W + c, t(p, r, c));
+    flushed = hi;
+  };
+  auto publish = [&]() {
+    if (flushed <= published) return;
     __syncwarp();
+    if (lane == 0) st_release(a.progress + ticket, flushed > a.c_hi ? INT_MAX : flushed);
+    published = flushed;
+  };
+
+  // Prologue: columns [c_lo - HALO, c_lo + GS + HALO), waited for and loaded.
+  int staged = min(a.c_lo + GS + HALO, c_stop);
+  wait_above(min(staged, a.c_hi + 1));
+#pragma unroll
+  for (int p = 0; p < NP; p++)
+    for (int c = a.c_lo - HALO + lc; c < staged; c += 16)
+      for (int r = st_r0 + lr; r <= st_r1; r += 2) {
+        const float* g = src[p] + (size_t)r * W + c;
+        if (upper(p, r))
+          t(p, r, c) = __ldcg(g);
+        else
+          cp_async4(&t(p, r, c), g);
+      }
+  cp_async_commit();
+
+  // Upper-halo values of the next group's columns, held in registers until
+  // the group starts (at most one per state plane per lane: GS columns x
+  // HALO rows spread over the 32 lanes).
+  float nh[NS];
+  int nh_lo = 0, nh_hi = 0;
+
+  for (int t0 = a.c_lo; t0 <= t_end; t0 += GS) {
+    flush(min(t0 - SPAN, a.c_hi + 1));
+    if (nh_hi > nh_lo) {
+#pragma unroll
+      for (int p = 0; p < NS; p++) {
+        const int c = nh_lo + lc, r = st_r0 + lr;
+        if (c < nh_hi && upper(p, r)) t(p, r, c) = nh[p];
+      }
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    const int lo = staged, hi = min(t0 + 2 * GS + HALO, c_stop);
+    nh_lo = nh_hi = 0;
+    if (hi > lo) {
+      wait_above(min(hi, a.c_hi + 1));
+#pragma unroll
+      for (int p = 0; p < NP; p++) {
+        const int c = lo + lc;
+        if (c >= hi) continue;
+        for (int r = st_r0 + lr; r <= st_r1; r += 2) {
+          const float* g = src[p] + (size_t)r * W + c;
+          if (upper(p, r)) {
+            if (p < NS) nh[p < NS ? p : 0] = __ldcg(g);
+          } else {
+            cp_async4(&t(p, r, c), g);
+          }
+        }
+      }
+      cp_async_commit();
+      nh_lo = lo;
+      nh_hi = hi;
+      staged = hi;
+    }
     const int r = r0 + lane;
     const bool row_on = r <= a.r_hi;
-    for (int s = 0; s < 32; s++) {
-      const int c = t0 + s - SKEW * lane;
+#pragma unroll 4
+    for (int s = 0; s < GS; s++) {
+      const int c = t0 + s - Op::SKEW * (lane / Op::PAIR);
       if (row_on && c >= a.c_lo && c <= a.c_hi) Op::cell(t, r, c, a.g);
       __syncwarp();
     }
+    publish();
   }
+  cp_async_wait_all();
   flush(a.c_hi + 1);
+  publish();
 }
 
 template <class Op>
 lre_status sweep(Context* c, const SweepArgs& base, int* sync, int nb_max, const char* what) {
   if (base.r_hi < base.r_lo || base.c_hi < base.c_lo) return LRE_OK;
-  using R = Ring<Op::NP, Op::HALO, Op::SKEW>;
-  const int nb = (base.r_hi - base.r_lo + 32) / 32;
+  using R = RingOf<Op>;
+  const int nb = (base.r_hi - base.r_lo + 32) / 32 * Op::NCH;
   if (nb > nb_max) return fail(c, LRE_ERR_CUDA, std::string(what) + ": band table too small");
   SweepArgs a = base;
   a.ticket = sync;
@@ -582,7 +709,7 @@ size_t plane_bytes(size_t w, size_t h) { return (w * h * sizeof(float) + 255) & 
 }  // namespace
 
 size_t ws_bytes_dcb(size_t w, size_t h) {
-  const size_t nb = (h + 31) / 32 + 1;
+  const size_t nb = 2 * ((h + 31) / 32 + 1);
   return 7 * plane_bytes(w, h) + ((w * h + 255) & ~size_t(255)) + (kSyncInts + nb) * sizeof(int) + 1024;
 }
 
@@ -601,7 +728,7 @@ lre_status launch_dcb(Context* c, const float* raw, int raw_c_stride, float* rgb
   float* P3 = reinterpret_cast<float*>(take(pb));
   float* P4 = reinterpret_cast<float*>(take(pb));
   uint8_t* M = reinterpret_cast<uint8_t*>(take((w * h + 255) & ~size_t(255)));
-  const int nb_max = (int)((h + 31) / 32 + 1);
+  const int nb_max = 2 * (int)((h + 31) / 32 + 1);
   int* sync = reinterpret_cast<int*>(take((kSyncInts + nb_max) * sizeof(int)));
   if (!R || !G || !B || !P1 || !P2 || !P3 || !P4 || !M || !sync)
     return fail(c, LRE_ERR_CUDA, "demosaic_bayer_dcb: workspace not reserved");
@@ -635,21 +762,24 @@ lre_status launch_dcb(Context* c, const float* raw, int raw_c_stride, float* rgb
     x.c_hi = W - 1 - m;
     return x;
   };
+  if (iterations > 0) DCB_LAUNCH(k_dcb_nyq_terms, R, B, P1, P2, g);
   for (int it = 1; it <= iterations; it++) {
     SweepArgs ny = rect(sa, 2);
     ny.plane[0] = G;
-    ny.plane[1] = R;
-    ny.plane[2] = B;
+    ny.plane[1] = P1;
+    ny.plane[2] = P2;
     for (int k = 0; k < 3; k++) LRE_TRY(sweep<OpNyquist>(c, ny, sync, nb_max, "dcb_nyquist"));
     DCB_LAUNCH(k_dcb_map, G, M, g);
     DCB_LAUNCH(k_dcb_correction, G, M, g);
   }
   DCB_LAUNCH(k_dcb_color, raw, raw_c_stride, G, R, B, g);
   {
+    DCB_LAUNCH(k_dcb_pp_terms, G, P1, g);
     SweepArgs pp = rect(sa, 2);
     pp.plane[0] = R;
     pp.plane[1] = B;
-    pp.plane[2] = G;
+    pp.plane[2] = P1;
+    pp.plane[3] = P1;
     LRE_TRY(sweep<OpPP>(c, pp, sync, nb_max, "dcb_pp"));
   }
   DCB_LAUNCH(k_dcb_map, G, M, g);
