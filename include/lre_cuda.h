@@ -276,6 +276,20 @@ lre_status lre_dev_demosaic_bayer_dcb(lre_ctx* ctx, const float* raw, float* rgb
                                       size_t height, uint32_t filters, float maximum_value, int iterations,
                                       int dcb_enhance);
 
+/* Accelerator::demosaic_bayer_aahd (core/accelerator.h:269-271; the
+ * reference GPU path falls back to the CPU, core/accelerator.cpp:159-178) and
+ * CPUAccelerator::demosaic_bayer_aahd (core/cpu_accelerator.cpp:617-633):
+ * hot-pixel hiding, directional greens and colours, YUV homogeneity choice
+ * and refinement, /max, 2-px border interpolation.  Results equal the
+ * reference run with one OpenMP thread.  Needs a 2x2 Bayer layout and
+ * samples in [0, 65536) (the reference indexes a 64 Ki gamma table with
+ * them).  Sparse (H,W,3) raw in. */
+lre_status lre_demosaic_bayer_aahd(lre_ctx* ctx, const float* raw_rgb, float* rgb, size_t width,
+                                   size_t height, uint32_t filters, float maximum_value);
+/* Same on a dense device mosaic; returns after the stream has drained. */
+lre_status lre_dev_demosaic_bayer_aahd(lre_ctx* ctx, const float* raw, float* rgb, size_t width,
+                                       size_t height, uint32_t filters, float maximum_value);
+
 /* ------------------------------------------------------ output end */
 /* GPUAccelerator::convert_color_space (core/gpu_accelerator.h:66-69;
  * core/cpu_accelerator.cpp:2874-2897): out = M[:, :3] * in + M[:, 3] with

@@ -183,6 +183,14 @@ class CudaAccelerator:
                                                      int(bool(dcb_enhance))))
         return out
 
+    def demosaic_bayer_aahd(self, raw_rgb, filters: int, maximum_value: float = 1.0):
+        """AAHD demosaic (Accelerator::demosaic_bayer_aahd, core/accelerator.h:269-271)."""
+        raw = _rgb(raw_rgb, "demosaic_bayer_aahd")
+        out = np.empty_like(raw)
+        self._check(self._lib.lre_demosaic_bayer_aahd(self._h, _ptr(raw), _ptr(out), raw.shape[1], raw.shape[0],
+                                                      int(filters), float(maximum_value)))
+        return out
+
     def demosaic_xtrans_1pass(self, raw_rgb, xtrans, color_matrix=None, maximum_value: float = 1.0):
         return self._xtrans(raw_rgb, xtrans, color_matrix, maximum_value, 1)
 
@@ -315,6 +323,10 @@ class CudaAccelerator:
         self._check(self._lib.lre_dev_demosaic_bayer_dcb(self._h, _dptr(raw), _dptr(rgb), int(width), int(height),
                                                          int(filters), float(maximum_value), int(iterations),
                                                          int(bool(dcb_enhance))))
+
+    def dev_demosaic_bayer_aahd(self, raw, rgb, width, height, filters, maximum_value=1.0):
+        self._check(self._lib.lre_dev_demosaic_bayer_aahd(self._h, _dptr(raw), _dptr(rgb), int(width), int(height),
+                                                          int(filters), float(maximum_value)))
 
     def dev_demosaic_xtrans(self, raw, rgb, width, height, xtrans, maximum_value=1.0, passes=3):
         self._check(self._lib.lre_dev_demosaic_xtrans(self._h, _dptr(raw), _dptr(rgb), int(width), int(height), _xtrans_bytes(xtrans), float(maximum_value), int(passes)))

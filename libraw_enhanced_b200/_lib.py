@@ -186,6 +186,8 @@ SIGNATURES = {
     "lre_dev_demosaic_bayer_linear": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _f]),
     "lre_demosaic_bayer_dcb": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _f, C.c_int, C.c_int]),
     "lre_dev_demosaic_bayer_dcb": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _f, C.c_int, C.c_int]),
+    "lre_demosaic_bayer_aahd": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _f]),
+    "lre_dev_demosaic_bayer_aahd": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _f]),
     "lre_convert_color_space": (_st, [_p, _p, _p, _sz, _sz, _p]),
     "lre_gamma_correct": (_st, [_p, _p, _p, _sz, _sz, _f, _f, _i]),
     "lre_dev_convert_color_space": (_st, [_p, _p, _p, _sz, _sz, _p]),

@@ -230,7 +230,7 @@ lre_status lre_dev_demosaic_bayer_dcb(lre_ctx* ctx, const float* raw, float* rgb
   if (!c) return LRE_ERR_INVALID_ARGUMENT;
   LRE_TRY(check_img(c, raw, rgb, w, h, "demosaic_bayer_dcb"));
   LRE_TRY(begin(c, lre::ws_bytes_dcb(w, h)));
-  return lre::launch_dcb(c, raw, 1, rgb, w, h, filters, maximum_value, iterations, dcb_enhance != 0);
+  return lre::launch_dcb(c, raw, 1, rgb, w, h, filters, maximum_value, iterations, dcb_enhance != 0, nullptr);
 }
 
 lre_status lre_demosaic_bayer_dcb(lre_ctx* ctx, const float* raw_rgb, float* rgb, size_t w, size_t h,
@@ -246,7 +246,35 @@ lre_status lre_demosaic_bayer_dcb(lre_ctx* ctx, const float* raw_rgb, float* rgb
   float* din = reinterpret_cast<float*>(c->d_in);
   float* dout = reinterpret_cast<float*>(c->d_out);
   LRE_CUDA_TRY(c, cudaMemcpyAsync(din, raw_rgb, bytes, cudaMemcpyHostToDevice, c->stream));
-  LRE_TRY(lre::launch_dcb(c, din, 3, dout, w, h, filters, maximum_value, iterations, dcb_enhance != 0));
+  LRE_TRY(lre::launch_dcb(c, din, 3, dout, w, h, filters, maximum_value, iterations, dcb_enhance != 0, nullptr));
+  LRE_CUDA_TRY(c, cudaMemcpyAsync(rgb, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return LRE_OK;
+}
+
+lre_status lre_dev_demosaic_bayer_aahd(lre_ctx* ctx, const float* raw, float* rgb, size_t w, size_t h,
+                                       uint32_t filters, float maximum_value) {
+  Context* c = C(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  LRE_TRY(check_img(c, raw, rgb, w, h, "demosaic_bayer_aahd"));
+  LRE_TRY(begin(c, lre::ws_bytes_aahd(w, h)));
+  return lre::launch_aahd(c, raw, 1, rgb, w, h, filters, maximum_value, nullptr);
+}
+
+lre_status lre_demosaic_bayer_aahd(lre_ctx* ctx, const float* raw_rgb, float* rgb, size_t w, size_t h,
+                                   uint32_t filters, float maximum_value) {
+  Context* c = C(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  LRE_TRY(check_img(c, raw_rgb, rgb, w, h, "demosaic_bayer_aahd"));
+  std::lock_guard<std::mutex> lk(c->mu);
+  LRE_TRY(begin(c, lre::ws_bytes_aahd(w, h)));
+  const size_t bytes = w * h * 3 * sizeof(float);
+  LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, bytes));
+  LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, bytes));
+  float* din = reinterpret_cast<float*>(c->d_in);
+  float* dout = reinterpret_cast<float*>(c->d_out);
+  LRE_CUDA_TRY(c, cudaMemcpyAsync(din, raw_rgb, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::launch_aahd(c, din, 3, dout, w, h, filters, maximum_value, nullptr));
   LRE_CUDA_TRY(c, cudaMemcpyAsync(rgb, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;

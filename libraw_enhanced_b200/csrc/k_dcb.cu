@@ -24,48 +24,23 @@
 // (Three of these are OpenMP row-parallel loops in the reference, so with
 // more than one thread rows at chunk boundaries depend on timing; the
 // sequential order is the defined result and the one computed here.)
-// k_dcb_sweep evaluates them in exactly that order: a warp owns a band of 32
-// rows (lane = row), walks the columns with a skew of SKEW columns per row,
-// so every neighbour that precedes a site in row-major order has already
-// been updated and every one that follows has not; the band's rows, halo
-// rows and inputs are staged through a shared-memory ring of 128 columns.
-// Bands are chained through per-band progress counters in global memory (a
-// band stages its upper halo only once the band above has flushed those
-// columns); band numbers are handed out in CTA start order by an atomic
-// ticket, so a band only ever waits for one that is already running.  Every
-// wait is bounded: on time-out the kernel raises an error flag, stops
-// waiting and the host reports the failure.
+// k_gs_sweep (sweep.cuh) evaluates them in exactly that order with one warp
+// per 32-row band walking the columns on a skewed wavefront.
 //
 // Arithmetic is the reference's, operation for operation (--fmad=false); the
 // result is bit-identical to the reference run single-threaded.
-#include <climits>
-
 #include "common.cuh"
 #include "lre_internal.h"
 #include "stencil.cuh"
+#include "sweep.cuh"
 
 namespace lre {
 
 namespace {
 
-constexpr int kRing = 128;  // shared-memory ring width in columns (power of two)
-
 __device__ __forceinline__ float dclip(float v, float m) { return v > m ? m : (v < 0.0f ? 0.0f : v); }
 // ulim_generic (core/metal/shader_common.h:37-42)
 __device__ __forceinline__ float ulim(float v, float hi, float lo) { return v > hi ? hi : (v < lo ? lo : v); }
-
-struct Geo {
-  int W, H;
-  uint32_t filters;
-  float maxv;
-  __device__ __forceinline__ unsigned fc(int r, int c) const { return fcol3((unsigned)r, (unsigned)c, filters); }
-  __device__ __forceinline__ size_t at(int r, int c) const { return (size_t)r * W + c; }
-};
-
-// 2D launch helper: (32 x 8) threads, grid-strided in y.
-#define DCB_FOR_PIXELS(g)                                                             \
-  for (int r = blockIdx.y * blockDim.y + threadIdx.y; r < (g).H; r += gridDim.y * blockDim.y) \
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < (g).W; c += gridDim.x * blockDim.x)
 
 __device__ __forceinline__ float raw_at(const float* __restrict__ raw, int cs, const Geo& g, int r, int c) {
   const size_t i = g.at(r, c);
@@ -77,7 +52,7 @@ __device__ __forceinline__ float raw_at(const float* __restrict__ raw, int cs, c
 // the 8-neighbourhood (summed in row-major order).
 __global__ void k_dcb_init(const float* __restrict__ raw, int cs, float* __restrict__ R, float* __restrict__ G,
                            float* __restrict__ B, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     const unsigned f = g.fc(r, c);
     float v[3] = {0.0f, 0.0f, 0.0f};
     v[f] = raw_at(raw, cs, g, r, c);
@@ -108,7 +83,7 @@ __global__ void k_dcb_init(const float* __restrict__ raw, int cs, float* __restr
 // non-green sites of rows/cols [2, n-3]; zero elsewhere (the scratch images
 // start zeroed).
 __global__ void k_dcb_hv(const float* __restrict__ G, float* __restrict__ H1, float* __restrict__ V1, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     const size_t i = g.at(r, c);
     float h = 0.0f, v = 0.0f;
     if (g.fc(r, c) != 1 && r >= 2 && r < g.H - 2 && c >= 2 && c < g.W - 2) {
@@ -126,7 +101,7 @@ __global__ void k_dcb_hv(const float* __restrict__ G, float* __restrict__ H1, fl
 // which dcb_decide never reads.)
 __global__ void k_dcb_hvc(const float* __restrict__ R, const float* __restrict__ B, const float* __restrict__ H1,
                           const float* __restrict__ V1, float* __restrict__ HC, float* __restrict__ VC, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     const size_t i = g.at(r, c);
     float hc = 0.0f, vc = 0.0f;
     const unsigned f = g.fc(r, c);
@@ -165,7 +140,7 @@ __device__ __forceinline__ float spread(const float* __restrict__ Pa, const floa
 __global__ void k_dcb_decide(const float* __restrict__ R, const float* __restrict__ B, const float* __restrict__ H1,
                              const float* __restrict__ V1, const float* __restrict__ HC,
                              const float* __restrict__ VC, float* __restrict__ G, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     const unsigned f = g.fc(r, c);
     if (f == 1 || r < 2 || r >= g.H - 2 || c < 2 || c >= g.W - 2) continue;
     const size_t i = g.at(r, c), u = g.W;
@@ -178,7 +153,7 @@ __global__ void k_dcb_decide(const float* __restrict__ R, const float* __restric
 
 // dcb_map (:917-930): direction flag per pixel of rows/cols [1, n-2].
 __global__ void k_dcb_map(const float* __restrict__ G, uint8_t* __restrict__ M, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     if (r < 1 || r >= g.H - 1 || c < 1 || c >= g.W - 1) continue;
     const size_t i = g.at(r, c), u = g.W;
     const float w = G[i - 1], e = G[i + 1], n = G[i - u], s = G[i + u];
@@ -200,7 +175,7 @@ __device__ __forceinline__ int map_weight(const uint8_t* __restrict__ M, size_t 
 // non-green sites re-blended from the map-weighted directions.  Both read
 // green only at green sites, so they run in place.
 __global__ void k_dcb_correction(float* __restrict__ G, const uint8_t* __restrict__ M, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     if (g.fc(r, c) == 1 || r < 2 || r >= g.H - 2 || c < 2 || c >= g.W - 2) continue;
     const size_t i = g.at(r, c), u = g.W;
     const int cur = map_weight(M, i, u);
@@ -210,7 +185,7 @@ __global__ void k_dcb_correction(float* __restrict__ G, const uint8_t* __restric
 
 __global__ void k_dcb_correction2(float* __restrict__ G, const float* __restrict__ R, const float* __restrict__ B,
                                   const uint8_t* __restrict__ M, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     const unsigned f = g.fc(r, c);
     if (f == 1 || r < 4 || r >= g.H - 4 || c < 4 || c >= g.W - 4) continue;
     const size_t i = g.at(r, c), u = g.W, v = 2 * (size_t)g.W;
@@ -230,7 +205,7 @@ __global__ void k_dcb_correction2(float* __restrict__ G, const float* __restrict
 // is a native sample, so the kernel reads the mosaic instead of R/B.
 __global__ void k_dcb_color(const float* __restrict__ raw, int cs, const float* __restrict__ G,
                             float* __restrict__ R, float* __restrict__ B, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     const size_t i = g.at(r, c), u = g.W;
     const unsigned f = g.fc(r, c);
     float rv = 0.0f, bv = 0.0f;
@@ -269,7 +244,7 @@ __global__ void k_dcb_color(const float* __restrict__ raw, int cs, const float* 
 __global__ void k_dcb_refine_pre(const float* __restrict__ G, const float* __restrict__ R,
                                  const float* __restrict__ B, const uint8_t* __restrict__ M,
                                  float* __restrict__ V, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     const unsigned f = g.fc(r, c);
     if (f == 1 || r < 4 || r >= g.H - 4 || c < 4 || c >= g.W - 4) continue;
     const size_t i = g.at(r, c), u = g.W, v = 2 * (size_t)g.W, w = 3 * (size_t)g.W;
@@ -312,7 +287,7 @@ __device__ __forceinline__ float chroma_native(const float* __restrict__ R, cons
 
 __global__ void k_dcb_chroma(const float* __restrict__ R, const float* __restrict__ B, const float* __restrict__ G,
                              float* __restrict__ C0, float* __restrict__ C1, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     const unsigned f = g.fc(r, c);
     if (f == 1) continue;
     const float nat = chroma_native(R, B, G, g, r, c);
@@ -342,7 +317,7 @@ __global__ void k_dcb_chroma(const float* __restrict__ R, const float* __restric
 // [6, n-7].
 __global__ void k_dcb_chroma_g(const float* __restrict__ C0, const float* __restrict__ C1,
                                const float* __restrict__ G, float* __restrict__ V0, float* __restrict__ V2, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     if (r < 6 || r >= g.H - 6 || c < 6 || c >= g.W - 6) continue;
     const size_t i = g.at(r, c), u = g.W, w = 3 * (size_t)g.W;
     float cr[2];
@@ -371,7 +346,7 @@ __global__ void k_dcb_chroma_g(const float* __restrict__ C0, const float* __rest
 
 __global__ void k_dcb_output(const float* __restrict__ R, const float* __restrict__ G, const float* __restrict__ B,
                              float* __restrict__ rgb, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     const size_t i = g.at(r, c);
     rgb[i * 3 + 0] = R[i] / g.maxv;
     rgb[i * 3 + 1] = G[i] / g.maxv;
@@ -383,7 +358,7 @@ __global__ void k_dcb_output(const float* __restrict__ R, const float* __restric
 // sample and (S + N + W + E) / 4 of the same colour two sites away.
 __global__ void k_dcb_nyq_terms(const float* __restrict__ R, const float* __restrict__ B, float* __restrict__ A,
                                 float* __restrict__ Q, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     const unsigned f = g.fc(r, c);
     if (f == 1 || r < 2 || r >= g.H - 2 || c < 2 || c >= g.W - 2) continue;
     const size_t i = g.at(r, c), v = 2 * (size_t)g.W;
@@ -395,7 +370,7 @@ __global__ void k_dcb_nyq_terms(const float* __restrict__ R, const float* __rest
 
 // dcb_pp's green term G - mean8(G), in the reference's summation order.
 __global__ void k_dcb_pp_terms(const float* __restrict__ G, float* __restrict__ K, Geo g) {
-  DCB_FOR_PIXELS(g) {
+  GS_FOR_PIXELS(g) {
     if (r < 2 || r >= g.H - 2 || c < 2 || c >= g.W - 2) continue;
     const size_t i = g.at(r, c), u = g.W;
     const float g1 = (G[i - 1] + G[i + 1] + G[i - u] + G[i + u] + G[i - u - 1] + G[i + u + 1] + G[i - u + 1] +
@@ -407,31 +382,6 @@ __global__ void k_dcb_pp_terms(const float* __restrict__ G, float* __restrict__ 
 
 // ------------------------------------------------------------------ sweeps
 
-struct SweepArgs {
-  float* plane[4];  // state planes first, then read-only inputs
-  Geo g;
-  int r_lo, r_hi, c_lo, c_hi;  // updated rectangle (inclusive)
-  int* ticket;
-  int* err;
-  int* progress;  // per band: columns < progress[b] of band b are final in HBM
-};
-
-// The sweep's shared-memory ring, addressed through the __shared__ symbol
-// itself so every access compiles to a shared-memory instruction.
-extern __shared__ float sweep_smem[];
-
-template <int NP, int HALO, int PAD>
-struct Ring {
-  static constexpr int ROWS = 32 + 2 * HALO;
-  static constexpr int PITCH = kRing + PAD;
-  static constexpr int PLANE = ROWS * PITCH;
-  static constexpr size_t BYTES = (size_t)NP * PLANE * sizeof(float);
-  int rbase;
-  __device__ __forceinline__ float& operator()(int p, int r, int c) const {
-    return sweep_smem[p * PLANE + (r - rbase) * PITCH + (c & (kRing - 1))];
-  }
-};
-
 // Each sweep op names its planes per warp: NS state planes first, then
 // inputs.  NCH = 2 runs two independent channels (R and B) as separate
 // warps; PAIR = 2 gives two adjacent rows the same column when a row only
@@ -442,7 +392,7 @@ struct Ring {
 // R and B do not change across the nyquist passes).  A site reads rows r +- 2
 // only, so rows r and r + 1 advance together.
 struct OpNyquist {
-  static constexpr int NS = 1, NP = 3, HALO = 2, SKEW = 1, PAIR = 2, NCH = 1;
+  static constexpr int NS = 1, NP = 3, HALO = 2, SKEW = 1, PAIR = 2, NCH = 1, LAG = 0;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo& g) {
     if (g.fc(r, c) == 1) return;
@@ -455,7 +405,7 @@ struct OpNyquist {
 // dcb_pp (:820-834), one channel (R or B) per warp: state the channel;
 // input K = G - mean8(G) (k_dcb_pp_terms; green does not change in the pass).
 struct OpPP {
-  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 2;
+  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 2, LAG = 0;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo& g) {
     const float x1 = (t(0, r, c - 1) + t(0, r, c + 1) + t(0, r - 1, c) + t(0, r + 1, c) + t(0, r - 1, c - 1) +
@@ -476,7 +426,7 @@ __device__ __forceinline__ void clamp8(const T& t, int p, int r, int c, float v)
 
 // dcb_refinement's closing clamp (:992-994): state G; input the pre-clamp value.
 struct OpRefine {
-  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 1;
+  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 1, LAG = 0;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo& g) {
     if (g.fc(r, c) == 1) return;
@@ -487,222 +437,12 @@ struct OpRefine {
 // dcb_color_full's last loop (:898-913), one channel per warp: state R or B;
 // input that channel's CLIP(chroma + G).
 struct OpColorFull {
-  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 2;
+  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 2, LAG = 0;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo&) {
     clamp8(t, 0, r, c, t(1, r, c));
   }
 };
-
-// Row padding so the 32 lanes of a step hit 32 different banks: lane l
-// reads row l + k at column t - SKEW * (l / PAIR), so with PAIR = 1 a pitch
-// of SKEW + 1 (mod 32) gives bank l + const; with PAIR = 2 (SKEW = 1) a
-// pitch of 16 (mod 32) gives bank 16 * (l & 1) - l / 2 + const.
-template <class Op>
-using RingOf = Ring<Op::NP, Op::HALO, (Op::PAIR == 2 ? 16 : Op::SKEW + 1)>;
-
-__device__ __forceinline__ int ld_acquire(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release(int* p, int v) {
-  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
-
-__device__ __forceinline__ void cp_async4(float* s, const float* g) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-// Steps per group.  Each group first makes the columns it needs resident
-// (copies issued one group earlier), then issues the copies for the next
-// group, then runs its GS steps while those copies are in flight.
-constexpr int kGroup = 16;
-
-template <class Op>
-__global__ void __launch_bounds__(32) k_dcb_sweep(SweepArgs a) {
-  using R = RingOf<Op>;
-  constexpr int HALO = Op::HALO, NS = Op::NS, NP = Op::NP, NCH = Op::NCH, GS = kGroup;
-  constexpr int SPAN = Op::SKEW * (31 / Op::PAIR);  // column lag of lane 31 behind lane 0
-  const int lane = threadIdx.x, lc = lane & 15, lr = lane >> 4;
-  int ticket = 0;
-  if (lane == 0) ticket = atomicAdd(a.ticket, 1);
-  ticket = __shfl_sync(0xffffffffu, ticket, 0);
-  // Tickets go out in CTA start order; ticket k is band k / NCH, channel
-  // k % NCH, and waits only for ticket k - NCH (same channel, band above).
-  const int band = ticket / NCH, ch = ticket % NCH;
-  // Per-warp plane pointers (with NCH = 2 the argument holds
-  // {state ch0, state ch1, input ch0, input ch1}).
-  const float* src[NP];
-  float* dst[NS];
-#pragma unroll
-  for (int p = 0; p < NP; p++) {
-    if (NCH == 1) src[p] = a.plane[p];
-    else src[p] = p < NS ? (ch ? a.plane[1] : a.plane[0]) : (ch ? a.plane[3] : a.plane[2]);
-  }
-#pragma unroll
-  for (int p = 0; p < NS; p++) dst[p] = NCH == 1 ? a.plane[p] : (ch ? a.plane[1] : a.plane[0]);
-  const int r0 = a.r_lo + band * 32;
-  const int W = a.g.W, H = a.g.H;
-  const R t{r0 - HALO};
-  const int st_r0 = max(r0 - HALO, 0), st_r1 = min(r0 + 31 + HALO, H - 1);
-  const int out_r1 = min(r0 + 31, a.r_hi);
-  const int t_end = a.c_hi + SPAN;
-  const int c_stop = a.c_hi + HALO + 1;  // staging never reaches past this column
-  int flushed = a.c_lo;
-  bool waiting = band > 0;
-
-  // Rows above r0 belong to the band above: its state planes are read only
-  // after that band has flushed the columns, and with L2-coherent loads.
-  auto upper = [&](int p, int r) { return band > 0 && p < NS && r < r0; };
-
-  // Progress of the band above as last observed by lane 0 (acquire loads;
-  // the warp barrier after the wait orders every lane's later loads).
-  int above = 0;
-  auto wait_above = [&](int need) {
-    if (!waiting) return;
-    int ok = 1;
-    if (lane == 0 && above < need) {
-      const long long start = clock64();
-      while ((above = ld_acquire(a.progress + ticket - NCH)) < need) {
-        __nanosleep(32);
-        if (clock64() - start > kWaitCycles) {
-          atomicExch(a.err, 1);
-          ok = 0;
-          break;
-        }
-      }
-    }
-    if (!__shfl_sync(0xffffffffu, ok, 0)) waiting = false;
-  };
-
-  // Flushing stores the final columns; publishing (a release by lane 0 after
-  // a warp barrier, so it covers every lane's stores) happens after the
-  // group's steps, by which time the stores have drained.
-  int published = a.c_lo;
-  auto flush = [&](int hi) {
-    if (hi <= flushed) return;
-#pragma unroll
-    for (int p = 0; p < NS; p++)
-      for (int c = flushed + lc; c < hi; c += 16)
-        for (int r = r0 + lr; r <= out_r1; r += 2) __stcg(dst[p] + (size_t)r * W + c, t(p, r, c));
-    flushed = hi;
-  };
-  auto publish = [&]() {
-    if (flushed <= published) return;
-    __syncwarp();
-    if (lane == 0) st_release(a.progress + ticket, flushed > a.c_hi ? INT_MAX : flushed);
-    published = flushed;
-  };
-
-  // Prologue: columns [c_lo - HALO, c_lo + GS + HALO), waited for and loaded.
-  int staged = min(a.c_lo + GS + HALO, c_stop);
-  wait_above(min(staged, a.c_hi + 1));
-#pragma unroll
-  for (int p = 0; p < NP; p++)
-    for (int c = a.c_lo - HALO + lc; c < staged; c += 16)
-      for (int r = st_r0 + lr; r <= st_r1; r += 2) {
-        const float* g = src[p] + (size_t)r * W + c;
-        if (upper(p, r))
-          t(p, r, c) = __ldcg(g);
-        else
-          cp_async4(&t(p, r, c), g);
-      }
-  cp_async_commit();
-
-  // Upper-halo values of the next group's columns, held in registers until
-  // the group starts (at most one per state plane per lane: GS columns x
-  // HALO rows spread over the 32 lanes).
-  float nh[NS];
-  int nh_lo = 0, nh_hi = 0;
-
-  for (int t0 = a.c_lo; t0 <= t_end; t0 += GS) {
-    flush(min(t0 - SPAN, a.c_hi + 1));
-    if (nh_hi > nh_lo) {
-#pragma unroll
-      for (int p = 0; p < NS; p++) {
-        const int c = nh_lo + lc, r = st_r0 + lr;
-        if (c < nh_hi && upper(p, r)) t(p, r, c) = nh[p];
-      }
-    }
-    cp_async_wait_all();
-    __syncwarp();
-    const int lo = staged, hi = min(t0 + 2 * GS + HALO, c_stop);
-    nh_lo = nh_hi = 0;
-    if (hi > lo) {
-      wait_above(min(hi, a.c_hi + 1));
-#pragma unroll
-      for (int p = 0; p < NP; p++) {
-        const int c = lo + lc;
-        if (c >= hi) continue;
-        for (int r = st_r0 + lr; r <= st_r1; r += 2) {
-          const float* g = src[p] + (size_t)r * W + c;
-          if (upper(p, r)) {
-            if (p < NS) nh[p < NS ? p : 0] = __ldcg(g);
-          } else {
-            cp_async4(&t(p, r, c), g);
-          }
-        }
-      }
-      cp_async_commit();
-      nh_lo = lo;
-      nh_hi = hi;
-      staged = hi;
-    }
-    const int r = r0 + lane;
-    const bool row_on = r <= a.r_hi;
-#pragma unroll 4
-    for (int s = 0; s < GS; s++) {
-      const int c = t0 + s - Op::SKEW * (lane / Op::PAIR);
-      if (row_on && c >= a.c_lo && c <= a.c_hi) Op::cell(t, r, c, a.g);
-      __syncwarp();
-    }
-    publish();
-  }
-  cp_async_wait_all();
-  flush(a.c_hi + 1);
-  publish();
-}
-
-template <class Op>
-lre_status sweep(Context* c, const SweepArgs& base, int* sync, int nb_max, const char* what) {
-  if (base.r_hi < base.r_lo || base.c_hi < base.c_lo) return LRE_OK;
-  using R = RingOf<Op>;
-  const int nb = (base.r_hi - base.r_lo + 32) / 32 * Op::NCH;
-  if (nb > nb_max) return fail(c, LRE_ERR_CUDA, std::string(what) + ": band table too small");
-  SweepArgs a = base;
-  a.ticket = sync;
-  a.progress = sync + 64;
-  LRE_CUDA_TRY(c, cudaMemsetAsync(sync, 0, sizeof(int), c->stream));
-  LRE_CUDA_TRY(c, cudaMemsetAsync(a.progress, 0, (size_t)nb * sizeof(int), c->stream));
-  LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_dcb_sweep<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R::BYTES));
-  k_dcb_sweep<Op><<<nb, 32, R::BYTES, c->stream>>>(a);
-  count_launch(c);
-  return check_launch(c, what);
-}
-
-bool bayer_2x2(uint32_t filters) {
-  // DCB's loops address non-green sites by column parity; that is the
-  // reference's intent only for 2x2 Bayer layouts with green on a
-  // checkerboard and R/B on the other two sites.
-  for (unsigned r = 0; r < 8; r++) {
-    const unsigned a = fcol3(r, 0, filters), b = fcol3(r, 1, filters);
-    if ((a == 1) == (b == 1)) return false;
-    if (fcol3(r, 2, filters) != a || fcol3((r + 2) & 7, 0, filters) != a || fcol3((r + 2) & 7, 1, filters) != b)
-      return false;
-  }
-  const unsigned n0 = fcol3(0, 0, filters) == 1 ? fcol3(0, 1, filters) : fcol3(0, 0, filters);
-  const unsigned n1 = fcol3(1, 0, filters) == 1 ? fcol3(1, 1, filters) : fcol3(1, 0, filters);
-  if (fcol3(0, 0, filters) == 1 && fcol3(1, 0, filters) == 1) return false;
-  return n0 + n1 == 2 && n0 != n1;
-}
-
-constexpr int kSyncInts = 64;  // ticket, error flag, then per-band progress
 
 size_t plane_bytes(size_t w, size_t h) { return (w * h * sizeof(float) + 255) & ~size_t(255); }
 
@@ -714,7 +454,7 @@ size_t ws_bytes_dcb(size_t w, size_t h) {
 }
 
 lre_status launch_dcb(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
-                      uint32_t filters, float maximum_value, int iterations, bool enhance) {
+                      uint32_t filters, float maximum_value, int iterations, bool enhance, int* d_err) {
   if (!bayer_2x2(filters))
     return fail(c, LRE_ERR_INVALID_ARGUMENT, "demosaic_bayer_dcb: needs a 2x2 Bayer layout (RGGB/BGGR/GRBG/GBRG)");
   if (iterations < 0) return fail(c, LRE_ERR_INVALID_ARGUMENT, "demosaic_bayer_dcb: negative iterations");
@@ -745,7 +485,8 @@ lre_status launch_dcb(Context* c, const float* raw, int raw_c_stride, float* rgb
   } while (0)
 
   LRE_CUDA_TRY(c, cudaMemsetAsync(M, 0, w * h, s));
-  LRE_CUDA_TRY(c, cudaMemsetAsync(sync + 1, 0, sizeof(int), s));  // error flag
+  int* err = d_err ? d_err : sync + 1;
+  if (!d_err) LRE_CUDA_TRY(c, cudaMemsetAsync(err, 0, sizeof(int), s));
   DCB_LAUNCH(k_dcb_init, raw, raw_c_stride, R, G, B, g);
   DCB_LAUNCH(k_dcb_hv, G, P1, P2, g);
   DCB_LAUNCH(k_dcb_hvc, R, B, P1, P2, P3, P4, g);
@@ -753,7 +494,7 @@ lre_status launch_dcb(Context* c, const float* raw, int raw_c_stride, float* rgb
 
   SweepArgs sa{};
   sa.g = g;
-  sa.err = sync + 1;
+  sa.err = err;
   const int W = (int)w, H = (int)h;
   auto rect = [&](SweepArgs x, int m) {
     x.r_lo = m;
@@ -808,10 +549,11 @@ lre_status launch_dcb(Context* c, const float* raw, int raw_c_stride, float* rgb
   DCB_LAUNCH(k_dcb_output, R, G, B, rgb, g);
 #undef DCB_LAUNCH
   LRE_TRY(launch_border_interp(c, rgb, w, h, filters, 3));
-  int err = 0;
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(&err, sync + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (d_err) return LRE_OK;  // the caller reads the flag after its own synchronisation
+  int e = 0;
+  LRE_CUDA_TRY(c, cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, s));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(s));
-  if (err) return fail(c, LRE_ERR_TIMEOUT, "demosaic_bayer_dcb: a sweep band timed out waiting for the band above");
+  if (e) return fail(c, LRE_ERR_TIMEOUT, "demosaic_bayer_dcb: a sweep band timed out waiting for the band above");
   return LRE_OK;
 }
 

@@ -184,9 +184,15 @@ namespace lre {
 lre_status launch_border_interp(Context* c, float* rgb, size_t w, size_t h, uint32_t filters, int band);
 lre_status launch_bayer_linear(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
                                uint32_t filters, float maximum_value);
-// DCB Bayer demosaic (k_dcb.cu).  Synchronises the stream at the end to read
-// the sweeps' error flag.
+// DCB and AAHD Bayer demosaics (k_dcb.cu, k_aahd.cu).  Their in-order
+// sweeps raise a device error flag if a band's bounded wait expires.  With
+// d_err == nullptr the launcher synchronises the stream and reports the flag
+// as LRE_ERR_TIMEOUT; otherwise it ORs into *d_err (device) and returns
+// without synchronising.
 size_t ws_bytes_dcb(size_t w, size_t h);
 lre_status launch_dcb(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
-                      uint32_t filters, float maximum_value, int iterations, bool enhance);
+                      uint32_t filters, float maximum_value, int iterations, bool enhance, int* d_err);
+size_t ws_bytes_aahd(size_t w, size_t h);
+lre_status launch_aahd(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
+                       uint32_t filters, float maximum_value, int* d_err);
 }  // namespace lre

@@ -63,6 +63,7 @@ _REF_SIGS = {
     "ref_demosaic_bayer_amaze": (C.c_int, [_p, _p, _sz, _sz, C.c_uint32, _p, _f]),
     "ref_demosaic_bayer_linear": (C.c_int, [_p, _p, _sz, _sz, C.c_uint32, _f]),
     "ref_demosaic_bayer_dcb": (C.c_int, [_p, _p, _sz, _sz, C.c_uint32, _f, C.c_int, C.c_int]),
+    "ref_demosaic_bayer_aahd": (C.c_int, [_p, _p, _sz, _sz, C.c_uint32, _f]),
     "ref_demosaic_xtrans": (C.c_int, [_p, _p, _sz, _sz, _p, _p, _f, C.c_int]),
     "ref_apply_white_balance": (C.c_int, [_p, _p, _sz, _sz, _p, C.c_uint32, _p]),
     "ref_tone_mapping": (C.c_int, [_p, _p, _sz, _sz, _f]),
@@ -163,6 +164,22 @@ def bayer_dcb(raw_sparse, filters, maximum=1.0, iterations=1, enhance=True, thre
     try:
         assert ref().ref_demosaic_bayer_dcb(_ptr(raw), _ptr(out), w, h, int(filters), float(maximum),
                                             int(iterations), int(bool(enhance)))
+    finally:
+        set_threads(saved)
+    return out
+
+
+def bayer_aahd(raw_sparse, filters, maximum=1.0, threads=1):
+    """The reference's AAHD demosaic (core/cpu_accelerator.cpp:617-633), by
+    default single-threaded: its in-place row loops and channel min/max scan
+    are order-dependent under OpenMP."""
+    raw = _img(raw_sparse)
+    h, w, _ = raw.shape
+    out = np.zeros_like(raw)
+    saved = num_threads()
+    set_threads(threads)
+    try:
+        assert ref().ref_demosaic_bayer_aahd(_ptr(raw), _ptr(out), w, h, int(filters), float(maximum))
     finally:
         set_threads(saved)
     return out

@@ -103,6 +103,17 @@ int ref_demosaic_bayer_linear(const float* raw, float* rgb, size_t w, size_t h, 
   return accel().demosaic_bayer_linear(in, out, filters, maximum_value) ? 1 : 0;
 }
 
+/* core/cpu_accelerator.cpp:617-633 (AAHD demosaic: AAHD_Processor at
+ * :177-601, border_interpolate(2)).  Its hide_hots and refine_hv_dirs are
+ * OpenMP row loops that rewrite in place, and its channel min/max scan is an
+ * unsynchronised OpenMP loop, so tests call this with one thread. */
+int ref_demosaic_bayer_aahd(const float* raw, float* rgb, size_t w, size_t h, uint32_t filters,
+                            float maximum_value) {
+  MuteCout m;
+  ImageBufferFloat in = fbuf(raw, w, h), out = fbuf(rgb, w, h);
+  return accel().demosaic_bayer_aahd(in, out, filters, maximum_value) ? 1 : 0;
+}
+
 /* core/cpu_accelerator.cpp:1043-1137 (DCB demosaic: sparse + 8-neighbour
  * bilinear seed, DCB_Processor::run_dcb at :998-1035, /maximum,
  * border_interpolate(3)).  Several of DCB's in-place passes are OpenMP
