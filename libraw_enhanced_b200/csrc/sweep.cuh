@@ -106,20 +106,65 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // group, then runs its GS steps while those copies are in flight.
 constexpr int kGroup = 16;
 
+// Groups staged ahead of the one being computed.
+constexpr int kAhead = 2;
+// Warps per CTA: one runs the steps, three move data.
+constexpr int kSweepWarps = 4;
+
+// One CTA per band (and channel), four warps:
+//   * warp 0 runs the GS-step groups, touching only shared memory;
+//   * warp 1 handles the band boundaries: in iteration g (while warp 0 runs
+//     group g) it publishes the progress of what it flushed in iteration
+//     g - 1, flushes the columns that became final with group g - 1, waits
+//     for the band above as far as group g + kAhead needs and loads those
+//     upper-halo rows (into registers; they reach the ring one iteration
+//     later);
+//   * warps 2 and 3 copy group g + kAhead's band-local rows and inputs with
+//     cp.async and wait for group g + 1's copies.
+// The warps meet at a named barrier once per group, so global-memory latency
+// overlaps the steps.  Ring capacity: a group reads columns down to
+// t0 - SPAN - HALO - LAG while the copies reach t0 + (kAhead + 1) * GS + HALO.
 template <class Op>
-__global__ void __launch_bounds__(32) k_gs_sweep(SweepArgs a) {
+__global__ void __launch_bounds__(kSweepWarps * 32) k_gs_sweep(SweepArgs a) {
   using R = RingOf<Op>;
   constexpr int HALO = Op::HALO, NS = Op::NS, NP = Op::NP, NCH = Op::NCH, GS = kGroup;
   constexpr int SPAN = Op::SKEW * (31 / Op::PAIR);  // column lag of lane 31 behind lane 0
+  static_assert((kAhead + 1) * GS + SPAN + 2 * HALO + Op::LAG <= kRing, "sweep ring too small for this op");
   if (a.skip_if_zero && *a.skip_if_zero == 0) return;
-  const int lane = threadIdx.x, lc = lane & 15, lr = lane >> 4;
-  int ticket = 0;
-  if (lane == 0) ticket = atomicAdd(a.ticket, 1);
-  ticket = __shfl_sync(0xffffffffu, ticket, 0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, lc = lane & 15, lr = lane >> 4;
+  __shared__ int s_ticket;
+  if (threadIdx.x == 0) s_ticket = atomicAdd(a.ticket, 1);
+  __syncthreads();
   // Tickets go out in CTA start order; ticket k is band k / NCH, channel
   // k % NCH, and waits only for ticket k - NCH (same channel, band above).
+  const int ticket = s_ticket;
   const int band = ticket / NCH, ch = ticket % NCH;
-  // Per-warp plane pointers (with NCH = 2 the argument holds
+  const int r0 = a.r_lo + band * 32;
+  const int W = a.g.W, H = a.g.H;
+  const R t{r0 - HALO};
+  const int t_end = a.c_hi + SPAN;
+  const int ngroups = (t_end - a.c_lo) / GS + 1;
+  auto group_barrier = []() { asm volatile("bar.sync 1, %0;" ::"n"(kSweepWarps * 32) : "memory"); };
+
+  if (warp == 0) {
+    const int r = r0 + lane;
+    const bool row_on = r <= a.r_hi;
+    __syncthreads();  // prologue staged
+    for (int g = 0; g < ngroups; g++) {
+      const int t0 = a.c_lo + g * GS;
+#pragma unroll 4
+      for (int s = 0; s < GS; s++) {
+        const int c = t0 + s - Op::SKEW * (lane / Op::PAIR);
+        if (row_on && c >= a.c_lo && c <= a.c_hi) Op::cell(t, r, c, a.g);
+        __syncwarp();
+      }
+      group_barrier();
+    }
+    return;
+  }
+
+  // ---- data movement
+  // Per-CTA plane pointers (with NCH = 2 the argument holds
   // {state ch0, state ch1, input ch0, input ch1}).
   const float* src[NP];
   float* dst[NS];
@@ -130,23 +175,49 @@ __global__ void __launch_bounds__(32) k_gs_sweep(SweepArgs a) {
   }
 #pragma unroll
   for (int p = 0; p < NS; p++) dst[p] = NCH == 1 ? a.plane[p] : (ch ? a.plane[1] : a.plane[0]);
-  const int r0 = a.r_lo + band * 32;
-  const int W = a.g.W, H = a.g.H;
-  const R t{r0 - HALO};
   const int st_r0 = max(r0 - HALO, 0), st_r1 = min(r0 + 31 + HALO, H - 1);
   const int out_r1 = min(r0 + 31, a.r_hi);
-  const int t_end = a.c_hi + SPAN;
   const int c_stop = a.c_hi + HALO + 1;  // staging never reaches past this column
-  int flushed = a.c_lo;
+  // Rows above r0 belong to the band above: its state planes are read by
+  // warp 1 only after that band has published the columns, with L2-coherent
+  // loads.  Everything else is band-local or read-only and goes through
+  // warps 2 and 3.
+  auto upper = [&](int p, int rr) { return band > 0 && p < NS && rr < r0; };
+  int staged = a.c_lo - HALO;
+
+  if (warp >= 2) {
+    const int sub = warp - 2;  // rows st_r0 + 2 * sub + lr, step 4
+    auto stage_local = [&](int hi) {
+      hi = min(hi, c_stop);
+      if (hi <= staged) return;
+#pragma unroll
+      for (int p = 0; p < NP; p++)
+        for (int c = staged + lc; c < hi; c += 16)
+          for (int rr = st_r0 + 2 * sub + lr; rr <= st_r1; rr += 4)
+            if (!upper(p, rr)) cp_async4(&t(p, rr, c), src[p] + (size_t)rr * W + c);
+      staged = hi;
+    };
+    stage_local(a.c_lo + kAhead * GS + HALO);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    for (int g = 0; g < ngroups; g++) {
+      const int t0 = a.c_lo + g * GS;
+      stage_local(t0 + (kAhead + 1) * GS + HALO);
+      cp_async_commit();
+      asm volatile("cp.async.wait_group 1;" ::: "memory");  // group g + 1 resident
+      group_barrier();
+    }
+    cp_async_wait_all();
+    return;
+  }
+
+  // ---- warp 1: band boundaries
+  int flushed = a.c_lo, published = a.c_lo;
   bool waiting = band > 0;
-
-  // Rows above r0 belong to the band above: its state planes are read only
-  // after that band has flushed the columns, and with L2-coherent loads.
-  auto upper = [&](int p, int r) { return band > 0 && p < NS && r < r0; };
-
-  // Progress of the band above as last observed by lane 0 (acquire loads;
-  // the warp barrier after the wait orders every lane's later loads).
   int above = 0;
+  // Progress of the band above as last observed by lane 0 (acquire loads;
+  // the shuffle after the wait orders every lane's later loads).
   auto wait_above = [&](int need) {
     if (!waiting) return;
     int ok = 1;
@@ -163,93 +234,67 @@ __global__ void __launch_bounds__(32) k_gs_sweep(SweepArgs a) {
     }
     if (!__shfl_sync(0xffffffffu, ok, 0)) waiting = false;
   };
-
-  // Flushing stores the final columns; publishing (a release by lane 0 after
-  // a warp barrier, so it covers every lane's stores) happens after the
-  // group's steps, by which time the stores have drained.
-  int published = a.c_lo;
+  // Upper-halo rows: at most one value per state plane per lane (GS = 16
+  // columns, HALO <= 2 rows, lane row st_r0 + lr).
+  float nh[NS];
+  int nh_c = 0;
+  bool nh_live = false;
+  auto stage_upper = [&](int hi, bool direct) {
+    hi = min(hi, c_stop);
+    if (hi <= staged) return;
+    if (band > 0) {
+      wait_above(min(hi, a.c_hi + 1));
+#pragma unroll
+      for (int p = 0; p < NS; p++)
+        for (int c = staged + lc; c < hi; c += 16)
+          for (int rr = st_r0 + lr; rr < r0; rr += 2) {
+            const float v = __ldcg(src[p] + (size_t)rr * W + c);
+            if (direct) t(p, rr, c) = v;
+            else nh[p] = v;
+          }
+      if (!direct) {
+        nh_c = staged + lc;
+        nh_live = nh_c < hi && st_r0 + lr < r0;
+      }
+    }
+    staged = hi;
+  };
+  auto land_upper = [&]() {
+    if (!nh_live) return;
+#pragma unroll
+    for (int p = 0; p < NS; p++) t(p, st_r0 + lr, nh_c) = nh[p];
+    nh_live = false;
+  };
   auto flush = [&](int hi) {
     if (hi <= flushed) return;
 #pragma unroll
     for (int p = 0; p < NS; p++)
       for (int c = flushed + lc; c < hi; c += 16)
-        for (int r = r0 + lr; r <= out_r1; r += 2) __stcg(dst[p] + (size_t)r * W + c, t(p, r, c));
+        for (int rr = r0 + lr; rr <= out_r1; rr += 2) __stcg(dst[p] + (size_t)rr * W + c, t(p, rr, c));
     flushed = hi;
   };
-  auto publish = [&]() {
-    if (flushed <= published) return;
+  // Release by lane 0 after a warp barrier, so it covers every lane's stores.
+  auto publish = [&](int upto) {
+    if (upto <= published) return;
     __syncwarp();
-    if (lane == 0) st_release(a.progress + ticket, flushed > a.c_hi ? INT_MAX : flushed);
-    published = flushed;
+    if (lane == 0) st_release(a.progress + ticket, upto > a.c_hi ? INT_MAX : upto);
+    published = upto;
   };
 
-  // Prologue: columns [c_lo - HALO, c_lo + GS + HALO), waited for and loaded.
-  int staged = min(a.c_lo + GS + HALO, c_stop);
-  wait_above(min(staged, a.c_hi + 1));
-#pragma unroll
-  for (int p = 0; p < NP; p++)
-    for (int c = a.c_lo - HALO + lc; c < staged; c += 16)
-      for (int r = st_r0 + lr; r <= st_r1; r += 2) {
-        const float* g = src[p] + (size_t)r * W + c;
-        if (upper(p, r))
-          t(p, r, c) = __ldcg(g);
-        else
-          cp_async4(&t(p, r, c), g);
-      }
-  cp_async_commit();
-
-  // Upper-halo values of the next group's columns, held in registers until
-  // the group starts (at most one per state plane per lane: GS columns x
-  // HALO rows spread over the 32 lanes).
-  float nh[NS];
-  int nh_lo = 0, nh_hi = 0;
-
-  for (int t0 = a.c_lo; t0 <= t_end; t0 += GS) {
+  stage_upper(a.c_lo + kAhead * GS + HALO, true);
+  __syncwarp();
+  __syncthreads();
+  for (int g = 0; g < ngroups; g++) {
+    const int t0 = a.c_lo + g * GS;
+    publish(flushed);
     flush(min(t0 - SPAN - Op::LAG, a.c_hi + 1));
-    if (nh_hi > nh_lo) {
-#pragma unroll
-      for (int p = 0; p < NS; p++) {
-        const int c = nh_lo + lc, r = st_r0 + lr;
-        if (c < nh_hi && upper(p, r)) t(p, r, c) = nh[p];
-      }
-    }
-    cp_async_wait_all();
+    land_upper();  // group g + kAhead - 1's upper rows
+    stage_upper(t0 + (kAhead + 1) * GS + HALO, false);
     __syncwarp();
-    const int lo = staged, hi = min(t0 + 2 * GS + HALO, c_stop);
-    nh_lo = nh_hi = 0;
-    if (hi > lo) {
-      wait_above(min(hi, a.c_hi + 1));
-#pragma unroll
-      for (int p = 0; p < NP; p++) {
-        const int c = lo + lc;
-        if (c >= hi) continue;
-        for (int r = st_r0 + lr; r <= st_r1; r += 2) {
-          const float* g = src[p] + (size_t)r * W + c;
-          if (upper(p, r)) {
-            if (p < NS) nh[p < NS ? p : 0] = __ldcg(g);
-          } else {
-            cp_async4(&t(p, r, c), g);
-          }
-        }
-      }
-      cp_async_commit();
-      nh_lo = lo;
-      nh_hi = hi;
-      staged = hi;
-    }
-    const int r = r0 + lane;
-    const bool row_on = r <= a.r_hi;
-#pragma unroll 4
-    for (int s = 0; s < GS; s++) {
-      const int c = t0 + s - Op::SKEW * (lane / Op::PAIR);
-      if (row_on && c >= a.c_lo && c <= a.c_hi) Op::cell(t, r, c, a.g);
-      __syncwarp();
-    }
-    publish();
+    group_barrier();
   }
-  cp_async_wait_all();
   flush(a.c_hi + 1);
-  publish();
+  publish(flushed);
 }
 
 template <class Op>
@@ -264,7 +309,7 @@ lre_status sweep(Context* c, const SweepArgs& base, int* sync, int nb_max, const
   LRE_CUDA_TRY(c, cudaMemsetAsync(sync, 0, sizeof(int), c->stream));
   LRE_CUDA_TRY(c, cudaMemsetAsync(a.progress, 0, (size_t)nb * sizeof(int), c->stream));
   LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_gs_sweep<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R::BYTES));
-  k_gs_sweep<Op><<<nb, 32, R::BYTES, c->stream>>>(a);
+  k_gs_sweep<Op><<<nb, kSweepWarps * 32, R::BYTES, c->stream>>>(a);
   count_launch(c);
   return check_launch(c, what);
 }
