@@ -235,6 +235,12 @@ typedef struct lre_develop_params {
   int output_bits; /* 32: float RGB out; 16: uint16 RGB out */
   int stage_order; /* 0: reference order (lateral, axial, defringe, tone);
                       1: demosaic, defringe, axial, tone */
+  int demosaic_algorithm; /* ProcessingParams::demosaic_algorithm routed as
+                             Accelerator::demosaic_compute does
+                             (core/accelerator.cpp:90-129): Bayer 0 bilinear,
+                             4 DCB (1 iteration, enhanced), 12 AAHD, anything
+                             else AMaZE; X-Trans 0 one-pass, else
+                             xtrans_passes.  Default 1. */
 } lre_develop_params;
 
 /* Fill `p` with the reference defaults (ProcessingParams()). */

@@ -64,6 +64,7 @@ class DevelopParams(C.Structure):
         ("tone_after_scale", C.c_float),
         ("output_bits", C.c_int),
         ("stage_order", C.c_int),
+        ("demosaic_algorithm", C.c_int),
     ]
 
 

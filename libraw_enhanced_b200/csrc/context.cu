@@ -131,6 +131,12 @@ lre_status lre_create(int device, lre_ctx** out) {
     delete c;
     return LRE_ERR_OUT_OF_MEMORY;
   }
+  if (lre::aahd_upload_gamma(c) != LRE_OK) {
+    cudaFree(c->d_scalars);
+    cudaStreamDestroy(c->own_stream);
+    delete c;
+    return LRE_ERR_CUDA;
+  }
   *out = reinterpret_cast<lre_ctx*>(c);
   return LRE_OK;
 }

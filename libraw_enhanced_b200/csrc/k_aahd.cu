@@ -355,11 +355,14 @@ __global__ void k_aahd_combine(Aahd A, float* __restrict__ rgb) {
 }
 
 // The reference's gamma table (:246-253), evaluated on the host with the
-// same expression and uploaded once per device.
+// same expression and uploaded once per device when a context is created
+// (outside any stream capture).
 std::mutex g_lut_mu;
 bool g_lut_done[64];
 
-lre_status upload_gamma(Context* c) {
+}  // namespace
+
+lre_status aahd_upload_gamma(Context* c) {
   std::lock_guard<std::mutex> lk(g_lut_mu);
   if (c->device >= 0 && c->device < 64 && g_lut_done[c->device]) return LRE_OK;
   static float lut[0x10000];
@@ -376,6 +379,8 @@ lre_status upload_gamma(Context* c) {
   return LRE_OK;
 }
 
+namespace {
+
 size_t padded_bytes(size_t w, size_t h) {
   return (((w + 2 * kMargin) * (h + 2 * kMargin) * sizeof(float)) + 255) & ~size_t(255);
 }
@@ -391,7 +396,6 @@ lre_status launch_aahd(Context* c, const float* raw, int raw_c_stride, float* rg
                        uint32_t filters, float maximum_value, int* d_err) {
   if (!bayer_2x2(filters))
     return fail(c, LRE_ERR_INVALID_ARGUMENT, "demosaic_bayer_aahd: needs a 2x2 Bayer layout (RGGB/BGGR/GRBG/GBRG)");
-  LRE_TRY(upload_gamma(c));
   const size_t pb = padded_bytes(w, h);
   Aahd A{};
   A.W = (int)w;

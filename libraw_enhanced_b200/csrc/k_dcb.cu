@@ -448,6 +448,8 @@ size_t plane_bytes(size_t w, size_t h) { return (w * h * sizeof(float) + 255) & 
 
 }  // namespace
 
+bool bayer_2x2_layout(uint32_t filters) { return bayer_2x2(filters); }
+
 size_t ws_bytes_dcb(size_t w, size_t h) {
   const size_t nb = 2 * ((h + 31) / 32 + 1);
   return 7 * plane_bytes(w, h) + ((w * h + 255) & ~size_t(255)) + (kSyncInts + nb) * sizeof(int) + 1024;

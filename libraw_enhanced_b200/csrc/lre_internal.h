@@ -193,6 +193,11 @@ size_t ws_bytes_dcb(size_t w, size_t h);
 lre_status launch_dcb(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
                       uint32_t filters, float maximum_value, int iterations, bool enhance, int* d_err);
 size_t ws_bytes_aahd(size_t w, size_t h);
+// Uploads AAHD's gamma table to the context's device (once per device).
+lre_status aahd_upload_gamma(Context* c);
+// True for filters words with a 2x2 Bayer layout (green checkerboard, R and
+// B on the other two sites), which DCB and AAHD need.
+bool bayer_2x2_layout(uint32_t filters);
 lre_status launch_aahd(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
                        uint32_t filters, float maximum_value, int* d_err);
 }  // namespace lre

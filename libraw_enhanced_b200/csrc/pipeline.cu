@@ -21,12 +21,30 @@ Context* C(lre_ctx* p) { return reinterpret_cast<Context*>(p); }
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
+// Demosaic routing (Accelerator::demosaic_compute, core/accelerator.cpp:90-129).
+enum class Demosaic { Amaze, Linear, Dcb, Aahd, Xtrans1, Xtrans3 };
+
+Demosaic route(const lre_develop_params& p) {
+  if (p.filters == LRE_FILTERS_XTRANS)
+    return (p.demosaic_algorithm == 0 || p.xtrans_passes == 1) ? Demosaic::Xtrans1 : Demosaic::Xtrans3;
+  switch (p.demosaic_algorithm) {
+    case 0: return Demosaic::Linear;
+    case 4: return Demosaic::Dcb;
+    case 12: return Demosaic::Aahd;
+    default: return Demosaic::Amaze;
+  }
+}
+
 size_t stage_ws(const lre_develop_params& p, size_t w, size_t h) {
   size_t m = 0;
-  if (p.filters == LRE_FILTERS_XTRANS)
-    m = std::max(m, lre::ws_bytes_xtrans(w, h, p.xtrans_passes));
-  else
-    m = std::max(m, lre::ws_bytes_amaze(w, h));
+  switch (route(p)) {
+    case Demosaic::Xtrans1: m = std::max(m, lre::ws_bytes_xtrans(w, h, 1)); break;
+    case Demosaic::Xtrans3: m = std::max(m, lre::ws_bytes_xtrans(w, h, 3)); break;
+    case Demosaic::Dcb: m = std::max(m, lre::ws_bytes_dcb(w, h)); break;
+    case Demosaic::Aahd: m = std::max(m, lre::ws_bytes_aahd(w, h)); break;
+    case Demosaic::Linear: break;
+    case Demosaic::Amaze: m = std::max(m, lre::ws_bytes_amaze(w, h)); break;
+  }
   if (p.lateral_ca_correction)
     m = std::max(m, lre::ws_bytes_lateral(w, h, p.lateral_ca_cell_size, p.lateral_ca_pyramid_levels, true));
   if (p.defringe) m = std::max(m, lre::ws_bytes_defringe(w, h, p.defringe_radius));
@@ -42,6 +60,9 @@ lre_status validate(Context* c, const lre_develop_params* p, size_t w, size_t h)
     return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: image too large");
   if (p->filters != LRE_FILTERS_XTRANS && p->filters < 1000)
     return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: filters is neither a Bayer word nor X-Trans");
+  if (p->filters != LRE_FILTERS_XTRANS && (p->demosaic_algorithm == 4 || p->demosaic_algorithm == 12) &&
+      !lre::bayer_2x2_layout(p->filters))
+    return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: DCB and AAHD need a 2x2 Bayer layout");
   if (p->output_bits != 32 && p->output_bits != 16)
     return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: output_bits must be 32 or 16");
   if (p->axial_ca_correction && p->axial_ca_radius > 16)
@@ -56,10 +77,30 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
   float* cur = rgb_a;
   float* other = rgb_b;
   const size_t mark = c->ws.used();
-  if (p.filters == LRE_FILTERS_XTRANS) {
-    LRE_TRY(lre::launch_xtrans(c, d_mosaic, 1, cur, w, h, p.xtrans, p.maximum_value, p.xtrans_passes == 1 ? 1 : 3));
-  } else {
-    LRE_TRY(lre::launch_amaze(c, d_mosaic, 1, cur, w, h, p.filters, p.cam_mul, p.maximum_value));
+  // The in-order sweeps of DCB/AAHD report a time-out through a device flag
+  // (d_scalars[63]); the host-buffer entry point reads it after its final
+  // synchronisation.
+  int* d_err = reinterpret_cast<int*>(c->d_scalars + 63);
+  switch (route(p)) {
+    case Demosaic::Xtrans1:
+    case Demosaic::Xtrans3:
+      LRE_TRY(lre::launch_xtrans(c, d_mosaic, 1, cur, w, h, p.xtrans, p.maximum_value,
+                                 route(p) == Demosaic::Xtrans1 ? 1 : 3));
+      break;
+    case Demosaic::Linear:
+      LRE_TRY(lre::launch_bayer_linear(c, d_mosaic, 1, cur, w, h, p.filters, p.maximum_value));
+      break;
+    case Demosaic::Dcb:
+      LRE_CUDA_TRY(c, cudaMemsetAsync(d_err, 0, sizeof(int), c->stream));
+      LRE_TRY(lre::launch_dcb(c, d_mosaic, 1, cur, w, h, p.filters, p.maximum_value, 1, true, d_err));
+      break;
+    case Demosaic::Aahd:
+      LRE_CUDA_TRY(c, cudaMemsetAsync(d_err, 0, sizeof(int), c->stream));
+      LRE_TRY(lre::launch_aahd(c, d_mosaic, 1, cur, w, h, p.filters, p.maximum_value, d_err));
+      break;
+    case Demosaic::Amaze:
+      LRE_TRY(lre::launch_amaze(c, d_mosaic, 1, cur, w, h, p.filters, p.cam_mul, p.maximum_value));
+      break;
   }
   c->ws.rewind(mark);
   auto tone = [&]() -> lre_status {
@@ -173,6 +214,7 @@ void lre_develop_params_default(lre_develop_params* p) {
   p->tone_after_scale = 1.0f;
   p->output_bits = 32;
   p->stage_order = 0;
+  p->demosaic_algorithm = 1;
 }
 
 lre_status lre_dev_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t w, size_t h,
@@ -215,6 +257,12 @@ lre_status lre_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t w, s
     LRE_CUDA_TRY(c, cudaMemcpyAsync(out, res, out_bytes, cudaMemcpyDeviceToHost, c->stream));
   }
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  const Demosaic d = route(p);
+  if (d == Demosaic::Dcb || d == Demosaic::Aahd) {
+    int err = 0;
+    LRE_CUDA_TRY(c, cudaMemcpy(&err, c->d_scalars + 63, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return lre::fail(c, LRE_ERR_TIMEOUT, "develop: a demosaic sweep band timed out");
+  }
   return LRE_OK;
 }
 
