@@ -423,6 +423,8 @@ def run_ours(args):
         }
         if world == 1 and not args.no_xtrans:
             line["xtrans"] = run_xtrans(args, acc, stream)
+        if world == 1 and not args.no_demosaics:
+            line["demosaics"] = run_demosaics(args, acc, stream, d_mos, W, H)
         if world == 1 and not args.no_batch:
             line["batched"] = run_batched(args, acc)
         if world == 1 and not args.no_serve:
@@ -592,6 +594,46 @@ def run_xtrans(args, acc, stream):
     }
 
 
+def run_demosaics(args, acc, stream, d_mos, W, H):
+    """The four Bayer demosaics the reference routes (bilinear, AMaZE, DCB,
+    AAHD) alone on the 51 MP mosaic, scaled to a 14-bit raw range (AAHD
+    indexes a 64 Ki gamma table with the sample); device-resident, CUDA
+    events on the library's stream."""
+    import torch
+
+    from libraw_enhanced_b200 import scenes
+
+    mos = (d_mos * 16383.0).contiguous()
+    out = torch.empty((H, W, 3), dtype=torch.float32, device=mos.device)
+    f = scenes.FILTERS["RGGB"]
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    reps = max(3, min(args.steps, 5))
+    legs = {
+        "linear": lambda: acc.dev_demosaic_bayer_linear(mos, out, W, H, f, 16383.0),
+        "amaze": lambda: acc.dev_demosaic_bayer_amaze(mos, out, W, H, f, WB, 16383.0),
+        "dcb": lambda: acc.dev_demosaic_bayer_dcb(mos, out, W, H, f, 16383.0, 1, True),
+        "aahd": lambda: acc.dev_demosaic_bayer_aahd(mos, out, W, H, f, 16383.0),
+    }
+    res = {}
+    for k, fn in legs.items():
+        ms = timed(fn, reps)
+        res[k] = {"ms": round(ms, 3), "mp_s": round(H * W / 1e6 / (ms / 1e3), 1)}
+    res["workload"] = f"{W}x{H} RGGB mosaic, 14-bit range, f32 RGB out; DCB 1 iteration + enhance"
+    return res
+
+
 def run_served(args):
     """Poisson arrivals of develop requests through lre_server_*: 60% 6000x4000
     Bayer, 25% 8256x5504 Bayer, 15% 6240x4160 X-Trans; defringe p=.5, axial
@@ -726,6 +768,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the 32-image batched develop")
     ap.add_argument("--no-serve", action="store_true", help="skip the request-server sweep")
     ap.add_argument("--no-xtrans", action="store_true", help="skip the X-Trans + lateral CA workload")
+    ap.add_argument("--no-demosaics", action="store_true", help="skip the per-algorithm Bayer demosaic timings")
     ap.add_argument("--xtrans-size", default="6240x4160", help="WxH of the X-Trans workload (reduced cases: profiling)")
     ap.add_argument("--size", default=None, help="WxH of a reduced case (profiling); default 8736x5856")
     args = ap.parse_args()

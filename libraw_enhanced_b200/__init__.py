@@ -318,6 +318,10 @@ class CudaAccelerator:
         cm = np.asarray(cam_mul, dtype=np.float32)
         self._check(self._lib.lre_dev_demosaic_bayer_amaze(self._h, _dptr(raw), _dptr(rgb), int(width), int(height), int(filters), _ptr(cm), float(maximum_value)))
 
+    def dev_demosaic_bayer_linear(self, raw, rgb, width, height, filters, maximum_value=1.0):
+        self._check(self._lib.lre_dev_demosaic_bayer_linear(self._h, _dptr(raw), _dptr(rgb), int(width), int(height),
+                                                            int(filters), float(maximum_value)))
+
     def dev_demosaic_bayer_dcb(self, raw, rgb, width, height, filters, maximum_value=1.0, iterations=1,
                                dcb_enhance=True):
         self._check(self._lib.lre_dev_demosaic_bayer_dcb(self._h, _dptr(raw), _dptr(rgb), int(width), int(height),

@@ -77,6 +77,19 @@ class CudaAccelerator {
     if (!same(raw, rgb)) return bad("demosaic_bayer_linear: buffer size mismatch");
     return ok(lre_demosaic_bayer_linear(ctx_, f(raw), f(rgb), raw.width, raw.height, filters, maximum_value));
   }
+  // Accelerator::demosaic_bayer_dcb / demosaic_bayer_aahd (core/accelerator.h:269-277); the
+  // reference's GPU path has neither and falls back to the CPU (core/accelerator.cpp:159-199).
+  bool demosaic_bayer_dcb(const ImageBufferFloat& raw, ImageBufferFloat& rgb, uint32_t filters,
+                          float maximum_value, int iterations = 1, bool dcb_enhance = true) {
+    if (!same(raw, rgb)) return bad("demosaic_bayer_dcb: buffer size mismatch");
+    return ok(lre_demosaic_bayer_dcb(ctx_, f(raw), f(rgb), raw.width, raw.height, filters, maximum_value,
+                                     iterations, dcb_enhance ? 1 : 0));
+  }
+  bool demosaic_bayer_aahd(const ImageBufferFloat& raw, ImageBufferFloat& rgb, uint32_t filters,
+                           float maximum_value) {
+    if (!same(raw, rgb)) return bad("demosaic_bayer_aahd: buffer size mismatch");
+    return ok(lre_demosaic_bayer_aahd(ctx_, f(raw), f(rgb), raw.width, raw.height, filters, maximum_value));
+  }
   bool demosaic_bayer_amaze(const ImageBufferFloat& raw, ImageBufferFloat& rgb, uint32_t filters,
                             const float (&cam_mul)[4], float maximum_value) {
     if (!same(raw, rgb)) return bad("demosaic_bayer_amaze: mismatched buffers");
