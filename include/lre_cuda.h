@@ -241,6 +241,11 @@ typedef struct lre_develop_params {
                              4 DCB (1 iteration, enhanced), 12 AAHD, anything
                              else AMaZE; X-Trans 0 one-pass, else
                              xtrans_passes.  Default 1. */
+  int highlight_recovery;    /* recover_highlights right after the demosaic, as
+                                the pipeline runs it for highlight_mode > 2
+                                (core/libraw_wrapper.cpp:1677-1683); default 0 */
+  float highlight_threshold; /* its saturation threshold (the pipeline passes
+                                maximum / data_maximum); default 1 */
 } lre_develop_params;
 
 /* Fill `p` with the reference defaults (ProcessingParams()). */
@@ -295,6 +300,25 @@ lre_status lre_demosaic_bayer_aahd(lre_ctx* ctx, const float* raw_rgb, float* rg
 /* Same on a dense device mosaic; returns after the stream has drained. */
 lre_status lre_dev_demosaic_bayer_aahd(lre_ctx* ctx, const float* raw, float* rgb, size_t width,
                                        size_t height, uint32_t filters, float maximum_value);
+
+/* ------------------------------------------------ highlight recovery */
+/* The develop pipeline's recover_highlights (core/libraw_wrapper.cpp:
+ * 1095-1383, run for highlight_mode > 2 at :1677-1683; standalone as
+ * LibRawWrapper::recover_highlights_numpy, :3066-3096): highlight R/G and
+ * B/G ratios, G rebuilt in highlights, white pixels blended with their 8
+ * neighbours, then the in-order LoCA green lift.  `rgb_in` and `rgb_out` are
+ * (H,W,3) float and may be the same buffer.  `mask_out` (W*H floats) receives
+ * the soft highlight mask when non-null; `wb_rgb` (3 floats) selects the
+ * WB-undone chroma edges as the reference does; `max_val_out` (nullable)
+ * receives the highlight maximum.  Bit-exact with the reference. */
+lre_status lre_recover_highlights(lre_ctx* ctx, const float* rgb_in, float* rgb_out, size_t width,
+                                  size_t height, float saturation_threshold, float* mask_out,
+                                  const float* wb_rgb, float* max_val_out);
+/* Same on device buffers (mask_out and max_val_out device pointers, wb_rgb
+ * host); returns after the stream has drained. */
+lre_status lre_dev_recover_highlights(lre_ctx* ctx, const float* rgb_in, float* rgb_out, size_t width,
+                                      size_t height, float saturation_threshold, float* mask_out,
+                                      const float* wb_rgb, float* max_val_out);
 
 /* ------------------------------------------------------ output end */
 /* GPUAccelerator::convert_color_space (core/gpu_accelerator.h:66-69;

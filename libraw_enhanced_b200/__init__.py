@@ -191,6 +191,21 @@ class CudaAccelerator:
                                                       int(filters), float(maximum_value)))
         return out
 
+    def recover_highlights(self, rgb, saturation_threshold: float, want_mask: bool = False, wb_rgb=None):
+        """The pipeline's highlight recovery (core/libraw_wrapper.cpp:1095-1383).
+
+        Returns (recovered copy, mask or None, highlight max)."""
+        img = _rgb(rgb, "recover_highlights")
+        out = np.empty_like(img)
+        h, w = img.shape[:2]
+        mask = np.empty((h, w), np.float32) if want_mask else None
+        wb = None if wb_rgb is None else np.ascontiguousarray(wb_rgb, dtype=np.float32)
+        mx = C.c_float(0.0)
+        self._check(self._lib.lre_recover_highlights(self._h, _ptr(img), _ptr(out), w, h, float(saturation_threshold),
+                                                     None if mask is None else _ptr(mask),
+                                                     None if wb is None else _ptr(wb), C.byref(mx)))
+        return out, mask, mx.value
+
     def demosaic_xtrans_1pass(self, raw_rgb, xtrans, color_matrix=None, maximum_value: float = 1.0):
         return self._xtrans(raw_rgb, xtrans, color_matrix, maximum_value, 1)
 
@@ -327,6 +342,15 @@ class CudaAccelerator:
         self._check(self._lib.lre_dev_demosaic_bayer_dcb(self._h, _dptr(raw), _dptr(rgb), int(width), int(height),
                                                          int(filters), float(maximum_value), int(iterations),
                                                          int(bool(dcb_enhance))))
+
+    def dev_recover_highlights(self, inp, out, width, height, saturation_threshold, mask=None, wb_rgb=None,
+                               max_val=None):
+        wb = None if wb_rgb is None else np.ascontiguousarray(wb_rgb, dtype=np.float32)
+        self._check(self._lib.lre_dev_recover_highlights(self._h, _dptr(inp), _dptr(out), int(width), int(height),
+                                                         float(saturation_threshold),
+                                                         None if mask is None else _dptr(mask),
+                                                         None if wb is None else _ptr(wb),
+                                                         None if max_val is None else _dptr(max_val)))
 
     def dev_demosaic_bayer_aahd(self, raw, rgb, width, height, filters, maximum_value=1.0):
         self._check(self._lib.lre_dev_demosaic_bayer_aahd(self._h, _dptr(raw), _dptr(rgb), int(width), int(height),

@@ -65,6 +65,8 @@ class DevelopParams(C.Structure):
         ("output_bits", C.c_int),
         ("stage_order", C.c_int),
         ("demosaic_algorithm", C.c_int),
+        ("highlight_recovery", C.c_int),
+        ("highlight_threshold", C.c_float),
     ]
 
 
@@ -188,6 +190,8 @@ SIGNATURES = {
     "lre_demosaic_bayer_dcb": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _f, C.c_int, C.c_int]),
     "lre_dev_demosaic_bayer_dcb": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _f, C.c_int, C.c_int]),
     "lre_demosaic_bayer_aahd": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _f]),
+    "lre_recover_highlights": (_st, [_p, _p, _p, _sz, _sz, _f, _p, _p, _p]),
+    "lre_dev_recover_highlights": (_st, [_p, _p, _p, _sz, _sz, _f, _p, _p, _p]),
     "lre_dev_demosaic_bayer_aahd": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _f]),
     "lre_convert_color_space": (_st, [_p, _p, _p, _sz, _sz, _p]),
     "lre_gamma_correct": (_st, [_p, _p, _p, _sz, _sz, _f, _f, _i]),

@@ -252,6 +252,40 @@ lre_status lre_demosaic_bayer_dcb(lre_ctx* ctx, const float* raw_rgb, float* rgb
   return LRE_OK;
 }
 
+lre_status lre_dev_recover_highlights(lre_ctx* ctx, const float* in, float* out, size_t w, size_t h, float thr,
+                                      float* mask_out, const float* wb_rgb, float* max_val_out) {
+  Context* c = C(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  LRE_TRY(check_img(c, in, out, w, h, "recover_highlights"));
+  LRE_TRY(begin(c, lre::ws_bytes_highlights(w, h)));
+  return lre::launch_recover_highlights(c, in, out, w, h, thr, mask_out, wb_rgb, max_val_out, nullptr);
+}
+
+lre_status lre_recover_highlights(lre_ctx* ctx, const float* in, float* out, size_t w, size_t h, float thr,
+                                  float* mask_out, const float* wb_rgb, float* max_val_out) {
+  Context* c = C(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  LRE_TRY(check_img(c, in, out, w, h, "recover_highlights"));
+  std::lock_guard<std::mutex> lk(c->mu);
+  LRE_TRY(begin(c, lre::ws_bytes_highlights(w, h)));
+  const size_t bytes = w * h * 3 * sizeof(float);
+  const size_t mbytes = w * h * sizeof(float);
+  LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, bytes));
+  LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, bytes));
+  if (mask_out) LRE_TRY(lre::ensure_buffer(c, &c->d_aux, &c->d_aux_cap, mbytes));
+  float* din = reinterpret_cast<float*>(c->d_in);
+  float* dout = reinterpret_cast<float*>(c->d_out);
+  float* dmask = mask_out ? reinterpret_cast<float*>(c->d_aux) : nullptr;
+  float* dmax = c->d_scalars + 40;
+  LRE_CUDA_TRY(c, cudaMemcpyAsync(din, in, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::launch_recover_highlights(c, din, dout, w, h, thr, dmask, wb_rgb, dmax, nullptr));
+  LRE_CUDA_TRY(c, cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+  if (mask_out) LRE_CUDA_TRY(c, cudaMemcpyAsync(mask_out, dmask, mbytes, cudaMemcpyDeviceToHost, c->stream));
+  if (max_val_out) LRE_CUDA_TRY(c, cudaMemcpyAsync(max_val_out, dmax, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return LRE_OK;
+}
+
 lre_status lre_dev_demosaic_bayer_aahd(lre_ctx* ctx, const float* raw, float* rgb, size_t w, size_t h,
                                        uint32_t filters, float maximum_value) {
   Context* c = C(ctx);

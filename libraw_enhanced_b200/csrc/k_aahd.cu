@@ -163,7 +163,7 @@ __global__ void k_aahd_hot_pretest(Aahd A) {
 // and r + 1 advance together, each row pair three columns behind the pair
 // above: (r - 2, c + 2) is then already rewritten and (r + 2, c - 2) not yet.
 struct OpHideHots {
-  static constexpr int NS = 1, NP = 1, HALO = 2, SKEW = 3, PAIR = 2, NCH = 1, LAG = 0;
+  static constexpr int NS = 1, NP = 1, HALO = 2, SKEW = 3, PAIR = 2, NCH = 1, LAG = 0, RING = kRing;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo& g) {
     // padded coordinates; the 2x2 pattern makes the 4-px offset invisible
@@ -321,7 +321,7 @@ __global__ void k_aahd_evaluate(Aahd A) {
 // image so the last odd column is reached.  Every neighbour read precedes or
 // follows the site exactly as in the row-major loops with skew 1.
 struct OpRefineDirs {
-  static constexpr int NS = 1, NP = 1, HALO = 1, SKEW = 1, PAIR = 1, NCH = 1, LAG = 1;
+  static constexpr int NS = 1, NP = 1, HALO = 1, SKEW = 1, PAIR = 1, NCH = 1, LAG = 1, RING = kRing;
   template <class T>
   __device__ static void upd(const T& t, int r, int c) {
     const int n = (int)t(0, r - 1, c), s = (int)t(0, r + 1, c), w = (int)t(0, r, c - 1), e = (int)t(0, r, c + 1);

@@ -392,7 +392,7 @@ __global__ void k_dcb_pp_terms(const float* __restrict__ G, float* __restrict__ 
 // R and B do not change across the nyquist passes).  A site reads rows r +- 2
 // only, so rows r and r + 1 advance together.
 struct OpNyquist {
-  static constexpr int NS = 1, NP = 3, HALO = 2, SKEW = 1, PAIR = 2, NCH = 1, LAG = 0;
+  static constexpr int NS = 1, NP = 3, HALO = 2, SKEW = 1, PAIR = 2, NCH = 1, LAG = 0, RING = kRing;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo& g) {
     if (g.fc(r, c) == 1) return;
@@ -405,7 +405,7 @@ struct OpNyquist {
 // dcb_pp (:820-834), one channel (R or B) per warp: state the channel;
 // input K = G - mean8(G) (k_dcb_pp_terms; green does not change in the pass).
 struct OpPP {
-  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 2, LAG = 0;
+  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 2, LAG = 0, RING = kRing;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo& g) {
     const float x1 = (t(0, r, c - 1) + t(0, r, c + 1) + t(0, r - 1, c) + t(0, r + 1, c) + t(0, r - 1, c - 1) +
@@ -426,7 +426,7 @@ __device__ __forceinline__ void clamp8(const T& t, int p, int r, int c, float v)
 
 // dcb_refinement's closing clamp (:992-994): state G; input the pre-clamp value.
 struct OpRefine {
-  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 1, LAG = 0;
+  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 1, LAG = 0, RING = kRing;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo& g) {
     if (g.fc(r, c) == 1) return;
@@ -437,7 +437,7 @@ struct OpRefine {
 // dcb_color_full's last loop (:898-913), one channel per warp: state R or B;
 // input that channel's CLIP(chroma + G).
 struct OpColorFull {
-  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 2, LAG = 0;
+  static constexpr int NS = 1, NP = 2, HALO = 1, SKEW = 2, PAIR = 1, NCH = 2, LAG = 0, RING = kRing;
   template <class T>
   __device__ static void cell(const T& t, int r, int c, const Geo&) {
     clamp8(t, 0, r, c, t(1, r, c));

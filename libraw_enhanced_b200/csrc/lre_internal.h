@@ -193,6 +193,13 @@ size_t ws_bytes_dcb(size_t w, size_t h);
 lre_status launch_dcb(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
                       uint32_t filters, float maximum_value, int iterations, bool enhance, int* d_err);
 size_t ws_bytes_aahd(size_t w, size_t h);
+// Highlight recovery (k_highlights.cu).  in may equal out; mask_out (W*H
+// floats, device) and d_max_val_out (device) may be null; wb_rgb is host.
+// d_err follows the DCB/AAHD convention above.
+size_t ws_bytes_highlights(size_t w, size_t h);
+lre_status launch_recover_highlights(Context* c, const float* in, float* out, size_t w, size_t h,
+                                     float saturation_threshold, float* mask_out, const float* wb_rgb,
+                                     float* d_max_val_out, int* d_err);
 // Uploads AAHD's gamma table to the context's device (once per device).
 lre_status aahd_upload_gamma(Context* c);
 // True for filters words with a 2x2 Bayer layout (green checkerboard, R and

@@ -45,6 +45,7 @@ size_t stage_ws(const lre_develop_params& p, size_t w, size_t h) {
     case Demosaic::Linear: break;
     case Demosaic::Amaze: m = std::max(m, lre::ws_bytes_amaze(w, h)); break;
   }
+  if (p.highlight_recovery) m = std::max(m, lre::ws_bytes_highlights(w, h));
   if (p.lateral_ca_correction)
     m = std::max(m, lre::ws_bytes_lateral(w, h, p.lateral_ca_cell_size, p.lateral_ca_pyramid_levels, true));
   if (p.defringe) m = std::max(m, lre::ws_bytes_defringe(w, h, p.defringe_radius));
@@ -77,9 +78,9 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
   float* cur = rgb_a;
   float* other = rgb_b;
   const size_t mark = c->ws.used();
-  // The in-order sweeps of DCB/AAHD report a time-out through a device flag
-  // (d_scalars[63]); the host-buffer entry point reads it after its final
-  // synchronisation.
+  // The in-order sweeps of DCB/AAHD and highlight recovery report a time-out
+  // through a device flag (d_scalars[63]); the host-buffer entry point reads
+  // it after its final synchronisation.
   int* d_err = reinterpret_cast<int*>(c->d_scalars + 63);
   switch (route(p)) {
     case Demosaic::Xtrans1:
@@ -101,6 +102,12 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
     case Demosaic::Amaze:
       LRE_TRY(lre::launch_amaze(c, d_mosaic, 1, cur, w, h, p.filters, p.cam_mul, p.maximum_value));
       break;
+  }
+  c->ws.rewind(mark);
+  if (p.highlight_recovery) {
+    if (route(p) != Demosaic::Dcb && route(p) != Demosaic::Aahd)
+      LRE_CUDA_TRY(c, cudaMemsetAsync(d_err, 0, sizeof(int), c->stream));
+    LRE_TRY(lre::launch_recover_highlights(c, cur, cur, w, h, p.highlight_threshold, nullptr, nullptr, nullptr, d_err));
   }
   c->ws.rewind(mark);
   auto tone = [&]() -> lre_status {
@@ -215,6 +222,8 @@ void lre_develop_params_default(lre_develop_params* p) {
   p->output_bits = 32;
   p->stage_order = 0;
   p->demosaic_algorithm = 1;
+  p->highlight_recovery = 0;
+  p->highlight_threshold = 1.0f;
 }
 
 lre_status lre_dev_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t w, size_t h,
@@ -258,7 +267,7 @@ lre_status lre_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t w, s
   }
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   const Demosaic d = route(p);
-  if (d == Demosaic::Dcb || d == Demosaic::Aahd) {
+  if (d == Demosaic::Dcb || d == Demosaic::Aahd || p.highlight_recovery) {
     int err = 0;
     LRE_CUDA_TRY(c, cudaMemcpy(&err, c->d_scalars + 63, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) return lre::fail(c, LRE_ERR_TIMEOUT, "develop: a demosaic sweep band timed out");

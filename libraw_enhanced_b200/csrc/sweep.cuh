@@ -21,8 +21,9 @@
 //     stops waiting, and the host reports the failure.
 // An op supplies NS state planes + inputs (NP planes per warp), HALO, SKEW,
 // PAIR, NCH (independent channels run as separate warps), LAG (how many
-// columns behind its walk position a cell may still write) and a cell(t, r,
-// c, g) that updates the site (r, c) through the ring accessor t.
+// columns behind its walk position a cell may still write), RING (ring
+// columns, a power of two) and a cell(t, r, c, g) that updates the site
+// (r, c) through the ring accessor t.
 #pragma once
 
 #include <climits>
@@ -34,12 +35,13 @@
 namespace lre {
 namespace {
 
-constexpr int kRing = 128;  // shared-memory ring width in columns (power of two)
+constexpr int kRing = 128;  // default shared-memory ring width in columns (power of two)
 
 struct Geo {
   int W, H;
   uint32_t filters;
   float maxv;
+  const float* aux;  // optional device scalars an op reads (nullptr when unused)
   __device__ __forceinline__ unsigned fc(int r, int c) const { return fcol3((unsigned)r, (unsigned)c, filters); }
   __device__ __forceinline__ size_t at(int r, int c) const { return (size_t)r * W + c; }
 };
@@ -63,15 +65,15 @@ struct SweepArgs {
 // itself so every access compiles to a shared-memory instruction.
 extern __shared__ float sweep_smem[];
 
-template <int NP, int HALO, int PAD>
+template <int NP, int HALO, int PAD, int RING>
 struct Ring {
   static constexpr int ROWS = 32 + 2 * HALO;
-  static constexpr int PITCH = kRing + PAD;
+  static constexpr int PITCH = RING + PAD;
   static constexpr int PLANE = ROWS * PITCH;
   static constexpr size_t BYTES = (size_t)NP * PLANE * sizeof(float);
   int rbase;
   __device__ __forceinline__ float& operator()(int p, int r, int c) const {
-    return sweep_smem[p * PLANE + (r - rbase) * PITCH + (c & (kRing - 1))];
+    return sweep_smem[p * PLANE + (r - rbase) * PITCH + (c & (RING - 1))];
   }
 };
 
@@ -81,7 +83,7 @@ struct Ring {
 // pitch of 16 (mod 32) gives bank (32 - SKEW) * (l / 2) + 16 * (l & 1) +
 // const, 32 distinct banks.
 template <class Op>
-using RingOf = Ring<Op::NP, Op::HALO, (Op::PAIR == 2 ? 16 : Op::SKEW + 1)>;
+using RingOf = Ring<Op::NP, Op::HALO, (Op::PAIR == 2 ? 16 : Op::SKEW + 1), Op::RING>;
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -129,7 +131,7 @@ __global__ void __launch_bounds__(kSweepWarps * 32) k_gs_sweep(SweepArgs a) {
   using R = RingOf<Op>;
   constexpr int HALO = Op::HALO, NS = Op::NS, NP = Op::NP, NCH = Op::NCH, GS = kGroup;
   constexpr int SPAN = Op::SKEW * (31 / Op::PAIR);  // column lag of lane 31 behind lane 0
-  static_assert((kAhead + 1) * GS + SPAN + 2 * HALO + Op::LAG <= kRing, "sweep ring too small for this op");
+  static_assert((kAhead + 1) * GS + SPAN + 2 * HALO + Op::LAG <= Op::RING, "sweep ring too small for this op");
   if (a.skip_if_zero && *a.skip_if_zero == 0) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, lc = lane & 15, lr = lane >> 4;
   __shared__ int s_ticket;

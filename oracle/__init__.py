@@ -169,6 +169,27 @@ def bayer_dcb(raw_sparse, filters, maximum=1.0, iterations=1, enhance=True, thre
     return out
 
 
+REF_HL_SO = os.path.join(HERE, "_ref", "liblre_ref_hl.so")
+_ref_hl = None
+
+
+def recover_highlights(rgb, saturation_threshold, want_mask=False, wb_rgb=None):
+    """The reference's highlight recovery (core/libraw_wrapper.cpp:1095-1383),
+    compiled from those lines alone.  Returns (recovered copy, mask or None)."""
+    global _ref_hl
+    if _ref_hl is None:
+        _ref_hl = C.CDLL(REF_HL_SO)
+        _ref_hl.ref_recover_highlights.restype = C.c_int
+        _ref_hl.ref_recover_highlights.argtypes = [_p, _sz, _sz, _f, _p, _p]
+    img = np.ascontiguousarray(rgb, dtype=np.float32).copy()
+    h, w, _ = img.shape
+    mask = np.zeros((h, w), np.float32) if want_mask else None
+    wb = None if wb_rgb is None else np.asarray(wb_rgb, np.float32)
+    _ref_hl.ref_recover_highlights(_ptr(img), w, h, float(saturation_threshold),
+                                   None if mask is None else _ptr(mask), None if wb is None else _ptr(wb))
+    return img, mask
+
+
 def bayer_aahd(raw_sparse, filters, maximum=1.0, threads=1):
     """The reference's AAHD demosaic (core/cpu_accelerator.cpp:617-633), by
     default single-threaded: its in-place row loops and channel min/max scan

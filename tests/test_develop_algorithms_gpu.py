@@ -91,3 +91,20 @@ def test_develop_dcb_aahd_need_2x2_bayer(lre, acc):
         with pytest.raises(lre.LibRawError) as ei:
             acc.develop(mos, p)
         assert ei.value.status == 1
+
+
+@pytest.mark.parametrize("algo", [10, 4])
+def test_develop_highlight_recovery_matches_standalone(lre, acc, algo):
+    # recover_highlights right after the demosaic, as the pipeline runs it
+    h, w = 150, 210
+    mos = scenes.bayer_scene(h, w, 64, cfa="RGGB")
+    p = lre.develop_params(cfa="RGGB", cam_mul=(2.0, 1.0, 1.5, 1.0), demosaic_algorithm=algo,
+                           highlight_recovery=1, highlight_threshold=0.9)
+    got = acc.develop(mos, p)
+    sp = scenes.sparse_rgb(mos, "RGGB")
+    f = scenes.FILTERS["RGGB"]
+    dem = (acc.demosaic_bayer_dcb(sp, f, 1.0) if algo == 4
+           else acc.demosaic_bayer_amaze(sp, f, (2.0, 1.0, 1.5, 1.0), 1.0))
+    ref, _, _ = acc.recover_highlights(dem, 0.9)
+    assert not np.array_equal(ref, dem)
+    assert np.array_equal(got, ref)
