@@ -63,6 +63,12 @@ struct Aahd {
   int* hot;        // count of sites hot against the original samples
   __device__ __forceinline__ unsigned fc(int i, int j) const { return fcol3((unsigned)i, (unsigned)j, filters); }
   __device__ __forceinline__ size_t pi(int i, int j) const { return (size_t)(i + kMargin) * NW + (j + kMargin); }
+  // Plane of direction d, channel c, selected without indexing the
+  // parameter array at run time (which would copy it to local memory).
+  __device__ __forceinline__ float* pl(int d, int c) const {
+    float* const* row = d ? P[1] : P[0];
+    return c == 0 ? row[0] : (c == 1 ? row[1] : row[2]);
+  }
 };
 
 #define AAHD_FOR_PIXELS(A)                                                                    \
@@ -109,8 +115,8 @@ __global__ void k_aahd_init(const float* __restrict__ raw, int cs, Aahd A) {
     if (d != 0) {
       const size_t p = A.pi(i, j);
       A.X[p] = d;
-      A.P[0][c][p] = d;
-      A.P[1][c][p] = d;
+      A.pl(0, c)[p] = d;
+      A.pl(1, c)[p] = d;
       atomic_max_f(&A.stats[c], d);
       atomic_min_f(&A.stats[3 + c], d);
     }
@@ -181,8 +187,8 @@ __global__ void k_aahd_greens(Aahd A) {
     const size_t p = A.pi(i, j);
     const float k0 = A.X[p];
     if (kc == 1) continue;
-    A.P[0][kc][p] = k0;
-    A.P[1][kc][p] = k0;
+    A.pl(0, kc)[p] = k0;
+    A.pl(1, kc)[p] = k0;
     const float gmax = A.stats[1], gmin = A.stats[4];
 #pragma unroll
     for (int d = 0; d < 2; d++) {
@@ -203,7 +209,7 @@ __global__ void k_aahd_greens(Aahd A) {
         eg = (int)gmax;
       else if ((float)eg < gmin)
         eg = (int)gmin;
-      A.P[d][1][p] = (float)eg;
+      A.pl(d, 1)[p] = (float)eg;
     }
   }
 }
@@ -226,10 +232,10 @@ __global__ void k_aahd_rb_hv(Aahd A) {
     for (int d = 0; d < 2; d++) {
       const ptrdiff_t dir = d ? (ptrdiff_t)A.NW : 1;
       const int c = kc ^ (d << 1);
-      const float* G = A.P[d][1];
-      const float* Cc = A.P[d][c];
+      const float* G = A.pl(d, 1);
+      const float* Cc = A.pl(d, c);
       int eg = (int)(G[p] + (Cc[p - dir] - G[p - dir] + Cc[p + dir] - G[p + dir]) / 2);
-      A.P[d][c][p] = (float)clamp_channel(eg, A.stats, c);
+      A.pl(d, c)[p] = (float)clamp_channel(eg, A.stats, c);
     }
   }
 }
@@ -247,8 +253,8 @@ __global__ void k_aahd_rb_last(Aahd A) {
       int c = kc ^ 2;
       if ((j & 1) != js) c ^= d << 1;
       const ptrdiff_t dirs[3] = {-1 - nw, d ? (ptrdiff_t)-1 : -nw, d ? nw - 1 : 1 - nw};
-      const float* G = A.P[d][1];
-      float* Cc = A.P[d][c];
+      const float* G = A.pl(d, 1);
+      float* Cc = A.pl(d, c);
       const float g0 = G[p];
       int bh = 0, bk = 0, bgd = 0;
       for (int k = 0; k < 3; ++k)
@@ -262,7 +268,8 @@ __global__ void k_aahd_rb_last(Aahd A) {
             bk = k;
           }
         }
-      const size_t a = p + dirs[bk], b = p - dirs[bh];
+      auto dir = [&](int k) { return k == 0 ? dirs[0] : (k == 1 ? dirs[1] : dirs[2]); };
+      const size_t a = p + dir(bk), b = p - dir(bh);
       const int eg = (int)(g0 + (Cc[a] - G[a] + Cc[b] - G[b]) / 2);
       Cc[p] = (float)clamp_channel(eg, A.stats, c);
     }
@@ -273,7 +280,7 @@ __device__ __forceinline__ void yuv_of(const Aahd& A, int d, size_t q, int* y) {
   float l[3];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    const float v = A.P[d][c][q];
+    const float v = A.pl(d, c)[q];
     const unsigned idx = v <= 0.0f ? 0u : (v >= 65535.0f ? 65535u : (unsigned)v);
     l[c] = g_aahd_gamma[idx];
   }
@@ -348,9 +355,9 @@ __global__ void k_aahd_combine(Aahd A, float* __restrict__ rgb) {
     const size_t p = A.pi(i, j);
     const int d = ((int)A.ND[p] & kVer) ? 1 : 0;
     float* o = rgb + ((size_t)i * A.W + j) * 3;
-    o[0] = A.P[d][0][p] / A.maxv;
-    o[1] = A.P[d][1][p] / A.maxv;
-    o[2] = A.P[d][2][p] / A.maxv;
+    o[0] = A.pl(d, 0)[p] / A.maxv;
+    o[1] = A.pl(d, 1)[p] / A.maxv;
+    o[2] = A.pl(d, 2)[p] / A.maxv;
   }
 }
 

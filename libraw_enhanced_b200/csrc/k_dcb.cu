@@ -285,15 +285,24 @@ __device__ __forceinline__ float chroma_native(const float* __restrict__ R, cons
   return (g.fc(r, c) == 0 ? R[i] : B[i]) - G[i];
 }
 
-__global__ void k_dcb_chroma(const float* __restrict__ R, const float* __restrict__ B, const float* __restrict__ G,
-                             float* __restrict__ C0, float* __restrict__ C1, Geo g) {
+// The native chroma of every non-green site (0 outside the first loop's
+// frame), stored once for the second loop's eight-site reads.
+__global__ void k_dcb_chroma_native(const float* __restrict__ R, const float* __restrict__ B,
+                                    const float* __restrict__ G, float* __restrict__ N, Geo g) {
+  GS_FOR_PIXELS(g) {
+    if (g.fc(r, c) == 1) continue;
+    N[g.at(r, c)] = chroma_native(R, B, G, g, r, c);
+  }
+}
+
+__global__ void k_dcb_chroma(const float* __restrict__ N, float* __restrict__ C0, float* __restrict__ C1, Geo g) {
   GS_FOR_PIXELS(g) {
     const unsigned f = g.fc(r, c);
     if (f == 1) continue;
-    const float nat = chroma_native(R, B, G, g, r, c);
+    const float nat = N[g.at(r, c)];
     float opp = 0.0f;
     if (r >= 3 && r < g.H - 3 && c >= 3 && c < g.W - 3) {
-      auto ch = [&](int dr, int dc) { return chroma_native(R, B, G, g, r + dr, c + dc); };
+      auto ch = [&](int dr, int dc) { return N[g.at(r + dr, c + dc)]; };
       const float a = ch(-1, -1), b = ch(1, 1), d = ch(-1, 1), e = ch(1, -1);
       const float f0 = 1.0f / (1.0f + fabsf(a - b) + fabsf(a - ch(-3, -3)) + fabsf(b - ch(-3, -3)));
       const float f1 = 1.0f / (1.0f + fabsf(d - e) + fabsf(d - ch(-3, 3)) + fabsf(e - ch(-3, 3)));
@@ -539,7 +548,8 @@ lre_status launch_dcb(Context* c, const float* raw, int raw_c_stride, float* rgb
     rf.plane[0] = G;
     rf.plane[1] = P1;
     LRE_TRY(sweep<OpRefine>(c, rf, sync, nb_max, "dcb_refinement"));
-    DCB_LAUNCH(k_dcb_chroma, R, B, G, P2, P3, g);
+    DCB_LAUNCH(k_dcb_chroma_native, R, B, G, P4, g);
+    DCB_LAUNCH(k_dcb_chroma, P4, P2, P3, g);
     DCB_LAUNCH(k_dcb_chroma_g, P2, P3, G, P1, P4, g);
     SweepArgs cf = rect(sa, 6);
     cf.plane[0] = R;
