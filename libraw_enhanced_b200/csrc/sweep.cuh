@@ -109,20 +109,19 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 constexpr int kGroup = 16;
 
 // Groups staged ahead of the one being computed.
-constexpr int kAhead = 2;
+constexpr int kAhead = 1;
 // Warps per CTA: one runs the steps, three move data.
 constexpr int kSweepWarps = 4;
 
 // One CTA per band (and channel), four warps:
 //   * warp 0 runs the GS-step groups, touching only shared memory;
 //   * warp 1 handles the band boundaries: in iteration g (while warp 0 runs
-//     group g) it publishes the progress of what it flushed in iteration
-//     g - 1, flushes the columns that became final with group g - 1, waits
-//     for the band above as far as group g + kAhead needs and loads those
-//     upper-halo rows (into registers; they reach the ring one iteration
-//     later);
+//     group g) it flushes the columns that became final with group g - 1,
+//     publishes them at once (a release after the stores), then waits for
+//     the band above as far as group g + kAhead needs and loads those
+//     upper-halo rows into the ring;
 //   * warps 2 and 3 copy group g + kAhead's band-local rows and inputs with
-//     cp.async and wait for group g + 1's copies.
+//     cp.async and wait for them.
 // The warps meet at a named barrier once per group, so global-memory latency
 // overlaps the steps.  Ring capacity: a group reads columns down to
 // t0 - SPAN - HALO - LAG while the copies reach t0 + (kAhead + 1) * GS + HALO.
@@ -207,7 +206,7 @@ __global__ void __launch_bounds__(kSweepWarps * 32) k_gs_sweep(SweepArgs a) {
       const int t0 = a.c_lo + g * GS;
       stage_local(t0 + (kAhead + 1) * GS + HALO);
       cp_async_commit();
-      asm volatile("cp.async.wait_group 1;" ::: "memory");  // group g + 1 resident
+      asm volatile("cp.async.wait_group %0;" ::"n"(kAhead - 1) : "memory");  // group g + 1 resident
       group_barrier();
     }
     cp_async_wait_all();
@@ -236,12 +235,8 @@ __global__ void __launch_bounds__(kSweepWarps * 32) k_gs_sweep(SweepArgs a) {
     }
     if (!__shfl_sync(0xffffffffu, ok, 0)) waiting = false;
   };
-  // Upper-halo rows: at most one value per state plane per lane (GS = 16
-  // columns, HALO <= 2 rows, lane row st_r0 + lr).
-  float nh[NS];
-  int nh_c = 0;
-  bool nh_live = false;
-  auto stage_upper = [&](int hi, bool direct) {
+  // Upper-halo rows of the band above, read once it has published them.
+  auto stage_upper = [&](int hi) {
     hi = min(hi, c_stop);
     if (hi <= staged) return;
     if (band > 0) {
@@ -249,23 +244,9 @@ __global__ void __launch_bounds__(kSweepWarps * 32) k_gs_sweep(SweepArgs a) {
 #pragma unroll
       for (int p = 0; p < NS; p++)
         for (int c = staged + lc; c < hi; c += 16)
-          for (int rr = st_r0 + lr; rr < r0; rr += 2) {
-            const float v = __ldcg(src[p] + (size_t)rr * W + c);
-            if (direct) t(p, rr, c) = v;
-            else nh[p] = v;
-          }
-      if (!direct) {
-        nh_c = staged + lc;
-        nh_live = nh_c < hi && st_r0 + lr < r0;
-      }
+          for (int rr = st_r0 + lr; rr < r0; rr += 2) t(p, rr, c) = __ldcg(src[p] + (size_t)rr * W + c);
     }
     staged = hi;
-  };
-  auto land_upper = [&]() {
-    if (!nh_live) return;
-#pragma unroll
-    for (int p = 0; p < NS; p++) t(p, st_r0 + lr, nh_c) = nh[p];
-    nh_live = false;
   };
   auto flush = [&](int hi) {
     if (hi <= flushed) return;
@@ -283,15 +264,14 @@ __global__ void __launch_bounds__(kSweepWarps * 32) k_gs_sweep(SweepArgs a) {
     published = upto;
   };
 
-  stage_upper(a.c_lo + kAhead * GS + HALO, true);
+  stage_upper(a.c_lo + kAhead * GS + HALO);
   __syncwarp();
   __syncthreads();
   for (int g = 0; g < ngroups; g++) {
     const int t0 = a.c_lo + g * GS;
-    publish(flushed);
     flush(min(t0 - SPAN - Op::LAG, a.c_hi + 1));
-    land_upper();  // group g + kAhead - 1's upper rows
-    stage_upper(t0 + (kAhead + 1) * GS + HALO, false);
+    publish(flushed);
+    stage_upper(t0 + (kAhead + 1) * GS + HALO);
     __syncwarp();
     group_barrier();
   }
