@@ -120,6 +120,7 @@ struct AmazeArgs {
   int ex, ey;
   float clip_pt, clip_pt8, scale;
   int n_top, n_left;
+  int tile_lo, tile_hi;  // tiles [tile_lo, tile_hi) of the n_top x n_left grid
   unsigned char* scratch;
   int* tile_counter;
 };
@@ -212,8 +213,8 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
   for (;;) {
     if (tid == 0) s_tile = atomicAdd(A.tile_counter, 1);
     __syncthreads();
-    const int tile = s_tile;
-    if (tile >= A.n_top * A.n_left) break;
+    const int tile = A.tile_lo + s_tile;
+    if (tile >= A.tile_hi) break;
     const int top = -16 + (tile / A.n_left) * (TS - 32);
     const int left = -16 + (tile % A.n_left) * (TS - 32);
     const int bottom = min(top + TS, H + 16);
@@ -898,8 +899,10 @@ size_t ws_bytes_amaze(size_t w, size_t h) {
   return 160u * kSlabBytes + 4096;
 }
 
-lre_status launch_amaze(Context* c, const float* raw, int cstride, float* rgb, size_t w, size_t h, uint32_t filters,
-                        const float cam_mul[4], float maximum_value) {
+namespace {
+
+AmazeArgs amaze_args(const float* raw, int cstride, float* rgb, size_t w, size_t h, uint32_t filters,
+                     const float cam_mul[4], float maximum_value) {
   AmazeArgs A;
   A.raw = raw;
   A.cstride = cstride;
@@ -929,9 +932,22 @@ lre_status launch_amaze(Context* c, const float* raw, int cstride, float* rgb, s
   for (int top = -16; top < (int)h; top += TS - 32) A.n_top++;
   A.n_left = 0;
   for (int left = -16; left < (int)w; left += TS - 32) A.n_left++;
-  const int tiles = A.n_top * A.n_left;
+  A.tile_lo = 0;
+  A.tile_hi = A.n_top * A.n_left;
+  A.scratch = nullptr;
+  A.tile_counter = nullptr;
+  return A;
+}
+
+// One persistent launch over the tile rows [row_lo, row_hi) of the grid.
+lre_status launch_amaze_rows(Context* c, AmazeArgs A, int row_lo, int row_hi) {
+  A.tile_lo = row_lo * A.n_left;
+  A.tile_hi = row_hi * A.n_left;
+  const int tiles = A.tile_hi - A.tile_lo;
+  if (tiles <= 0) return LRE_OK;
   int nblk = std::min(tiles, c->sm_count);
   if (nblk < 1) nblk = 1;
+  const size_t mark = c->ws.used();
   A.scratch = reinterpret_cast<unsigned char*>(c->ws.take((size_t)nblk * kSlabBytes));
   A.tile_counter = reinterpret_cast<int*>(c->ws.take(256));
   if (!A.scratch || !A.tile_counter) return fail(c, LRE_ERR_OUT_OF_MEMORY, "demosaic_bayer_amaze: workspace too small");
@@ -939,7 +955,44 @@ lre_status launch_amaze(Context* c, const float* raw, int cstride, float* rgb, s
   LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_amaze, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
   k_amaze<<<nblk, AMZ_THREADS, kSmemBytes, c->stream>>>(A);
   count_launch(c);
-  LRE_TRY(check_launch(c, "demosaic_bayer_amaze"));
+  c->ws.rewind(mark);
+  return check_launch(c, "demosaic_bayer_amaze");
+}
+
+}  // namespace
+
+lre_status launch_amaze(Context* c, const float* raw, int cstride, float* rgb, size_t w, size_t h, uint32_t filters,
+                        const float cam_mul[4], float maximum_value) {
+  const AmazeArgs A = amaze_args(raw, cstride, rgb, w, h, filters, cam_mul, maximum_value);
+  LRE_TRY(launch_amaze_rows(c, A, 0, A.n_top));
+  return launch_border_interp(c, rgb, w, h, filters, 4);
+}
+
+lre_status launch_amaze_from_host(Context* c, const float* h_mosaic, float* d_mosaic, float* rgb, size_t w,
+                                  size_t h, uint32_t filters, const float cam_mul[4], float maximum_value,
+                                  cudaStream_t copy_stream, cudaEvent_t* events, int n_events) {
+  const AmazeArgs A = amaze_args(d_mosaic, 1, rgb, w, h, filters, cam_mul, maximum_value);
+  const int bands = std::max(1, std::min(n_events, A.n_top / 4));
+  size_t copied = 0;  // mosaic rows already queued for upload
+  for (int b = 0; b < bands; b++) {
+    const int row_lo = A.n_top * b / bands, row_hi = A.n_top * (b + 1) / bands;
+    // a tile row k reads mosaic rows [128k - 16, 128k + 144) (clamped)
+    const size_t need = std::min(h, (size_t)std::max(0, -16 + (row_hi - 1) * (TS - 32) + TS));
+    if (need > copied) {
+      LRE_CUDA_TRY(c, cudaMemcpyAsync(d_mosaic + copied * w, h_mosaic + copied * w, (need - copied) * w * sizeof(float),
+                                      cudaMemcpyHostToDevice, copy_stream));
+      copied = need;
+    }
+    LRE_CUDA_TRY(c, cudaEventRecord(events[b], copy_stream));
+    LRE_CUDA_TRY(c, cudaStreamWaitEvent(c->stream, events[b], 0));
+    LRE_TRY(launch_amaze_rows(c, A, row_lo, row_hi));
+  }
+  if (copied < h) {  // rows no tile reads still belong to the resident mosaic
+    LRE_CUDA_TRY(c, cudaMemcpyAsync(d_mosaic + copied * w, h_mosaic + copied * w, (h - copied) * w * sizeof(float),
+                                    cudaMemcpyHostToDevice, copy_stream));
+    LRE_CUDA_TRY(c, cudaEventRecord(events[bands - 1], copy_stream));
+    LRE_CUDA_TRY(c, cudaStreamWaitEvent(c->stream, events[bands - 1], 0));
+  }
   return launch_border_interp(c, rgb, w, h, filters, 4);
 }
 

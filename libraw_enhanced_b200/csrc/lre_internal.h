@@ -74,6 +74,10 @@ struct Context {
   void* d_aux = nullptr;
   size_t d_aux_cap = 0;
   float* d_scalars = nullptr;  // 64 floats of per-call scalars (reductions)
+  // Host-buffer develop: a copy stream and events so the mosaic upload
+  // overlaps the demosaic (created on first use, destroyed with the context).
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t band_ev[8] = {};
   std::mutex mu;               // one host-buffer call at a time per context
   int sm_count = 148;
 };
@@ -134,6 +138,13 @@ lre_status launch_lateral_ca(Context* c, const float* in, float* out, size_t w, 
                              int iters, float max_shift, float min_conf, int levels);
 lre_status launch_amaze(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
                         uint32_t filters, const float cam_mul[4], float maximum_value);
+// AMaZE on a mosaic still in host memory: the upload runs in row chunks on
+// copy_stream and each band of tile rows starts as soon as the rows it reads
+// have arrived (results identical to launch_amaze).  d_mosaic receives the
+// whole mosaic.
+lre_status launch_amaze_from_host(Context* c, const float* h_mosaic, float* d_mosaic, float* rgb, size_t w,
+                                  size_t h, uint32_t filters, const float cam_mul[4], float maximum_value,
+                                  cudaStream_t copy_stream, cudaEvent_t* events, int n_events);
 lre_status launch_xtrans(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w,
                          size_t h, const char* xtrans, float maximum_value, int passes);
 

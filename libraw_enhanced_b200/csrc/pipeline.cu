@@ -73,8 +73,18 @@ lre_status validate(Context* c, const lre_develop_params* p, size_t w, size_t h)
 
 // Runs the stage chain on device buffers; returns the buffer holding the
 // final RGB in *result.
+lre_status ensure_copy_stream(Context* c) {
+  if (!c->copy_stream) LRE_CUDA_TRY(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+  for (cudaEvent_t& e : c->band_ev)
+    if (!e) LRE_CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return LRE_OK;
+}
+
+// h_mosaic (nullable): the mosaic is still in host memory and d_mosaic is
+// its destination; the AMaZE route overlaps the upload with the demosaic,
+// every other route uploads it first.
 lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb_b, size_t w, size_t h,
-                     const lre_develop_params& p, float** result) {
+                     const lre_develop_params& p, float** result, const float* h_mosaic = nullptr) {
   float* cur = rgb_a;
   float* other = rgb_b;
   const size_t mark = c->ws.used();
@@ -82,6 +92,9 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
   // through a device flag (d_scalars[63]); the host-buffer entry point reads
   // it after its final synchronisation.
   int* d_err = reinterpret_cast<int*>(c->d_scalars + 63);
+  if (h_mosaic && route(p) != Demosaic::Amaze)
+    LRE_CUDA_TRY(c, cudaMemcpyAsync(const_cast<float*>(d_mosaic), h_mosaic, w * h * sizeof(float),
+                                    cudaMemcpyHostToDevice, c->stream));
   switch (route(p)) {
     case Demosaic::Xtrans1:
     case Demosaic::Xtrans3:
@@ -100,7 +113,16 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
       LRE_TRY(lre::launch_aahd(c, d_mosaic, 1, cur, w, h, p.filters, p.maximum_value, d_err));
       break;
     case Demosaic::Amaze:
-      LRE_TRY(lre::launch_amaze(c, d_mosaic, 1, cur, w, h, p.filters, p.cam_mul, p.maximum_value));
+      if (h_mosaic) {
+        LRE_TRY(ensure_copy_stream(c));
+        // the copy stream must not start before earlier work on the mosaic buffer
+        LRE_CUDA_TRY(c, cudaEventRecord(c->band_ev[7], c->stream));
+        LRE_CUDA_TRY(c, cudaStreamWaitEvent(c->copy_stream, c->band_ev[7], 0));
+        LRE_TRY(lre::launch_amaze_from_host(c, h_mosaic, const_cast<float*>(d_mosaic), cur, w, h, p.filters, p.cam_mul,
+                                            p.maximum_value, c->copy_stream, c->band_ev, 6));
+      } else {
+        LRE_TRY(lre::launch_amaze(c, d_mosaic, 1, cur, w, h, p.filters, p.cam_mul, p.maximum_value));
+      }
       break;
   }
   c->ws.rewind(mark);
@@ -256,9 +278,8 @@ lre_status lre_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t w, s
   LRE_CUDA_TRY(c, c->ws.reserve(2 * rgb_bytes + stage_ws(p, w, h), c->stream));
   float* rgb_a = reinterpret_cast<float*>(c->ws.take(rgb_bytes));
   float* rgb_b = reinterpret_cast<float*>(c->ws.take(rgb_bytes));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, mosaic, in_bytes, cudaMemcpyHostToDevice, c->stream));
   float* res = nullptr;
-  LRE_TRY(run_chain(c, reinterpret_cast<const float*>(c->d_in), rgb_a, rgb_b, w, h, p, &res));
+  LRE_TRY(run_chain(c, reinterpret_cast<const float*>(c->d_in), rgb_a, rgb_b, w, h, p, &res, mosaic));
   if (p.output_bits == 16) {
     LRE_TRY(lre::launch_quantize_u16(c, res, reinterpret_cast<uint16_t*>(c->d_out), w * h * 3));
     LRE_CUDA_TRY(c, cudaMemcpyAsync(out, c->d_out, out_bytes, cudaMemcpyDeviceToHost, c->stream));
