@@ -647,6 +647,7 @@ def run_demosaics(args, acc, stream, d_mos, W, H):
 
     from libraw_enhanced_b200 import scenes
 
+    acc.set_stream(stream.cuda_stream)  # the e2e leg leaves the library on its own stream
     mos = (d_mos * 16383.0).contiguous()
     out = torch.empty((H, W, 3), dtype=torch.float32, device=mos.device)
     f = scenes.FILTERS["RGGB"]

@@ -152,7 +152,12 @@ void lre_destroy(lre_ctx* ctx) {
   if (c->d_scalars) cudaFree(c->d_scalars);
   for (cudaEvent_t& e : c->band_ev)
     if (e) cudaEventDestroy(e);
-  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  for (cudaEvent_t& e : c->tail_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->copy_stream) {
+    cudaStreamSynchronize(c->copy_stream);
+    cudaStreamDestroy(c->copy_stream);
+  }
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }

@@ -24,6 +24,8 @@
 // remains for the allocation-free entry point at the end of this file.
 #include <mutex>
 
+#include <functional>
+
 #include "common.cuh"
 #include "lre_internal.h"
 
@@ -466,13 +468,13 @@ template <int WS>
 __global__ void __launch_bounds__(32) k_ax_ab(const float* __restrict__ src, int W, int H, int r, float eps, int HS,
                                              const float* __restrict__ d_maxg, float* __restrict__ aR,
                                              float* __restrict__ bR, float* __restrict__ aB, float* __restrict__ bB,
-                                             float* __restrict__ er) {
+                                             float* __restrict__ er, int yb0) {
   constexpr int NQ = 6;
   constexpr int PL = WS / 32;
   __shared__ double Vs[NQ][vs_len<WS>()];
   const int VC = WS + 2 * r;
   const float inv_norm = 1.f / fmaxf(*d_maxg, 1e-6f);
-  const int x0 = blockIdx.x * WS, y0 = blockIdx.y * HS;
+  const int x0 = blockIdx.x * WS, y0 = (blockIdx.y + yb0) * HS;  // yb0: first row chunk of this launch
   const int xv0 = x0 - r;
   const int y_end = min(y0 + HS, H);
   auto ld = [&](int x, int y, double* q) { AbQ::load(src, W, H, x, y, inv_norm, q); };
@@ -528,14 +530,14 @@ __global__ void __launch_bounds__(32) k_ax_q(const float* __restrict__ src, floa
                                             int r, float strength, int HS, const float* __restrict__ d_maxg,
                                             const float* __restrict__ aR, const float* __restrict__ bR,
                                             const float* __restrict__ aB, const float* __restrict__ bB,
-                                            const float* __restrict__ er) {
+                                            const float* __restrict__ er, int yb0) {
   constexpr int NQ = 5;
   constexpr int PL = WS / 32;
   __shared__ double Vs[NQ][vs_len<WS>()];
   const int VC = WS + 2 * r;
   const float norm_ref = fmaxf(*d_maxg, 1e-6f);
   const float inv_norm = 1.f / norm_ref;
-  const int x0 = blockIdx.x * WS, y0 = blockIdx.y * HS;
+  const int x0 = blockIdx.x * WS, y0 = (blockIdx.y + yb0) * HS;  // yb0: first row chunk of this launch
   const int xv0 = x0 - r;
   const int y_end = min(y0 + HS, H);
   auto ld = [&](int x, int y, double* q) {
@@ -602,8 +604,30 @@ cudaError_t axial_stream(size_t w, size_t h, int HS, cudaStream_t s, const float
   float* bB = planes + 3 * n;
   float* er = planes + 4 * n;
   dim3 grid((unsigned)((w + WS - 1) / WS), (unsigned)((h + HS - 1) / HS));
-  k_ax_ab<WS><<<grid, 32, 0, s>>>(src, (int)w, (int)h, r, eps, HS, d_max, aR, bR, aB, bB, er);
-  k_ax_q<WS><<<grid, 32, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max, aR, bR, aB, bB, er);
+  k_ax_ab<WS><<<grid, 32, 0, s>>>(src, (int)w, (int)h, r, eps, HS, d_max, aR, bR, aB, bB, er, 0);
+  k_ax_q<WS><<<grid, 32, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max, aR, bR, aB, bB, er, 0);
+  return cudaPeekAtLastError();
+}
+
+// The same two passes over row chunks [k0, k1) (pass A) or [k0, k1) (pass B).
+template <int WS>
+cudaError_t axial_pass_a(size_t w, size_t h, int HS, int k0, int k1, cudaStream_t s, const float* src, int r,
+                         float eps, const float* d_max, float* planes) {
+  if (k1 <= k0) return cudaSuccess;
+  const size_t n = w * h;
+  dim3 grid((unsigned)((w + WS - 1) / WS), (unsigned)(k1 - k0));
+  k_ax_ab<WS><<<grid, 32, 0, s>>>(src, (int)w, (int)h, r, eps, HS, d_max, planes, planes + n, planes + 2 * n,
+                                  planes + 3 * n, planes + 4 * n, k0);
+  return cudaPeekAtLastError();
+}
+template <int WS>
+cudaError_t axial_pass_b(size_t w, size_t h, int HS, int k0, int k1, cudaStream_t s, const float* src, float* out,
+                         int r, float strength, const float* d_max, float* planes) {
+  if (k1 <= k0) return cudaSuccess;
+  const size_t n = w * h;
+  dim3 grid((unsigned)((w + WS - 1) / WS), (unsigned)(k1 - k0));
+  k_ax_q<WS><<<grid, 32, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max, planes, planes + n,
+                                 planes + 2 * n, planes + 3 * n, planes + 4 * n, k0);
   return cudaPeekAtLastError();
 }
 
@@ -615,6 +639,51 @@ size_t ws_bytes_axial(size_t w, size_t h, int radius) {
   // when the caller runs in place (pass B reads input rows below the rows it
   // writes).
   return ((w * h * 5 * sizeof(float) + 255) & ~size_t(255)) + w * h * 3 * sizeof(float) + 256;
+}
+
+lre_status launch_axial_ca_banded(Context* c, const float* in, float* out, size_t w, size_t h, int radius, float eps,
+                                  float strength, const float* d_max_g, int bands,
+                                  const std::function<lre_status(size_t, size_t)>& rows_done) {
+  if (radius < 1) radius = 1;
+  if (radius > 16) return fail(c, LRE_ERR_INVALID_ARGUMENT, "ca_axial_cleanup: radius > 16 is not supported");
+  if (in == out) return fail(c, LRE_ERR_INVALID_ARGUMENT, "ca_axial_cleanup: banded form runs out of place");
+  strength = fminf(fmaxf(strength, 0.f), 1.f);
+  float* planes = reinterpret_cast<float*>(c->ws.take(w * h * 5 * sizeof(float)));
+  if (!planes) return fail(c, LRE_ERR_OUT_OF_MEMORY, "ca_axial_cleanup: workspace too small");
+  const int WS = c->tune.axial_strip == 64 ? 64 : 128;
+  const size_t strips_x = (w + WS - 1) / WS;
+  const size_t want = (size_t)c->sm_count * 24;
+  // each launch covers one band, so the strip height is chosen for a band
+  // (not the whole image) to fill the GPU
+  bands = std::max(1, bands);
+  int HS = c->tune.axial_rows == 128 ? 128 : 64;
+  while (HS > 16 && strips_x * ((h + HS - 1) / HS) < want * (size_t)bands) HS /= 2;
+  // pass B of a chunk reads pass A's planes up to `radius` (<= HS) rows below
+  // it, so pass A runs one band ahead of pass B
+  const int nch = (int)((h + HS - 1) / HS);
+  bands = std::min(bands, nch);
+  auto edge = [&](int b) { return (int)((long long)nch * b / bands); };
+  auto pass_a = [&](int b) {
+    return WS == 64 ? axial_pass_a<64>(w, h, HS, edge(b), edge(b + 1), c->stream, in, radius, eps, d_max_g, planes)
+                    : axial_pass_a<128>(w, h, HS, edge(b), edge(b + 1), c->stream, in, radius, eps, d_max_g, planes);
+  };
+  LRE_CUDA_TRY(c, pass_a(0));
+  count_launch(c);
+  for (int b = 0; b < bands; b++) {
+    if (b + 1 < bands) {
+      LRE_CUDA_TRY(c, pass_a(b + 1));
+      count_launch(c);
+    }
+    LRE_CUDA_TRY(c, WS == 64 ? axial_pass_b<64>(w, h, HS, edge(b), edge(b + 1), c->stream, in, out, radius, strength,
+                                                  d_max_g, planes)
+                             : axial_pass_b<128>(w, h, HS, edge(b), edge(b + 1), c->stream, in, out, radius, strength,
+                                                   d_max_g, planes));
+    count_launch(c);
+    LRE_TRY(check_launch(c, "ca_axial_cleanup"));
+    const size_t r0 = std::min(h, (size_t)edge(b) * HS), r1 = std::min(h, (size_t)edge(b + 1) * HS);
+    LRE_TRY(rows_done(r0, r1));
+  }
+  return LRE_OK;
 }
 
 lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, size_t h, int radius, float eps,

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <functional>
 #include <cstddef>
 #include <cstdint>
 #include <mutex>
@@ -78,6 +79,7 @@ struct Context {
   // overlaps the demosaic (created on first use, destroyed with the context).
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t band_ev[8] = {};
+  cudaEvent_t tail_ev[8] = {};  // rows of the final RGB ready for download
   std::mutex mu;               // one host-buffer call at a time per context
   int sm_count = 148;
 };
@@ -128,6 +130,11 @@ lre_status launch_channel_max(Context* c, const float* rgb, size_t n_px, int cha
                               bool clamp0);
 lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, size_t h, int radius,
                            float eps, float strength, const float* d_max_g);
+// The guided filter in row bands (out of place): after pass B of each band,
+// rows_done(row_lo, row_hi) enqueues what may follow on those rows.
+lre_status launch_axial_ca_banded(Context* c, const float* in, float* out, size_t w, size_t h, int radius, float eps,
+                                  float strength, const float* d_max_g, int bands,
+                                  const std::function<lre_status(size_t, size_t)>& rows_done);
 lre_status launch_defringe(Context* c, const float* in, float* out, size_t w, size_t h, float radius,
                            float edge_thr, float chroma_thr, float strength, bool green,
                            float green_scale, const float* d_max_g);

@@ -10,6 +10,7 @@
 // other stage runs in place.
 #include <algorithm>
 #include <cstring>
+#include <functional>
 
 #include "lre_internal.h"
 
@@ -77,14 +78,30 @@ lre_status ensure_copy_stream(Context* c) {
   if (!c->copy_stream) LRE_CUDA_TRY(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
   for (cudaEvent_t& e : c->band_ev)
     if (!e) LRE_CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (cudaEvent_t& e : c->tail_ev)
+    if (!e) LRE_CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   return LRE_OK;
+}
+
+// Called for each row band [r0, r1) of the final RGB (buffer `rgb`) as soon
+// as its last stage is enqueued, when the chain can finish in row bands.
+using RowsReady = std::function<lre_status(const float* rgb, size_t r0, size_t r1)>;
+
+// The chain can hand out its result in row bands when it ends with the axial
+// guided filter followed only by pointwise work (the 51 MP workload's order:
+// ... -> defringe -> axial -> ACES tone map).
+bool banded_tail(const lre_develop_params& p) {
+  return p.stage_order == 1 && p.axial_ca_correction && p.tone_mapping != 2;
 }
 
 // h_mosaic (nullable): the mosaic is still in host memory and d_mosaic is
 // its destination; the AMaZE route overlaps the upload with the demosaic,
 // every other route uploads it first.
+// tail (nullable): when banded_tail(p), the axial filter and the tone map run
+// in row bands and each finished band is passed to *tail.
 lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb_b, size_t w, size_t h,
-                     const lre_develop_params& p, float** result, const float* h_mosaic = nullptr) {
+                     const lre_develop_params& p, float** result, const float* h_mosaic = nullptr,
+                     const RowsReady* tail = nullptr) {
   float* cur = rgb_a;
   float* other = rgb_b;
   const size_t mark = c->ws.used();
@@ -147,11 +164,25 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
     c->ws.rewind(mark);
     return LRE_OK;
   };
+  const bool in_bands = tail && banded_tail(p);
   auto axial = [&]() -> lre_status {
     if (!p.axial_ca_correction) return LRE_OK;
     float* dmax = c->d_scalars + 1;
     LRE_TRY(lre::launch_channel_max(c, cur, w * h, 1, dmax, true));
-    LRE_TRY(lre::launch_axial_ca(c, cur, other, w, h, p.axial_ca_radius, p.axial_ca_epsilon, p.axial_ca_strength, dmax));
+    if (in_bands) {
+      float* dst = other;
+      LRE_TRY(lre::launch_axial_ca_banded(
+          c, cur, dst, w, h, p.axial_ca_radius, p.axial_ca_epsilon, p.axial_ca_strength, dmax, 8,
+          [&](size_t r0, size_t r1) -> lre_status {
+            if (p.tone_mapping == 1)
+              LRE_TRY(lre::launch_tone_mapping(c, dst + r0 * w * 3, dst + r0 * w * 3, (r1 - r0) * w,
+                                               p.tone_after_scale));
+            return (*tail)(dst, r0, r1);
+          }));
+    } else {
+      LRE_TRY(lre::launch_axial_ca(c, cur, other, w, h, p.axial_ca_radius, p.axial_ca_epsilon, p.axial_ca_strength,
+                                   dmax));
+    }
     std::swap(cur, other);
     c->ws.rewind(mark);
     return LRE_OK;
@@ -167,7 +198,7 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
   if (p.stage_order == 1) {
     LRE_TRY(defringe());
     LRE_TRY(axial());
-    LRE_TRY(tone());
+    if (!in_bands) LRE_TRY(tone());
   } else {
     LRE_TRY(tone());
     LRE_TRY(lateral());
@@ -279,12 +310,48 @@ lre_status lre_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t w, s
   float* rgb_a = reinterpret_cast<float*>(c->ws.take(rgb_bytes));
   float* rgb_b = reinterpret_cast<float*>(c->ws.take(rgb_bytes));
   float* res = nullptr;
-  LRE_TRY(run_chain(c, reinterpret_cast<const float*>(c->d_in), rgb_a, rgb_b, w, h, p, &res, mosaic));
-  if (p.output_bits == 16) {
-    LRE_TRY(lre::launch_quantize_u16(c, res, reinterpret_cast<uint16_t*>(c->d_out), w * h * 3));
-    LRE_CUDA_TRY(c, cudaMemcpyAsync(out, c->d_out, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+  const size_t px_bytes = 3 * (p.output_bits == 16 ? 2 : 4);
+  if (banded_tail(p)) {
+    // The download overlaps the rest of the chain: each row band of the
+    // result (quantised when 16-bit) is downloaded on the copy stream once
+    // the main stream has finished it.  All kernels are enqueued before the
+    // first copy, so a pageable destination (whose copies return only when
+    // done) does not hold back the kernel queue.
+    LRE_TRY(ensure_copy_stream(c));
+    struct Band {
+      const void* src;
+      size_t r0, r1;
+    };
+    Band bands[8];
+    int nb = 0;
+    const RowsReady tail = [&](const float* rgb, size_t r0, size_t r1) -> lre_status {
+      if (nb >= 8) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "develop: internal: more than 8 row bands");
+      const void* src = rgb + r0 * w * 3;
+      if (p.output_bits == 16) {
+        uint16_t* q = reinterpret_cast<uint16_t*>(c->d_out) + r0 * w * 3;
+        LRE_TRY(lre::launch_quantize_u16(c, rgb + r0 * w * 3, q, (r1 - r0) * w * 3));
+        src = q;
+      }
+      LRE_CUDA_TRY(c, cudaEventRecord(c->tail_ev[nb], c->stream));
+      bands[nb++] = {src, r0, r1};
+      return LRE_OK;
+    };
+    LRE_TRY(run_chain(c, reinterpret_cast<const float*>(c->d_in), rgb_a, rgb_b, w, h, p, &res, mosaic, &tail));
+    for (int b = 0; b < nb; b++) {
+      LRE_CUDA_TRY(c, cudaStreamWaitEvent(c->copy_stream, c->tail_ev[b], 0));
+      LRE_CUDA_TRY(c, cudaMemcpyAsync(static_cast<char*>(out) + bands[b].r0 * w * px_bytes, bands[b].src,
+                                      (bands[b].r1 - bands[b].r0) * w * px_bytes, cudaMemcpyDeviceToHost,
+                                      c->copy_stream));
+    }
+    LRE_CUDA_TRY(c, cudaStreamSynchronize(c->copy_stream));
   } else {
-    LRE_CUDA_TRY(c, cudaMemcpyAsync(out, res, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+    LRE_TRY(run_chain(c, reinterpret_cast<const float*>(c->d_in), rgb_a, rgb_b, w, h, p, &res, mosaic));
+    if (p.output_bits == 16) {
+      LRE_TRY(lre::launch_quantize_u16(c, res, reinterpret_cast<uint16_t*>(c->d_out), w * h * 3));
+      LRE_CUDA_TRY(c, cudaMemcpyAsync(out, c->d_out, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+    } else {
+      LRE_CUDA_TRY(c, cudaMemcpyAsync(out, res, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+    }
   }
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   const Demosaic d = route(p);
