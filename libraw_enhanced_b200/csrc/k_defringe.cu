@@ -525,305 +525,427 @@ __global__ void __launch_bounds__(256) k_df_line(const float* __restrict__ src, 
 }
 
 // ---------------------------------------------------------------- K7
-__global__ void __launch_bounds__(256, 3) k_df_main(const float* src, float* dst, int W, int H, DfPlanes P, DfConst k, const DfScalars* sc) {
+// Constants of the main pass (core/cpu_accelerator.cpp:4376-4706), formed
+// once per thread.
+struct DfMainK {
+  float inv_s, mask_cutoff, scene_highlight_gate, edge_threshold, chroma_threshold, strength, green_strength_scale;
+  float e0_edge, e0_raw;
+  bool enable_green, can_skip;
+};
+
+// The eleven planes the main pass reads at one pixel.
+struct DfPx {
+  float be, ber, srb, sbb, bg, blrg, blbg, bfs, lfs, lrg, lbg;
+};
+
+// Pixels that provably keep their input: with green correction off, either
+// edge factor at or below its lower smoothstep edge zeroes both edge weights
+// (the other factor is finite, or NaN, and a NaN mask never passes the
+// cutoff), so no ratio/direct correction applies; zero solo blurs make the
+// solo masks zero.  The output is then the input whatever the other planes
+// hold, so those pixels need 4 planes instead of 11 and skip the rest.
+__device__ __forceinline__ bool df_keeps_input(const DfMainK& K, float be, float ber, float srb, float sbb) {
+  return K.can_skip && (be <= K.e0_edge || ber <= K.e0_raw) && srb == 0.f && sbb == 0.f;
+}
+
+// The correction of one pixel (s0, s1, s2) -> (d0, d1, d2).
+__device__ __forceinline__ void df_main_px(float s0, float s1, float s2, const DfPx& v, const DfMainK& K, float& d0,
+                                           float& d1, float& d2) {
+  const float inv_s = K.inv_s;
+  const float mask_cutoff = K.mask_cutoff;
+  const float scene_highlight_gate = K.scene_highlight_gate;
+  const bool enable_green = K.enable_green;
+  const float edge_threshold = K.edge_threshold, chroma_threshold = K.chroma_threshold, strength = K.strength;
+  const float green_strength_scale = K.green_strength_scale;
+  d0 = s0;
+  d1 = s1;
+  d2 = s2;
+  const float blur_guide = v.bg;
+  const float blur_log_rg = v.blrg;
+  const float blur_log_bg = v.blbg;
+  const float blur_fringe_support = v.bfs;
+  const float line_support = v.lfs;
+
+  const float rg = v.lrg;
+  const float bg = v.lbg;
+  const float dr = rg - blur_log_rg;
+  const float db = bg - blur_log_bg;
+  const float r0 = smax(s0, 0.f);
+  const float g0 = smax(s1, 0.f);
+  const float b0 = smax(s2, 0.f);
+  const float rb_avg_pre = 0.5f * (r0 + b0);
+  const float purple_r = smax(0.f, dr);
+  const float purple_b = smax(0.f, db);
+  const float green_r = smax(0.f, -dr);
+  const float green_b = smax(0.f, -db);
+  const float purple_excess = smin(purple_r, purple_b);
+  const float denom = smax(blur_guide, 0.05f);
+  const float g_over_min = smax(0.f, g0 - smin(r0, b0)) / denom;
+  const float green_dom = ssmooth(0.010f, 0.060f, g_over_min);
+  const float green_excess = smax(green_r, green_b) * green_dom;
+  const bool is_purple = purple_excess >= green_excess;
+  const float excess = is_purple ? purple_excess : green_excess;
+  const float min_dir = is_purple ? smax(0.f, smin(rg, bg)) : smax(0.f, smin(-rg, -bg));
+  const float max_dir = is_purple ? smax(1e-4f, smax(rg, bg)) : smax(1e-4f, smax(-rg, -bg));
+  const float balance = min_dir / max_dir;
+  const float c_edge_core = ssmooth(edge_threshold * 0.35f * inv_s, edge_threshold * 1.50f * inv_s, v.be) *
+                            ssmooth(0.55f * inv_s, 1.35f * inv_s, v.ber);
+  const float c_edge_low = ssmooth(edge_threshold * 0.10f * inv_s, edge_threshold * 0.80f * inv_s, v.be) *
+                           ssmooth(0.20f * inv_s, 0.90f * inv_s, v.ber);
+  const float linked_fringe = ssmooth(0.004f, 0.045f, smax(blur_fringe_support, line_support * 0.90f));
+  const float c_bright = ssmooth(0.24f * inv_s, 0.52f * inv_s, blur_guide);
+  const float c_chroma = ssmooth(chroma_threshold * 0.45f * inv_s, chroma_threshold * 1.60f * inv_s, excess);
+  const float red_blue_balance_hue = b0 / smax(r0, 1e-4f);
+  const float blue_lift_hue = smax(0.f, b0 - g0) / smax(r0 - g0, 1e-4f);
+  const float red_purple_hue_signal = ssmooth(0.50f, 0.72f, red_blue_balance_hue) * ssmooth(0.24f, 0.42f, blue_lift_hue);
+  const float balanced_hue = ssmooth(0.06f * inv_s, 0.22f * inv_s, min_dir) * ssmooth(0.35f, 0.75f, balance);
+  const float red_purple_hue_gate = is_purple ? smin(1.f, red_purple_hue_signal * 1.50f) *
+                                                    ssmooth(0.035f * inv_s, 0.16f * inv_s, min_dir) *
+                                                    ssmooth(0.18f, 0.58f, balance)
+                                              : 0.f;
+  const float green_unbalanced_hue =
+      (enable_green && !is_purple) ? ssmooth(0.035f * inv_s, 0.16f * inv_s, max_dir) : 0.f;
+  const float c_hue = smax(balanced_hue, smax(red_purple_hue_gate, green_unbalanced_hue));
+  const float rb_avg = rb_avg_pre;
+  const float purple_abs = smin(smax(0.f, r0 - g0), smax(0.f, b0 - g0)) / smax(blur_guide, 0.05f);
+  const float green_abs_base = smax(0.f, g0 - rb_avg) / smax(blur_guide, 0.05f);
+  const float green_abs_alt = smax(0.f, g0 - smin(r0, b0)) / smax(blur_guide, 0.05f);
+  const float green_abs = smax(green_abs_base, 0.55f * green_abs_alt);
+  const bool abs_is_purple = purple_abs >= green_abs;
+  const float abs_excess = abs_is_purple ? purple_abs : green_abs;
+  const float c_abs = ssmooth(chroma_threshold * 0.35f * inv_s, chroma_threshold * 1.20f * inv_s, abs_excess);
+  const float low_contrast_color =
+      ssmooth(chroma_threshold * 1.20f * inv_s, chroma_threshold * 2.40f * inv_s, abs_excess);
+  const float green_soft_edge_boost =
+      (enable_green && !is_purple) ? c_edge_low * ssmooth(0.05f * inv_s, 0.20f * inv_s, max_dir) : 0.f;
+  const float c_edge = smax(c_edge_core, smax(c_edge_low * linked_fringe * 1.45f,
+                                              smax(c_edge_low * low_contrast_color * 0.35f, green_soft_edge_boost)));
+  const float ratio_mask = c_edge * c_bright * c_hue * c_chroma;
+  const float direct_mask = c_edge * c_bright * c_hue * c_abs;
+  const bool use_direct = direct_mask > ratio_mask;
+  float mask = smax(ratio_mask, direct_mask) * scene_highlight_gate;
+  const bool correct_purple = use_direct ? abs_is_purple : is_purple;
+  float local_gate = 0.f;
+  if (correct_purple) {
+    local_gate = ssmooth(chroma_threshold * 0.10f * inv_s, chroma_threshold * 0.55f * inv_s, purple_abs);
+    mask *= local_gate;
+  } else {
+    local_gate = ssmooth(chroma_threshold * 0.10f * inv_s, chroma_threshold * 0.55f * inv_s, green_abs);
+    if (enable_green) {
+      const float peak_chroma_signal =
+          ssmooth(chroma_threshold * 0.80f * inv_s, chroma_threshold * 2.50f * inv_s, green_abs);
+      const float peak_neighbourhood = ssmooth(0.005f, 0.030f, blur_fringe_support);
+      const float green_peak_mask = peak_chroma_signal * peak_neighbourhood * c_bright * c_hue;
+      mask = smax(mask, green_peak_mask * scene_highlight_gate);
+    }
+    const float green_highlight_protect = 1.f - 0.85f * ssmooth(0.62f, 0.88f, blur_guide);
+    const float rb_to_green = rb_avg / smax(g0, 1e-4f);
+    const float natural_green_highlight = ssmooth(0.22f, 0.46f, rb_to_green) * ssmooth(0.30f, 0.55f, g0);
+    const float natural_green_suppress = 1.f - 0.99f * natural_green_highlight;
+    const float natural_green_suppress_sq = natural_green_suppress * natural_green_suppress;
+    const float green_halo_strength =
+        ssmooth(chroma_threshold * 0.55f * inv_s, chroma_threshold * 1.65f * inv_s, green_abs);
+    const float green_gain_base = enable_green ? 0.60f : 0.35f;
+    const float green_gain_slope = enable_green ? 1.10f : 0.95f;
+    const float green_gain = green_gain_base + green_gain_slope * green_halo_strength;
+    const float min_ratio_ref = smin(blur_log_rg, blur_log_bg);
+    const float green_neighbour = ssmooth(0.02f, 0.10f, smax(0.f, -min_ratio_ref));
+    const float src_max = smax(r0, smax(g0, b0));
+    const float src_min = smin(r0, smin(g0, b0));
+    const float src_chroma = src_max - src_min;
+    const float src_sat = src_chroma / smax(src_max, 1e-4f);
+    const float whiteish = 1.f - ssmooth(0.05f, 0.13f, src_sat);
+    const float foliage_guard =
+        green_neighbour * whiteish * ssmooth(0.35f, 0.75f, blur_guide) * (1.f - green_halo_strength);
+    const float strength_release = enable_green ? ssmooth(2.0f, 6.0f, strength) : 0.f;
+    const float green_line_evidence = ssmooth(0.004f, 0.030f, line_support) *
+                                      ssmooth(0.20f, 0.55f, green_halo_strength) * ssmooth(0.05f, 0.15f, src_sat);
+    const float not_natural_green = 1.f - natural_green_highlight;
+    const float guard_release = strength_release * green_line_evidence * not_natural_green;
+    const float released_highlight_protect = green_highlight_protect + (1.f - green_highlight_protect) * guard_release;
+    const float released_natural_suppress =
+        natural_green_suppress_sq + (1.f - natural_green_suppress_sq) * guard_release;
+    const float foliage_term = 1.f - 0.999f * foliage_guard;
+    const float released_foliage_term = foliage_term + (1.f - foliage_term) * guard_release;
+    mask *= local_gate * green_gain * released_highlight_protect * released_natural_suppress * released_foliage_term;
+    const float line_kill_evidence = ssmooth(0.04f, 0.15f, line_support);
+    const float natural_blob =
+        sqrtf(smax(0.f, natural_green_highlight)) * (1.f - line_kill_evidence) * green_neighbour;
+    mask *= 1.f - 0.999f * natural_blob;
+    if (!enable_green) mask = 0.f;
+  }
+
+  bool skip_rest = false;
+  if (mask > mask_cutoff) {
+    const float g = smax(s1, 0.f);
+    const float red_strength = smax(0.f, r0 - smax(g0, b0)) / smax(r0, 1e-4f);
+    const float red_blue_balance = b0 / smax(r0, 1e-4f);
+    const float blue_lift = smax(0.f, b0 - g0) / smax(r0 - g0, 1e-4f);
+    const float red_purple_balance = ssmooth(0.55f, 0.78f, red_blue_balance);
+    const float red_purple_lift = ssmooth(0.16f, 0.34f, blue_lift);
+    const float red_purple = smax(red_purple_balance, red_purple_lift);
+    const float red_strength_guard = ssmooth(0.08f, 0.25f, red_strength);
+    float red_purple_context = 0.f;
+    float contextual_red_purple = 0.f;
+    float red_magenta_surface = 0.f;
+    if (red_purple > 0.50f) {
+      red_purple_context = linked_fringe;
+      contextual_red_purple = red_purple * red_purple_context;
+      if (red_purple_context < 0.20f && red_strength_guard < 0.50f && red_purple > 0.50f) {
+        red_magenta_surface = ssmooth(0.02f, 0.12f, purple_abs) * (1.f - red_purple_context);
+      }
+    }
+    float neutral_gray_surface = 0.f;
+    if (strength > 3.f && red_purple_context > 0.80f && line_support > 0.012f && red_strength_guard < 0.98f &&
+        blue_lift > 1.10f && red_blue_balance > 0.82f && purple_abs > 0.015f) {
+      const float neutral_gray_edge = ssmooth(1.10f, 1.80f, blue_lift) * ssmooth(0.82f, 1.05f, red_blue_balance) *
+                                      (1.f - red_strength_guard);
+      neutral_gray_surface = neutral_gray_edge * ssmooth(0.015f, 0.08f, purple_abs) * ssmooth(3.f, 8.f, strength);
+    }
+    const float red_object_strength = smax(red_strength_guard, red_magenta_surface);
+    const float natural_warm_guard_base = 1.f - red_object_strength * (1.f - contextual_red_purple);
+    const float natural_warm_guard_sq =
+        natural_warm_guard_base * natural_warm_guard_base * natural_warm_guard_base * natural_warm_guard_base;
+    const float natural_warm_guard = natural_warm_guard_sq * natural_warm_guard_sq;
+    const float line_purple_relief = ssmooth(0.012f, 0.06f, line_support) * ssmooth(0.10f, 0.24f, blue_lift);
+    const float red_object_guard = ssmooth(0.55f, 0.90f, red_object_strength);
+    const float linked_override = linked_fringe * 1.05f * (1.f - 0.85f * red_object_guard);
+    const float line_override = line_purple_relief * (1.f - 0.85f * red_object_guard);
+    const bool force_warm_guard = (red_object_guard > 0.75f) && (linked_fringe < 0.65f) && (line_purple_relief < 0.45f);
+    const float warm_protect = correct_purple
+                                   ? (force_warm_guard ? natural_warm_guard
+                                                       : smax(natural_warm_guard, smax(linked_override, line_override)))
+                                   : 1.f;
+    const float red_without_support =
+        ssmooth(0.22f, 0.45f, red_strength) * (1.f - ssmooth(0.02f, 0.12f, blur_fringe_support));
+    const float protect = correct_purple ? red_without_support : 0.f;
+    const float smooth_mask = ssmooth(mask_cutoff, mask_cutoff * 5.0f, mask);
+    const float threshold_soften = 1.f - 0.86f * ssmooth(0.22f, 0.40f, chroma_threshold);
+    const float src_max = smax(r0, smax(g0, b0));
+    const float src_min = smin(r0, smin(g0, b0));
+    const float src_chroma = src_max - src_min;
+    const float src_sat = src_chroma / smax(src_max, 1e-4f);
+    const float neutral_guard_base = ssmooth(0.008f, 0.030f, src_sat);
+    const float neutral_guard = 1.f - (1.f - neutral_guard_base) * ssmooth(0.35f, 0.80f, red_object_strength);
+    float amount = sclamp(smooth_mask * strength * 1.90f * (1.f - protect) * warm_protect * neutral_guard *
+                              threshold_soften,
+                          0.f, 1.f);
+    const float warm_edge_surface = ssmooth(0.006f, 0.035f, purple_abs) * ssmooth(0.25f, 0.65f, red_purple) *
+                                    ssmooth(0.15f, 0.65f, red_purple_context) * (1.f - 0.55f * red_strength_guard) *
+                                    ssmooth(3.f, 8.f, strength);
+    const float safe_surface = smax(neutral_gray_surface, warm_edge_surface);
+    if (correct_purple && safe_surface > 1e-4f) {
+      const float safe_amount_cap = 1.f - 0.99f * safe_surface;
+      amount = smin(amount, safe_amount_cap);
+    }
+    if (amount <= 1e-4f) {
+      skip_rest = true;
+    } else {
+      const float e_rg = exp_cr(blur_log_rg);
+      const float e_bg = exp_cr(blur_log_bg);
+      const float target_r = smin(g, g * e_rg);
+      const float target_b = smin(g, g * e_bg);
+      if (correct_purple) {
+        float corrected_r = sclamp(s0 * (1.f - amount) + target_r * amount, 0.f, s0);
+        float corrected_g = s1;
+        float corrected_b = sclamp(s2 * (1.f - amount) + target_b * amount, 0.f, s2);
+        if (safe_surface > 1e-4f) {
+          const float luma_before = 0.2126f * s0 + 0.7152f * s1 + 0.0722f * s2;
+          const float luma_after = 0.2126f * corrected_r + 0.7152f * corrected_g + 0.0722f * corrected_b;
+          const float max_luma_drop = luma_before * 0.02f * (1.f - neutral_gray_surface);
+          const float min_luma = smax(0.f, luma_before - max_luma_drop);
+          if (luma_after < min_luma) {
+            const float lift = min_luma - luma_after;
+            const float channel_ceil = smax(s0, smax(s1, s2));
+            corrected_r = smin(s0, corrected_r + lift);
+            corrected_g = smin(channel_ceil, corrected_g + lift);
+            corrected_b = smin(s2, corrected_b + lift);
+          }
+          const float smx = smax(s0, smax(s1, s2));
+          const float smn = smin(s0, smin(s1, s2));
+          const float cmx = smax(corrected_r, smax(corrected_g, corrected_b));
+          const float cmn = smin(corrected_r, smin(corrected_g, corrected_b));
+          const float sch = smx - smn;
+          const float cch = cmx - cmn;
+          const float min_chroma = sch * (1.f - 0.12f * safe_surface);
+          if (sch > 1e-4f && cch < min_chroma) {
+            const float dn = smax(sch - cch, 1e-4f);
+            const float keep = sclamp((sch - min_chroma) / dn, 0.f, 1.f);
+            corrected_r = s0 * (1.f - keep) + corrected_r * keep;
+            corrected_g = s1 * (1.f - keep) + corrected_g * keep;
+            corrected_b = s2 * (1.f - keep) + corrected_b * keep;
+          }
+        }
+        d0 = corrected_r;
+        d1 = corrected_g;
+        d2 = corrected_b;
+      } else {
+        float target_g = s1;
+        const float rg_ref = e_rg;
+        const float bg_ref = e_bg;
+        if (rg_ref > 1e-4f && bg_ref > 1e-4f) {
+          const float g_from_r = smax(s0, 0.f) / rg_ref;
+          const float g_from_b = smax(s2, 0.f) / bg_ref;
+          target_g = 0.5f * (g_from_r + g_from_b);
+        }
+        const float rb_avg_target = 0.5f * (smax(s0, 0.f) + smax(s2, 0.f));
+        target_g = smax(target_g, rb_avg_target);
+        const float green_amount = sclamp(amount * green_strength_scale, 0.f, 1.f);
+        d0 = s0;
+        d1 = sclamp(s1 * (1.f - green_amount) + target_g * green_amount, 0.f, s1);
+        d2 = s2;
+      }
+    }
+  }
+
+  if (!skip_rest) {
+    const float solo_enable = ssmooth(1.25f, 3.0f, strength);
+    if (solo_enable > 0.f) {
+      const float g = smax(s1, 0.f);
+      const float target_r = g * exp_cr(blur_log_rg);
+      const float target_b = g * exp_cr(blur_log_bg);
+      const float solo_r = smax(0.f, s0 - target_r) / smax(blur_guide, 0.05f);
+      const float solo_b = smax(0.f, s2 - target_b) / smax(blur_guide, 0.05f);
+      const float local_solo_r =
+          ssmooth(chroma_threshold * 0.12f * inv_s, chroma_threshold * 0.65f * inv_s, solo_r);
+      const float local_solo_b =
+          ssmooth(chroma_threshold * 0.12f * inv_s, chroma_threshold * 0.65f * inv_s, solo_b);
+      const float rr0 = smax(s0, 0.f);
+      const float gg0 = g;
+      const float bb0 = smax(s2, 0.f);
+      const float g_over_min2 = smax(0.f, gg0 - smin(rr0, bb0)) / smax(blur_guide, 0.05f);
+      const float green_dom2 = ssmooth(0.010f, 0.060f, g_over_min2);
+      const float denom_solo = smax(blur_guide, 0.05f);
+      const float purpleish =
+          ssmooth(0.010f, 0.060f, smax(smax(0.f, rr0 - gg0), smax(0.f, bb0 - gg0)) / denom_solo);
+      const float solo_allow = 1.f - green_dom2 * (1.f - purpleish);
+      const float solo_r_mask = v.srb * local_solo_r * solo_allow;
+      const float solo_b_mask = v.sbb * local_solo_b * solo_allow;
+      if (solo_r_mask > mask_cutoff) {
+        const float amount = sclamp(solo_r_mask * strength * 0.85f, 0.f, 0.85f);
+        d0 = sclamp(d0 * (1.f - amount) + target_r * amount, 0.f, d0);
+      }
+      if (solo_b_mask > mask_cutoff) {
+        const float amount = sclamp(solo_b_mask * strength * 0.95f, 0.f, 0.90f);
+        d2 = sclamp(d2 * (1.f - amount) + target_b * amount, 0.f, d2);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void ld4(const float* p, float* o) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  o[0] = t.x;
+  o[1] = t.y;
+  o[2] = t.z;
+  o[3] = t.w;
+}
+__device__ __forceinline__ void st4(float* p, const float* o) {
+  *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+}
+
+// Four consecutive pixels per thread and step, read and written as float4
+// (src/dst 16-byte aligned; the planes are 256-byte aligned), so every load
+// of a step is issued before the first use; the one-pixel loop was bound by
+// load latency.  The keep-input test reads 4 planes; the other 7 are read
+// only when a pixel of the group needs them.  The group's operands are then
+// staged in shared memory (one column per thread) and one copy of the
+// per-pixel code runs over the four pixels.
+constexpr int DFM_THREADS = 128;
+constexpr int DFM_VALS = 14;  // s0 s1 s2 be ber srb sbb bg blrg blbg bfs lfs lrg lbg
+
+__global__ void __launch_bounds__(DFM_THREADS, 6) k_df_main(const float* src, float* dst, int W, int H, DfPlanes P,
+                                                           DfConst k, const DfScalars* sc) {
+  __shared__ float S[DFM_VALS * 4][DFM_THREADS];
+  DfMainK K;
   const float sensitivity = sclamp(sqrtf(smax(k.strength, 1.0f)), 1.0f, 2.5f);
-  const float inv_s = 1.0f / sensitivity;
-  const float mask_cutoff = 0.02f * inv_s;
+  K.inv_s = 1.0f / sensitivity;
+  K.mask_cutoff = 0.02f * K.inv_s;
   const float max_guide = df_max_guide(sc);
-  const float scene_highlight_gate = ssmooth(0.55f, 0.75f, max_guide);
-  const bool enable_green = k.green != 0;
-  const float edge_threshold = k.edge_thr, chroma_threshold = k.chroma_thr, strength = k.strength;
-  const float green_strength_scale = sclamp(k.green_scale, 0.f, 1.f);
-  // Pixels that provably keep their input: with green correction off, either
-  // edge factor at or below its lower smoothstep edge zeroes both edge
-  // weights (the other factor is finite, or NaN, and a NaN mask never passes
-  // the cutoff), so no ratio/direct correction applies; zero solo blurs make
-  // the solo masks zero.  The output is then the input whatever the other
-  // planes hold, so those pixels read 4 planes instead of 11 and skip the
-  // rest.
-  const float e0_edge = edge_threshold * 0.10f * inv_s;
-  const float e0_raw = 0.20f * inv_s;
-  const bool can_skip = !enable_green && edge_threshold > 0.f;  // smoothstep edges strictly ordered
-  size_t n = (size_t)W * H;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const float s0 = src[i * 3 + 0], s1 = src[i * 3 + 1], s2 = src[i * 3 + 2];
-    float d0 = s0, d1 = s1, d2 = s2;
-    if (can_skip && (P.be[i] <= e0_edge || P.ber[i] <= e0_raw) && P.srb[i] == 0.f && P.sbb[i] == 0.f) {
-      dst[i * 3 + 0] = d0;
-      dst[i * 3 + 1] = d1;
-      dst[i * 3 + 2] = d2;
+  K.scene_highlight_gate = ssmooth(0.55f, 0.75f, max_guide);
+  K.enable_green = k.green != 0;
+  K.edge_threshold = k.edge_thr;
+  K.chroma_threshold = k.chroma_thr;
+  K.strength = k.strength;
+  K.green_strength_scale = sclamp(k.green_scale, 0.f, 1.f);
+  K.e0_edge = K.edge_threshold * 0.10f * K.inv_s;
+  K.e0_raw = 0.20f * K.inv_s;
+  K.can_skip = !K.enable_green && K.edge_threshold > 0.f;  // smoothstep edges strictly ordered
+  const size_t n = (size_t)W * H;
+  const bool vec = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0;
+  const size_t n4 = vec ? n / 4 : 0;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const int tid = threadIdx.x;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + tid; q < n4; q += stride) {
+    const size_t i = q * 4;
+    float s[12], be[4], ber[4], srb[4], sbb[4];
+    ld4(src + i * 3, s);
+    ld4(src + i * 3 + 4, s + 4);
+    ld4(src + i * 3 + 8, s + 8);
+    ld4(P.be + i, be);
+    ld4(P.ber + i, ber);
+    ld4(P.srb + i, srb);
+    ld4(P.sbb + i, sbb);
+    unsigned keep = 0;
+#pragma unroll
+    for (int t = 0; t < 4; t++) keep |= df_keeps_input(K, be[t], ber[t], srb[t], sbb[t]) ? 1u << t : 0u;
+    if (keep == 0xFu) {
+      st4(dst + i * 3, s);
+      st4(dst + i * 3 + 4, s + 4);
+      st4(dst + i * 3 + 8, s + 8);
       continue;
     }
-    const float blur_guide = P.bg[i];
-    const float blur_log_rg = P.blrg[i];
-    const float blur_log_bg = P.blbg[i];
-    const float blur_fringe_support = P.bfs[i];
-    const float line_support = P.lfs[i];
-
-    const float rg = P.lrg[i];
-    const float bg = P.lbg[i];
-    const float dr = rg - blur_log_rg;
-    const float db = bg - blur_log_bg;
-    const float r0 = smax(s0, 0.f);
-    const float g0 = smax(s1, 0.f);
-    const float b0 = smax(s2, 0.f);
-    const float rb_avg_pre = 0.5f * (r0 + b0);
-    const float purple_r = smax(0.f, dr);
-    const float purple_b = smax(0.f, db);
-    const float green_r = smax(0.f, -dr);
-    const float green_b = smax(0.f, -db);
-    const float purple_excess = smin(purple_r, purple_b);
-    const float denom = smax(blur_guide, 0.05f);
-    const float g_over_min = smax(0.f, g0 - smin(r0, b0)) / denom;
-    const float green_dom = ssmooth(0.010f, 0.060f, g_over_min);
-    const float green_excess = smax(green_r, green_b) * green_dom;
-    const bool is_purple = purple_excess >= green_excess;
-    const float excess = is_purple ? purple_excess : green_excess;
-    const float min_dir = is_purple ? smax(0.f, smin(rg, bg)) : smax(0.f, smin(-rg, -bg));
-    const float max_dir = is_purple ? smax(1e-4f, smax(rg, bg)) : smax(1e-4f, smax(-rg, -bg));
-    const float balance = min_dir / max_dir;
-    const float c_edge_core = ssmooth(edge_threshold * 0.35f * inv_s, edge_threshold * 1.50f * inv_s, P.be[i]) *
-                              ssmooth(0.55f * inv_s, 1.35f * inv_s, P.ber[i]);
-    const float c_edge_low = ssmooth(edge_threshold * 0.10f * inv_s, edge_threshold * 0.80f * inv_s, P.be[i]) *
-                             ssmooth(0.20f * inv_s, 0.90f * inv_s, P.ber[i]);
-    const float linked_fringe = ssmooth(0.004f, 0.045f, smax(blur_fringe_support, line_support * 0.90f));
-    const float c_bright = ssmooth(0.24f * inv_s, 0.52f * inv_s, blur_guide);
-    const float c_chroma = ssmooth(chroma_threshold * 0.45f * inv_s, chroma_threshold * 1.60f * inv_s, excess);
-    const float red_blue_balance_hue = b0 / smax(r0, 1e-4f);
-    const float blue_lift_hue = smax(0.f, b0 - g0) / smax(r0 - g0, 1e-4f);
-    const float red_purple_hue_signal = ssmooth(0.50f, 0.72f, red_blue_balance_hue) * ssmooth(0.24f, 0.42f, blue_lift_hue);
-    const float balanced_hue = ssmooth(0.06f * inv_s, 0.22f * inv_s, min_dir) * ssmooth(0.35f, 0.75f, balance);
-    const float red_purple_hue_gate = is_purple ? smin(1.f, red_purple_hue_signal * 1.50f) *
-                                                      ssmooth(0.035f * inv_s, 0.16f * inv_s, min_dir) *
-                                                      ssmooth(0.18f, 0.58f, balance)
-                                                : 0.f;
-    const float green_unbalanced_hue =
-        (enable_green && !is_purple) ? ssmooth(0.035f * inv_s, 0.16f * inv_s, max_dir) : 0.f;
-    const float c_hue = smax(balanced_hue, smax(red_purple_hue_gate, green_unbalanced_hue));
-    const float rb_avg = rb_avg_pre;
-    const float purple_abs = smin(smax(0.f, r0 - g0), smax(0.f, b0 - g0)) / smax(blur_guide, 0.05f);
-    const float green_abs_base = smax(0.f, g0 - rb_avg) / smax(blur_guide, 0.05f);
-    const float green_abs_alt = smax(0.f, g0 - smin(r0, b0)) / smax(blur_guide, 0.05f);
-    const float green_abs = smax(green_abs_base, 0.55f * green_abs_alt);
-    const bool abs_is_purple = purple_abs >= green_abs;
-    const float abs_excess = abs_is_purple ? purple_abs : green_abs;
-    const float c_abs = ssmooth(chroma_threshold * 0.35f * inv_s, chroma_threshold * 1.20f * inv_s, abs_excess);
-    const float low_contrast_color =
-        ssmooth(chroma_threshold * 1.20f * inv_s, chroma_threshold * 2.40f * inv_s, abs_excess);
-    const float green_soft_edge_boost =
-        (enable_green && !is_purple) ? c_edge_low * ssmooth(0.05f * inv_s, 0.20f * inv_s, max_dir) : 0.f;
-    const float c_edge = smax(c_edge_core, smax(c_edge_low * linked_fringe * 1.45f,
-                                                smax(c_edge_low * low_contrast_color * 0.35f, green_soft_edge_boost)));
-    const float ratio_mask = c_edge * c_bright * c_hue * c_chroma;
-    const float direct_mask = c_edge * c_bright * c_hue * c_abs;
-    const bool use_direct = direct_mask > ratio_mask;
-    float mask = smax(ratio_mask, direct_mask) * scene_highlight_gate;
-    const bool correct_purple = use_direct ? abs_is_purple : is_purple;
-    float local_gate = 0.f;
-    if (correct_purple) {
-      local_gate = ssmooth(chroma_threshold * 0.10f * inv_s, chroma_threshold * 0.55f * inv_s, purple_abs);
-      mask *= local_gate;
-    } else {
-      local_gate = ssmooth(chroma_threshold * 0.10f * inv_s, chroma_threshold * 0.55f * inv_s, green_abs);
-      if (enable_green) {
-        const float peak_chroma_signal =
-            ssmooth(chroma_threshold * 0.80f * inv_s, chroma_threshold * 2.50f * inv_s, green_abs);
-        const float peak_neighbourhood = ssmooth(0.005f, 0.030f, blur_fringe_support);
-        const float green_peak_mask = peak_chroma_signal * peak_neighbourhood * c_bright * c_hue;
-        mask = smax(mask, green_peak_mask * scene_highlight_gate);
-      }
-      const float green_highlight_protect = 1.f - 0.85f * ssmooth(0.62f, 0.88f, blur_guide);
-      const float rb_to_green = rb_avg / smax(g0, 1e-4f);
-      const float natural_green_highlight = ssmooth(0.22f, 0.46f, rb_to_green) * ssmooth(0.30f, 0.55f, g0);
-      const float natural_green_suppress = 1.f - 0.99f * natural_green_highlight;
-      const float natural_green_suppress_sq = natural_green_suppress * natural_green_suppress;
-      const float green_halo_strength =
-          ssmooth(chroma_threshold * 0.55f * inv_s, chroma_threshold * 1.65f * inv_s, green_abs);
-      const float green_gain_base = enable_green ? 0.60f : 0.35f;
-      const float green_gain_slope = enable_green ? 1.10f : 0.95f;
-      const float green_gain = green_gain_base + green_gain_slope * green_halo_strength;
-      const float min_ratio_ref = smin(blur_log_rg, blur_log_bg);
-      const float green_neighbour = ssmooth(0.02f, 0.10f, smax(0.f, -min_ratio_ref));
-      const float src_max = smax(r0, smax(g0, b0));
-      const float src_min = smin(r0, smin(g0, b0));
-      const float src_chroma = src_max - src_min;
-      const float src_sat = src_chroma / smax(src_max, 1e-4f);
-      const float whiteish = 1.f - ssmooth(0.05f, 0.13f, src_sat);
-      const float foliage_guard =
-          green_neighbour * whiteish * ssmooth(0.35f, 0.75f, blur_guide) * (1.f - green_halo_strength);
-      const float strength_release = enable_green ? ssmooth(2.0f, 6.0f, strength) : 0.f;
-      const float green_line_evidence = ssmooth(0.004f, 0.030f, line_support) *
-                                        ssmooth(0.20f, 0.55f, green_halo_strength) * ssmooth(0.05f, 0.15f, src_sat);
-      const float not_natural_green = 1.f - natural_green_highlight;
-      const float guard_release = strength_release * green_line_evidence * not_natural_green;
-      const float released_highlight_protect = green_highlight_protect + (1.f - green_highlight_protect) * guard_release;
-      const float released_natural_suppress =
-          natural_green_suppress_sq + (1.f - natural_green_suppress_sq) * guard_release;
-      const float foliage_term = 1.f - 0.999f * foliage_guard;
-      const float released_foliage_term = foliage_term + (1.f - foliage_term) * guard_release;
-      mask *= local_gate * green_gain * released_highlight_protect * released_natural_suppress * released_foliage_term;
-      const float line_kill_evidence = ssmooth(0.04f, 0.15f, line_support);
-      const float natural_blob =
-          sqrtf(smax(0.f, natural_green_highlight)) * (1.f - line_kill_evidence) * green_neighbour;
-      mask *= 1.f - 0.999f * natural_blob;
-      if (!enable_green) mask = 0.f;
+    float pl[7][4];
+    ld4(P.bg + i, pl[0]);
+    ld4(P.blrg + i, pl[1]);
+    ld4(P.blbg + i, pl[2]);
+    ld4(P.bfs + i, pl[3]);
+    ld4(P.lfs + i, pl[4]);
+    ld4(P.lrg + i, pl[5]);
+    ld4(P.lbg + i, pl[6]);
+    // S[v * 4 + t][tid]: value v of pixel t
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      S[0 * 4 + t][tid] = s[3 * t];
+      S[1 * 4 + t][tid] = s[3 * t + 1];
+      S[2 * 4 + t][tid] = s[3 * t + 2];
+      S[3 * 4 + t][tid] = be[t];
+      S[4 * 4 + t][tid] = ber[t];
+      S[5 * 4 + t][tid] = srb[t];
+      S[6 * 4 + t][tid] = sbb[t];
+#pragma unroll
+      for (int v = 0; v < 7; v++) S[(7 + v) * 4 + t][tid] = pl[v][t];
     }
-
-    bool skip_rest = false;
-    if (mask > mask_cutoff) {
-      const float g = smax(s1, 0.f);
-      const float red_strength = smax(0.f, r0 - smax(g0, b0)) / smax(r0, 1e-4f);
-      const float red_blue_balance = b0 / smax(r0, 1e-4f);
-      const float blue_lift = smax(0.f, b0 - g0) / smax(r0 - g0, 1e-4f);
-      const float red_purple_balance = ssmooth(0.55f, 0.78f, red_blue_balance);
-      const float red_purple_lift = ssmooth(0.16f, 0.34f, blue_lift);
-      const float red_purple = smax(red_purple_balance, red_purple_lift);
-      const float red_strength_guard = ssmooth(0.08f, 0.25f, red_strength);
-      float red_purple_context = 0.f;
-      float contextual_red_purple = 0.f;
-      float red_magenta_surface = 0.f;
-      if (red_purple > 0.50f) {
-        red_purple_context = linked_fringe;
-        contextual_red_purple = red_purple * red_purple_context;
-        if (red_purple_context < 0.20f && red_strength_guard < 0.50f && red_purple > 0.50f) {
-          red_magenta_surface = ssmooth(0.02f, 0.12f, purple_abs) * (1.f - red_purple_context);
-        }
-      }
-      float neutral_gray_surface = 0.f;
-      if (strength > 3.f && red_purple_context > 0.80f && line_support > 0.012f && red_strength_guard < 0.98f &&
-          blue_lift > 1.10f && red_blue_balance > 0.82f && purple_abs > 0.015f) {
-        const float neutral_gray_edge = ssmooth(1.10f, 1.80f, blue_lift) * ssmooth(0.82f, 1.05f, red_blue_balance) *
-                                        (1.f - red_strength_guard);
-        neutral_gray_surface = neutral_gray_edge * ssmooth(0.015f, 0.08f, purple_abs) * ssmooth(3.f, 8.f, strength);
-      }
-      const float red_object_strength = smax(red_strength_guard, red_magenta_surface);
-      const float natural_warm_guard_base = 1.f - red_object_strength * (1.f - contextual_red_purple);
-      const float natural_warm_guard_sq =
-          natural_warm_guard_base * natural_warm_guard_base * natural_warm_guard_base * natural_warm_guard_base;
-      const float natural_warm_guard = natural_warm_guard_sq * natural_warm_guard_sq;
-      const float line_purple_relief = ssmooth(0.012f, 0.06f, line_support) * ssmooth(0.10f, 0.24f, blue_lift);
-      const float red_object_guard = ssmooth(0.55f, 0.90f, red_object_strength);
-      const float linked_override = linked_fringe * 1.05f * (1.f - 0.85f * red_object_guard);
-      const float line_override = line_purple_relief * (1.f - 0.85f * red_object_guard);
-      const bool force_warm_guard = (red_object_guard > 0.75f) && (linked_fringe < 0.65f) && (line_purple_relief < 0.45f);
-      const float warm_protect = correct_purple
-                                     ? (force_warm_guard ? natural_warm_guard
-                                                         : smax(natural_warm_guard, smax(linked_override, line_override)))
-                                     : 1.f;
-      const float red_without_support =
-          ssmooth(0.22f, 0.45f, red_strength) * (1.f - ssmooth(0.02f, 0.12f, blur_fringe_support));
-      const float protect = correct_purple ? red_without_support : 0.f;
-      const float smooth_mask = ssmooth(mask_cutoff, mask_cutoff * 5.0f, mask);
-      const float threshold_soften = 1.f - 0.86f * ssmooth(0.22f, 0.40f, chroma_threshold);
-      const float src_max = smax(r0, smax(g0, b0));
-      const float src_min = smin(r0, smin(g0, b0));
-      const float src_chroma = src_max - src_min;
-      const float src_sat = src_chroma / smax(src_max, 1e-4f);
-      const float neutral_guard_base = ssmooth(0.008f, 0.030f, src_sat);
-      const float neutral_guard = 1.f - (1.f - neutral_guard_base) * ssmooth(0.35f, 0.80f, red_object_strength);
-      float amount = sclamp(smooth_mask * strength * 1.90f * (1.f - protect) * warm_protect * neutral_guard *
-                                threshold_soften,
-                            0.f, 1.f);
-      const float warm_edge_surface = ssmooth(0.006f, 0.035f, purple_abs) * ssmooth(0.25f, 0.65f, red_purple) *
-                                      ssmooth(0.15f, 0.65f, red_purple_context) * (1.f - 0.55f * red_strength_guard) *
-                                      ssmooth(3.f, 8.f, strength);
-      const float safe_surface = smax(neutral_gray_surface, warm_edge_surface);
-      if (correct_purple && safe_surface > 1e-4f) {
-        const float safe_amount_cap = 1.f - 0.99f * safe_surface;
-        amount = smin(amount, safe_amount_cap);
-      }
-      if (amount <= 1e-4f) {
-        skip_rest = true;
-      } else {
-        const float e_rg = exp_cr(blur_log_rg);
-        const float e_bg = exp_cr(blur_log_bg);
-        const float target_r = smin(g, g * e_rg);
-        const float target_b = smin(g, g * e_bg);
-        if (correct_purple) {
-          float corrected_r = sclamp(s0 * (1.f - amount) + target_r * amount, 0.f, s0);
-          float corrected_g = s1;
-          float corrected_b = sclamp(s2 * (1.f - amount) + target_b * amount, 0.f, s2);
-          if (safe_surface > 1e-4f) {
-            const float luma_before = 0.2126f * s0 + 0.7152f * s1 + 0.0722f * s2;
-            const float luma_after = 0.2126f * corrected_r + 0.7152f * corrected_g + 0.0722f * corrected_b;
-            const float max_luma_drop = luma_before * 0.02f * (1.f - neutral_gray_surface);
-            const float min_luma = smax(0.f, luma_before - max_luma_drop);
-            if (luma_after < min_luma) {
-              const float lift = min_luma - luma_after;
-              const float channel_ceil = smax(s0, smax(s1, s2));
-              corrected_r = smin(s0, corrected_r + lift);
-              corrected_g = smin(channel_ceil, corrected_g + lift);
-              corrected_b = smin(s2, corrected_b + lift);
-            }
-            const float smx = smax(s0, smax(s1, s2));
-            const float smn = smin(s0, smin(s1, s2));
-            const float cmx = smax(corrected_r, smax(corrected_g, corrected_b));
-            const float cmn = smin(corrected_r, smin(corrected_g, corrected_b));
-            const float sch = smx - smn;
-            const float cch = cmx - cmn;
-            const float min_chroma = sch * (1.f - 0.12f * safe_surface);
-            if (sch > 1e-4f && cch < min_chroma) {
-              const float dn = smax(sch - cch, 1e-4f);
-              const float keep = sclamp((sch - min_chroma) / dn, 0.f, 1.f);
-              corrected_r = s0 * (1.f - keep) + corrected_r * keep;
-              corrected_g = s1 * (1.f - keep) + corrected_g * keep;
-              corrected_b = s2 * (1.f - keep) + corrected_b * keep;
-            }
-          }
-          d0 = corrected_r;
-          d1 = corrected_g;
-          d2 = corrected_b;
-        } else {
-          float target_g = s1;
-          const float rg_ref = e_rg;
-          const float bg_ref = e_bg;
-          if (rg_ref > 1e-4f && bg_ref > 1e-4f) {
-            const float g_from_r = smax(s0, 0.f) / rg_ref;
-            const float g_from_b = smax(s2, 0.f) / bg_ref;
-            target_g = 0.5f * (g_from_r + g_from_b);
-          }
-          const float rb_avg_target = 0.5f * (smax(s0, 0.f) + smax(s2, 0.f));
-          target_g = smax(target_g, rb_avg_target);
-          const float green_amount = sclamp(amount * green_strength_scale, 0.f, 1.f);
-          d0 = s0;
-          d1 = sclamp(s1 * (1.f - green_amount) + target_g * green_amount, 0.f, s1);
-          d2 = s2;
-        }
-      }
+#pragma unroll 1
+    for (int t = 0; t < 4; t++) {
+      if (keep >> t & 1u) continue;
+      const DfPx v{S[3 * 4 + t][tid],  S[4 * 4 + t][tid],  S[5 * 4 + t][tid],  S[6 * 4 + t][tid],
+                   S[7 * 4 + t][tid],  S[8 * 4 + t][tid],  S[9 * 4 + t][tid],  S[10 * 4 + t][tid],
+                   S[11 * 4 + t][tid], S[12 * 4 + t][tid], S[13 * 4 + t][tid]};
+      float r0, r1, r2;
+      df_main_px(S[0 * 4 + t][tid], S[1 * 4 + t][tid], S[2 * 4 + t][tid], v, K, r0, r1, r2);
+      S[0 * 4 + t][tid] = r0;
+      S[1 * 4 + t][tid] = r1;
+      S[2 * 4 + t][tid] = r2;
     }
-
-    if (!skip_rest) {
-      const float solo_enable = ssmooth(1.25f, 3.0f, strength);
-      if (solo_enable > 0.f) {
-        const float g = smax(s1, 0.f);
-        const float target_r = g * exp_cr(blur_log_rg);
-        const float target_b = g * exp_cr(blur_log_bg);
-        const float solo_r = smax(0.f, s0 - target_r) / smax(blur_guide, 0.05f);
-        const float solo_b = smax(0.f, s2 - target_b) / smax(blur_guide, 0.05f);
-        const float local_solo_r =
-            ssmooth(chroma_threshold * 0.12f * inv_s, chroma_threshold * 0.65f * inv_s, solo_r);
-        const float local_solo_b =
-            ssmooth(chroma_threshold * 0.12f * inv_s, chroma_threshold * 0.65f * inv_s, solo_b);
-        const float rr0 = smax(s0, 0.f);
-        const float gg0 = g;
-        const float bb0 = smax(s2, 0.f);
-        const float g_over_min2 = smax(0.f, gg0 - smin(rr0, bb0)) / smax(blur_guide, 0.05f);
-        const float green_dom2 = ssmooth(0.010f, 0.060f, g_over_min2);
-        const float denom_solo = smax(blur_guide, 0.05f);
-        const float purpleish =
-            ssmooth(0.010f, 0.060f, smax(smax(0.f, rr0 - gg0), smax(0.f, bb0 - gg0)) / denom_solo);
-        const float solo_allow = 1.f - green_dom2 * (1.f - purpleish);
-        const float solo_r_mask = P.srb[i] * local_solo_r * solo_allow;
-        const float solo_b_mask = P.sbb[i] * local_solo_b * solo_allow;
-        if (solo_r_mask > mask_cutoff) {
-          const float amount = sclamp(solo_r_mask * strength * 0.85f, 0.f, 0.85f);
-          d0 = sclamp(d0 * (1.f - amount) + target_r * amount, 0.f, d0);
-        }
-        if (solo_b_mask > mask_cutoff) {
-          const float amount = sclamp(solo_b_mask * strength * 0.95f, 0.f, 0.90f);
-          d2 = sclamp(d2 * (1.f - amount) + target_b * amount, 0.f, d2);
-        }
-      }
+    float d[12];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      d[3 * t] = S[0 * 4 + t][tid];
+      d[3 * t + 1] = S[1 * 4 + t][tid];
+      d[3 * t + 2] = S[2 * 4 + t][tid];
+    }
+    st4(dst + i * 3, d);
+    st4(dst + i * 3 + 4, d + 4);
+    st4(dst + i * 3 + 8, d + 8);
+  }
+  for (size_t i = n4 * 4 + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    const float s0 = src[i * 3 + 0], s1 = src[i * 3 + 1], s2 = src[i * 3 + 2];
+    float d0 = s0, d1 = s1, d2 = s2;
+    if (!df_keeps_input(K, P.be[i], P.ber[i], P.srb[i], P.sbb[i])) {
+      const DfPx v{P.be[i], P.ber[i], P.srb[i], P.sbb[i], P.bg[i],  P.blrg[i],
+                   P.blbg[i], P.bfs[i], P.lfs[i], P.lrg[i], P.lbg[i]};
+      df_main_px(s0, s1, s2, v, K, d0, d1, d2);
     }
     dst[i * 3 + 0] = d0;
     dst[i * 3 + 1] = d1;
@@ -929,7 +1051,8 @@ lre_status launch_defringe(Context* c, const float* in, float* out, size_t w, si
   j3.in[1] = P.sbs; j3.mode[1] = BS_PLANE; j3.out[1] = P.sbb;
   LRE_TRY(run_blur(c, j3, taps, W, H, sc));
 
-  k_df_main<<<gstream, 256, 0, c->stream>>>(in, out, W, H, P, k, sc);
+  k_df_main<<<grid_for((n + 3) / 4, DFM_THREADS, c->sm_count * 6), DFM_THREADS, 0, c->stream>>>(in, out, W, H, P, k,
+                                                                                                sc);
   count_launch(c);
   return check_launch(c, "defringe main");
 }
