@@ -445,6 +445,47 @@ __device__ __forceinline__ void strip_update(double (*Vs)[vs_len<WS>()], int VC,
   }
 }
 
+// One row step of a strip's vertical window sums (the row entering and the
+// row leaving the window), fetched as raw samples one step ahead of its use.
+// The fetch is issued after the step's last __syncwarp, so the loads stay in
+// flight while the warp writes the current row's outputs.  The per-sample
+// doubles and the order of the additions are those of strip_update.
+template <int NQ, int NR, int WS>
+struct StripStep {
+  static constexpr int SL = WS / 32 + 1;  // window columns per lane: WS + 2r <= WS + 32
+  float add[SL][NR], sub[SL][NR];
+  template <typename Fetch>
+  __device__ __forceinline__ void fetch(int VC, int xv0, int y_add, int y_sub, Fetch f) {
+#pragma unroll
+    for (int s = 0; s < SL; s++) {
+      const int j = threadIdx.x + 32 * s;
+      if (j < VC) {
+        f(xv0 + j, y_add, add[s]);
+        f(xv0 + j, y_sub, sub[s]);
+      }
+    }
+  }
+  template <typename Conv>
+  __device__ __forceinline__ void apply(double (*Vs)[vs_len<WS>()], int VC, Conv cv) const {
+#pragma unroll
+    for (int s = 0; s < SL; s++) {
+      const int j = threadIdx.x + 32 * s;
+      if (j < VC) {
+        double qa[NQ], qs[NQ];
+        cv(add[s], qa);
+        cv(sub[s], qs);
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+          double v = Vs[q][vidx(j)];
+          v += qa[q];
+          v -= qs[q];
+          Vs[q][vidx(j)] = v;
+        }
+      }
+    }
+  }
+};
+
 // Horizontal window sums of the lane's 4 output columns: hs[q][k].
 template <int NQ, int WS>
 __device__ __forceinline__ void strip_hsum(double (*Vs)[vs_len<WS>()], int r, double hs[NQ][WS / 32]) {
@@ -465,7 +506,7 @@ __device__ __forceinline__ void strip_hsum(double (*Vs)[vs_len<WS>()], int r, do
 }
 
 template <int WS>
-__global__ void __launch_bounds__(32) k_ax_ab(const float* __restrict__ src, int W, int H, int r, float eps, int HS,
+__global__ void __launch_bounds__(32, WS == 128 ? 16 : 20) k_ax_ab(const float* __restrict__ src, int W, int H, int r, float eps, int HS,
                                              const float* __restrict__ d_maxg, float* __restrict__ aR,
                                              float* __restrict__ bR, float* __restrict__ aB, float* __restrict__ bB,
                                              float* __restrict__ er, int yb0) {
@@ -489,12 +530,34 @@ __global__ void __launch_bounds__(32) k_ax_ab(const float* __restrict__ src, int
     const int x = x0 + threadIdx.x * PL + k;
     inv_cx[k] = x < W ? 1.0 / (double)win_count(x, r, W) : 0.0;
   }
+  // raw (r, g, b) of the sample, zeros outside the image; cv forms the six
+  // doubles exactly as AbQ::load does
+  auto fetch = [&](int x, int y, float* v) {
+    v[0] = v[1] = v[2] = 0.f;
+    if (x >= 0 && x < W && y >= 0 && y < H) {
+      const float* p = src + ((size_t)y * W + x) * 3;
+      v[0] = p[0];
+      v[1] = p[1];
+      v[2] = p[2];
+    }
+  };
+  auto cv = [&](const float* v, double* q) {
+    const float rr = v[0] * inv_norm, g = v[1] * inv_norm, b = v[2] * inv_norm;
+    q[0] = (double)g;
+    q[1] = (double)(g * g);
+    q[2] = (double)rr;
+    q[3] = (double)(g * rr);
+    q[4] = (double)b;
+    q[5] = (double)(g * b);
+  };
+  StripStep<NQ, 3, WS> step;
   for (int y = y0; y < y_end; y++) {
-    if (y > y0) strip_update<NQ, WS>(Vs, VC, xv0, y + r, y - r - 1, ld);
+    if (y > y0) step.apply(Vs, VC, cv);
     __syncwarp();
     double hs[NQ][PL];
     strip_hsum<NQ, WS>(Vs, r, hs);
     __syncwarp();  // the next update rewrites Vs
+    if (y + 1 < y_end) step.fetch(VC, xv0, y + 1 + r, y - r, fetch);
     const double inv_cy = 1.0 / (double)win_count(y, r, H);
 #pragma unroll
     for (int k = 0; k < PL; k++) {
@@ -526,7 +589,7 @@ __global__ void __launch_bounds__(32) k_ax_ab(const float* __restrict__ src, int
 }
 
 template <int WS>
-__global__ void __launch_bounds__(32) k_ax_q(const float* __restrict__ src, float* __restrict__ dst, int W, int H,
+__global__ void __launch_bounds__(32, WS == 128 ? 16 : 20) k_ax_q(const float* __restrict__ src, float* __restrict__ dst, int W, int H,
                                             int r, float strength, int HS, const float* __restrict__ d_maxg,
                                             const float* __restrict__ aR, const float* __restrict__ bR,
                                             const float* __restrict__ aB, const float* __restrict__ bB,
@@ -566,12 +629,29 @@ __global__ void __launch_bounds__(32) k_ax_q(const float* __restrict__ src, floa
     const int x = x0 + threadIdx.x * PL + k;
     inv_cx[k] = x < W ? 1.0 / (double)win_count(x, r, W) : 0.0;
   }
+  auto fetch = [&](int x, int y, float* v) {
+    v[0] = v[1] = v[2] = v[3] = v[4] = 0.f;
+    if (x >= 0 && x < W && y >= 0 && y < H) {
+      const size_t i = (size_t)y * W + x;
+      v[0] = aR[i];
+      v[1] = bR[i];
+      v[2] = aB[i];
+      v[3] = bB[i];
+      v[4] = er[i];
+    }
+  };
+  auto cv = [](const float* v, double* q) {
+#pragma unroll
+    for (int t = 0; t < 5; t++) q[t] = (double)v[t];
+  };
+  StripStep<NQ, 5, WS> step;
   for (int y = y0; y < y_end; y++) {
-    if (y > y0) strip_update<NQ, WS>(Vs, VC, xv0, y + r, y - r - 1, ld);
+    if (y > y0) step.apply(Vs, VC, cv);
     __syncwarp();
     double hs[NQ][PL];
     strip_hsum<NQ, WS>(Vs, r, hs);
     __syncwarp();
+    if (y + 1 < y_end) step.fetch(VC, xv0, y + 1 + r, y - r, fetch);
     const double inv_cy = 1.0 / (double)win_count(y, r, H);
 #pragma unroll
     for (int k = 0; k < PL; k++) {
