@@ -43,8 +43,8 @@ METRIC = "develop MP/s on 1 B200 (51 MP Bayer: AMaZE->defringe->axial CA->tone m
 STAGE_BYTES = {"amaze": 16.0, "defringe": 24.0, "axial": 24.0, "tone": 24.0}
 # From one ncu capture of k_amaze at 4096x3072 (profiles/develop_12mp_full.md):
 # DRAM read+write bytes and executed warp-instructions per output pixel.
-AMAZE_DRAM_BYTES_PER_PX = (109.713152e6 + 900.116224e6) / (4096 * 3072)
-AMAZE_WARP_INST_PER_PX = 883750708 / (4096 * 3072)
+AMAZE_DRAM_BYTES_PER_PX = (124.060416e6 + 909.380352e6) / (4096 * 3072)
+AMAZE_WARP_INST_PER_PX = 925190063 / (4096 * 3072)
 # issue roofline: 148 SMs x 4 schedulers x 1.965 GHz, one warp-instruction per cycle each
 ISSUE_PEAK_G = 148 * 4 * 1.965
 

@@ -43,7 +43,7 @@ constexpr int TS = 160;
 constexpr int TSH = TS / 2;
 constexpr int TS2 = TS * TS;
 constexpr int HALF = TS * TSH;
-constexpr int AMZ_THREADS = 640;
+constexpr int AMZ_THREADS = 1024;
 
 constexpr float eps = 1e-5f;
 constexpr float epssq = 1e-10f;
