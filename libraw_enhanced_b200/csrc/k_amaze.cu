@@ -123,6 +123,7 @@ struct AmazeArgs {
   int tile_lo, tile_hi;  // tiles [tile_lo, tile_hi) of the n_top x n_left grid
   unsigned char* scratch;
   int* tile_counter;
+  float* max_g;  // nullable: max(0, G) of the interior outputs (the 4-px frame is left to the border pass)
 };
 
 // (a packed lookup: indexing the parameter's array at run time would copy the
@@ -209,6 +210,7 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
   const Slab S = make_slab(A.scratch + (size_t)blockIdx.x * kSlabBytes, cfa);
   __shared__ int s_tile;
   __shared__ int s_doNyq;
+  float mg = 0.f;  // max G of this thread's interior outputs
 
   for (;;) {
     if (tid == 0) s_tile = atomicAdd(A.tile_counter, 1);
@@ -850,15 +852,22 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
       __stcs(o + 0, fmaxf(0.f, r));
       __stcs(o + 1, fmaxf(0.f, g));
       __stcs(o + 2, fmaxf(0.f, b));
+      if (row >= 4 && row < H - 4 && col >= 4 && col < W - 4) mg = fmaxf(mg, fmaxf(0.f, g));
     }
     __syncthreads();
+  }
+  // every thread leaves the tile loop together (s_tile is shared)
+  if (A.max_g) {
+    mg = warp_max(mg);
+    if ((tid & 31) == 0) atomic_max_float(A.max_g, mg);
   }
 }
 
 // LibRaw-style border interpolation (core/cpu_accelerator.cpp:2984-3028):
 // only pixels within `border` of the frame; non-native channels become the
 // mean of that colour's samples in the clipped 3x3 neighbourhood.
-__global__ void k_border_interp(float* rgb, int W, int H, uint32_t filters, int border) {
+__global__ void k_border_interp(float* rgb, int W, int H, uint32_t filters, int border, float* max_g) {
+  float mg = 0.f;  // max of the final G of this thread's border pixels
   // enumerate only border pixels: top/bottom bands then left/right bands
   const int band = border;
   const long long n_tb = 2LL * band * W;
@@ -888,6 +897,16 @@ __global__ void k_border_interp(float* rgb, int W, int H, uint32_t filters, int 
     const unsigned f = fcol3((unsigned)row, (unsigned)col, filters);
     for (unsigned c = 0; c < 3; c++)
       if (c != f && sum[c + 4] > 0) rgb[((size_t)row * W + col) * 3 + c] = sum[c] / sum[c + 4];
+    if (max_g) {
+      // G as this pass leaves it: a G site keeps its own sample, an R/B site
+      // takes the neighbours' mean when it has G neighbours
+      const float gv = (f != 1 && sum[5] > 0) ? sum[1] / sum[5] : rgb[((size_t)row * W + col) * 3 + 1];
+      mg = fmaxf(mg, fmaxf(0.f, gv));
+    }
+  }
+  if (max_g) {
+    mg = warp_max(mg);
+    if ((threadIdx.x & 31) == 0) atomic_max_float(max_g, mg);
   }
 }
 
@@ -936,6 +955,7 @@ AmazeArgs amaze_args(const float* raw, int cstride, float* rgb, size_t w, size_t
   A.tile_hi = A.n_top * A.n_left;
   A.scratch = nullptr;
   A.tile_counter = nullptr;
+  A.max_g = nullptr;
   return A;
 }
 
@@ -962,16 +982,20 @@ lre_status launch_amaze_rows(Context* c, AmazeArgs A, int row_lo, int row_hi) {
 }  // namespace
 
 lre_status launch_amaze(Context* c, const float* raw, int cstride, float* rgb, size_t w, size_t h, uint32_t filters,
-                        const float cam_mul[4], float maximum_value) {
-  const AmazeArgs A = amaze_args(raw, cstride, rgb, w, h, filters, cam_mul, maximum_value);
+                        const float cam_mul[4], float maximum_value, float* max_g) {
+  AmazeArgs A = amaze_args(raw, cstride, rgb, w, h, filters, cam_mul, maximum_value);
+  A.max_g = max_g;
+  if (max_g) LRE_CUDA_TRY(c, cudaMemsetAsync(max_g, 0, sizeof(float), c->stream));
   LRE_TRY(launch_amaze_rows(c, A, 0, A.n_top));
-  return launch_border_interp(c, rgb, w, h, filters, 4);
+  return launch_border_interp(c, rgb, w, h, filters, 4, max_g);
 }
 
 lre_status launch_amaze_from_host(Context* c, const float* h_mosaic, float* d_mosaic, float* rgb, size_t w,
                                   size_t h, uint32_t filters, const float cam_mul[4], float maximum_value,
-                                  cudaStream_t copy_stream, cudaEvent_t* events, int n_events) {
-  const AmazeArgs A = amaze_args(d_mosaic, 1, rgb, w, h, filters, cam_mul, maximum_value);
+                                  cudaStream_t copy_stream, cudaEvent_t* events, int n_events, float* max_g) {
+  AmazeArgs A = amaze_args(d_mosaic, 1, rgb, w, h, filters, cam_mul, maximum_value);
+  A.max_g = max_g;
+  if (max_g) LRE_CUDA_TRY(c, cudaMemsetAsync(max_g, 0, sizeof(float), c->stream));
   const int bands = std::max(1, std::min(n_events, A.n_top / 4));
   size_t copied = 0;  // mosaic rows already queued for upload
   for (int b = 0; b < bands; b++) {
@@ -993,12 +1017,13 @@ lre_status launch_amaze_from_host(Context* c, const float* h_mosaic, float* d_mo
     LRE_CUDA_TRY(c, cudaEventRecord(events[bands - 1], copy_stream));
     LRE_CUDA_TRY(c, cudaStreamWaitEvent(c->stream, events[bands - 1], 0));
   }
-  return launch_border_interp(c, rgb, w, h, filters, 4);
+  return launch_border_interp(c, rgb, w, h, filters, 4, max_g);
 }
 
-lre_status launch_border_interp(Context* c, float* rgb, size_t w, size_t h, uint32_t filters, int band) {
+lre_status launch_border_interp(Context* c, float* rgb, size_t w, size_t h, uint32_t filters, int band, float* max_g) {
   const long long nb = 2LL * band * (long long)w + 2LL * band * (long long)(h > (size_t)(2 * band) ? h - 2 * band : 0);
-  k_border_interp<<<grid_for((size_t)nb, 256, c->sm_count * 2), 256, 0, c->stream>>>(rgb, (int)w, (int)h, filters, band);
+  k_border_interp<<<grid_for((size_t)nb, 256, c->sm_count * 2), 256, 0, c->stream>>>(rgb, (int)w, (int)h, filters, band,
+                                                                                     max_g);
   count_launch(c);
   return check_launch(c, "border_interpolate");
 }

@@ -855,7 +855,7 @@ constexpr int DFM_THREADS = 128;
 constexpr int DFM_VALS = 14;  // s0 s1 s2 be ber srb sbb bg blrg blbg bfs lfs lrg lbg
 
 __global__ void __launch_bounds__(DFM_THREADS, 6) k_df_main(const float* src, float* dst, int W, int H, DfPlanes P,
-                                                           DfConst k, const DfScalars* sc) {
+                                                           DfConst k, const DfScalars* sc, float* out_max_g) {
   __shared__ float S[DFM_VALS * 4][DFM_THREADS];
   DfMainK K;
   const float sensitivity = sclamp(sqrtf(smax(k.strength, 1.0f)), 1.0f, 2.5f);
@@ -876,6 +876,7 @@ __global__ void __launch_bounds__(DFM_THREADS, 6) k_df_main(const float* src, fl
   const size_t n4 = vec ? n / 4 : 0;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   const int tid = threadIdx.x;
+  float mg = 0.f;  // max(0, G) of what this thread writes (fmaxf drops NaN)
   for (size_t q = blockIdx.x * (size_t)blockDim.x + tid; q < n4; q += stride) {
     const size_t i = q * 4;
     float s[12], be[4], ber[4], srb[4], sbb[4];
@@ -893,6 +894,7 @@ __global__ void __launch_bounds__(DFM_THREADS, 6) k_df_main(const float* src, fl
       st4(dst + i * 3, s);
       st4(dst + i * 3 + 4, s + 4);
       st4(dst + i * 3 + 8, s + 8);
+      mg = fmaxf(mg, fmaxf(fmaxf(s[1], s[4]), fmaxf(s[7], s[10])));
       continue;
     }
     float pl[7][4];
@@ -938,6 +940,7 @@ __global__ void __launch_bounds__(DFM_THREADS, 6) k_df_main(const float* src, fl
     st4(dst + i * 3, d);
     st4(dst + i * 3 + 4, d + 4);
     st4(dst + i * 3 + 8, d + 8);
+    mg = fmaxf(mg, fmaxf(fmaxf(d[1], d[4]), fmaxf(d[7], d[10])));
   }
   for (size_t i = n4 * 4 + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += stride) {
     const float s0 = src[i * 3 + 0], s1 = src[i * 3 + 1], s2 = src[i * 3 + 2];
@@ -950,12 +953,18 @@ __global__ void __launch_bounds__(DFM_THREADS, 6) k_df_main(const float* src, fl
     dst[i * 3 + 0] = d0;
     dst[i * 3 + 1] = d1;
     dst[i * 3 + 2] = d2;
+    mg = fmaxf(mg, d1);
+  }
+  if (out_max_g) {  // every thread of the block gets here
+    mg = warp_max(mg);
+    if ((tid & 31) == 0) atomic_max_float(out_max_g, mg);
   }
 }
 
-__global__ void k_df_init(DfScalars* sc) {
-  sc->max_guide_raw = 0.f;
+__global__ void k_df_init(DfScalars* sc, const float* in_max_g, float* out_max_g) {
+  sc->max_guide_raw = in_max_g ? *in_max_g : 0.f;
   sc->max_edge = 0.f;
+  if (out_max_g) *out_max_g = 0.f;
 }
 
 __global__ void k_df_maxg(const float* __restrict__ src, size_t n, DfScalars* sc) {
@@ -987,8 +996,7 @@ size_t ws_bytes_defringe(size_t w, size_t h, float radius) {
 
 lre_status launch_defringe(Context* c, const float* in, float* out, size_t w, size_t h, float radius,
                            float edge_thr, float chroma_thr, float strength, bool green, float green_scale,
-                           const float* d_max_g) {
-  (void)d_max_g;
+                           const float* in_max_g, float* out_max_g) {
   GaussTaps taps = make_defringe_taps(radius);
   {
     const float sigma = std::max(radius / 3.f, 0.5f);
@@ -1010,12 +1018,16 @@ lre_status launch_defringe(Context* c, const float* in, float* out, size_t w, si
   const size_t n = w * h;
   const unsigned gstream = grid_for(n, 256, c->sm_count * 8);
 
-  k_df_init<<<1, 1, 0, c->stream>>>(sc);
-  k_df_maxg<<<grid_for(n, 256, c->sm_count * 4), 256, 0, c->stream>>>(in, n, sc);
+  k_df_init<<<1, 1, 0, c->stream>>>(sc, in_max_g, out_max_g);
+  count_launch(c);
+  if (!in_max_g) {
+    k_df_maxg<<<grid_for(n, 256, c->sm_count * 4), 256, 0, c->stream>>>(in, n, sc);
+    count_launch(c);
+  }
   const size_t prep_tiles = (size_t)((W + PT_X - 1) / PT_X) * ((H + PT_Y - 1) / PT_Y);
   k_df_prep_tiled<<<(unsigned)std::min<size_t>(prep_tiles, (size_t)c->sm_count * 8), 256, 0, c->stream>>>(
       in, W, H, sc, P.lrg, P.lbg, P.er);
-  count_launch(c, 3);
+  count_launch(c);
   LRE_TRY(check_launch(c, "defringe prep"));
 
   BlurJob j1{};
@@ -1052,7 +1064,7 @@ lre_status launch_defringe(Context* c, const float* in, float* out, size_t w, si
   LRE_TRY(run_blur(c, j3, taps, W, H, sc));
 
   k_df_main<<<grid_for((n + 3) / 4, DFM_THREADS, c->sm_count * 6), DFM_THREADS, 0, c->stream>>>(in, out, W, H, P, k,
-                                                                                                sc);
+                                                                                                sc, out_max_g);
   count_launch(c);
   return check_launch(c, "defringe main");
 }

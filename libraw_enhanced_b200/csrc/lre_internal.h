@@ -135,23 +135,30 @@ lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, si
 lre_status launch_axial_ca_banded(Context* c, const float* in, float* out, size_t w, size_t h, int radius, float eps,
                                   float strength, const float* d_max_g, int bands,
                                   const std::function<lre_status(size_t, size_t)>& rows_done);
+// in_max_g (nullable): max(0, max G) of `in`, already reduced on the device
+// by the stage that wrote it (the defringe then skips its own reduction).
+// out_max_g (nullable): receives max(0, max G) of `out`, reduced in the
+// main pass for the stage that follows.
 lre_status launch_defringe(Context* c, const float* in, float* out, size_t w, size_t h, float radius,
                            float edge_thr, float chroma_thr, float strength, bool green,
-                           float green_scale, const float* d_max_g);
+                           float green_scale, const float* in_max_g = nullptr, float* out_max_g = nullptr);
 lre_status launch_detail_tonemap(Context* c, const float* in, float* out, size_t w, size_t h);
 lre_status launch_micro_contrast(Context* c, const float* in, float* out, size_t w, size_t h,
                                  float threshold, float strength, float target, const float* mask);
 lre_status launch_lateral_ca(Context* c, const float* in, float* out, size_t w, size_t h, int cell,
                              int iters, float max_shift, float min_conf, int levels);
+// max_g (nullable): receives max(0, max G) of the finished RGB (AMaZE's
+// interior outputs and the interpolated border), reduced in the kernels.
 lre_status launch_amaze(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
-                        uint32_t filters, const float cam_mul[4], float maximum_value);
+                        uint32_t filters, const float cam_mul[4], float maximum_value, float* max_g = nullptr);
 // AMaZE on a mosaic still in host memory: the upload runs in row chunks on
 // copy_stream and each band of tile rows starts as soon as the rows it reads
 // have arrived (results identical to launch_amaze).  d_mosaic receives the
 // whole mosaic.
 lre_status launch_amaze_from_host(Context* c, const float* h_mosaic, float* d_mosaic, float* rgb, size_t w,
                                   size_t h, uint32_t filters, const float cam_mul[4], float maximum_value,
-                                  cudaStream_t copy_stream, cudaEvent_t* events, int n_events);
+                                  cudaStream_t copy_stream, cudaEvent_t* events, int n_events,
+                                  float* max_g = nullptr);
 lre_status launch_xtrans(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w,
                          size_t h, const char* xtrans, float maximum_value, int passes);
 
@@ -199,7 +206,9 @@ lre_status launch_output_epilogue(Context* c, const float* in, void* out, size_t
 namespace lre {
 // LibRaw border interpolation of the `band`-px frame (k_amaze.cu) and the
 // bilinear Bayer demosaic (k_linear.cu).
-lre_status launch_border_interp(Context* c, float* rgb, size_t w, size_t h, uint32_t filters, int band);
+// max_g (nullable): the max of the border pixels' final G is folded into it.
+lre_status launch_border_interp(Context* c, float* rgb, size_t w, size_t h, uint32_t filters, int band,
+                                float* max_g = nullptr);
 lre_status launch_bayer_linear(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
                                uint32_t filters, float maximum_value);
 // DCB and AAHD Bayer demosaics (k_dcb.cu, k_aahd.cu).  Their in-order

@@ -112,6 +112,14 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
   if (h_mosaic && route(p) != Demosaic::Amaze)
     LRE_CUDA_TRY(c, cudaMemcpyAsync(const_cast<float*>(d_mosaic), h_mosaic, w * h * sizeof(float),
                                     cudaMemcpyHostToDevice, c->stream));
+  // cur_max_g: a device scalar holding max(0, max G) of `cur`, when the stage
+  // that wrote `cur` reduced it on the way (nullptr otherwise).  Defringe and
+  // the axial filter each need that maximum of their input; with the
+  // 51 MP order (demosaic -> defringe -> axial) the producer supplies it and
+  // saves a full read of the image per consumer.
+  float* cur_max_g = nullptr;
+  const bool max_after_demosaic =
+      p.stage_order == 1 && !p.highlight_recovery && (p.defringe || p.axial_ca_correction);
   switch (route(p)) {
     case Demosaic::Xtrans1:
     case Demosaic::Xtrans3:
@@ -136,20 +144,25 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
         LRE_CUDA_TRY(c, cudaEventRecord(c->band_ev[7], c->stream));
         LRE_CUDA_TRY(c, cudaStreamWaitEvent(c->copy_stream, c->band_ev[7], 0));
         LRE_TRY(lre::launch_amaze_from_host(c, h_mosaic, const_cast<float*>(d_mosaic), cur, w, h, p.filters, p.cam_mul,
-                                            p.maximum_value, c->copy_stream, c->band_ev, 6));
+                                            p.maximum_value, c->copy_stream, c->band_ev, 6,
+                                            max_after_demosaic ? c->d_scalars + 2 : nullptr));
       } else {
-        LRE_TRY(lre::launch_amaze(c, d_mosaic, 1, cur, w, h, p.filters, p.cam_mul, p.maximum_value));
+        LRE_TRY(lre::launch_amaze(c, d_mosaic, 1, cur, w, h, p.filters, p.cam_mul, p.maximum_value,
+                                  max_after_demosaic ? c->d_scalars + 2 : nullptr));
       }
+      if (max_after_demosaic) cur_max_g = c->d_scalars + 2;
       break;
   }
   c->ws.rewind(mark);
   if (p.highlight_recovery) {
+    cur_max_g = nullptr;
     if (route(p) != Demosaic::Dcb && route(p) != Demosaic::Aahd)
       LRE_CUDA_TRY(c, cudaMemsetAsync(d_err, 0, sizeof(int), c->stream));
     LRE_TRY(lre::launch_recover_highlights(c, cur, cur, w, h, p.highlight_threshold, nullptr, nullptr, nullptr, d_err));
   }
   c->ws.rewind(mark);
   auto tone = [&]() -> lre_status {
+    if (p.tone_mapping) cur_max_g = nullptr;
     if (p.tone_mapping == 1) LRE_TRY(lre::launch_tone_mapping(c, cur, cur, w * h, p.tone_after_scale));
     if (p.tone_mapping == 2) {
       LRE_TRY(lre::launch_detail_tonemap(c, cur, cur, w, h));
@@ -159,6 +172,7 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
   };
   auto lateral = [&]() -> lre_status {
     if (!p.lateral_ca_correction) return LRE_OK;
+    cur_max_g = nullptr;
     LRE_TRY(lre::launch_lateral_ca(c, cur, cur, w, h, p.lateral_ca_cell_size, p.lateral_ca_max_iterations,
                                    p.lateral_ca_max_shift, p.lateral_ca_min_confidence, p.lateral_ca_pyramid_levels));
     c->ws.rewind(mark);
@@ -167,8 +181,11 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
   const bool in_bands = tail && banded_tail(p);
   auto axial = [&]() -> lre_status {
     if (!p.axial_ca_correction) return LRE_OK;
-    float* dmax = c->d_scalars + 1;
-    LRE_TRY(lre::launch_channel_max(c, cur, w * h, 1, dmax, true));
+    float* dmax = cur_max_g;
+    if (!dmax) {
+      dmax = c->d_scalars + 1;
+      LRE_TRY(lre::launch_channel_max(c, cur, w * h, 1, dmax, true));
+    }
     if (in_bands) {
       float* dst = other;
       LRE_TRY(lre::launch_axial_ca_banded(
@@ -184,14 +201,18 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
                                    dmax));
     }
     std::swap(cur, other);
+    cur_max_g = nullptr;
     c->ws.rewind(mark);
     return LRE_OK;
   };
   auto defringe = [&]() -> lre_status {
     if (!p.defringe) return LRE_OK;
+    // the axial filter follows directly in the 51 MP order
+    float* out_max = (p.stage_order == 1 && p.axial_ca_correction) ? c->d_scalars + 3 : nullptr;
     LRE_TRY(lre::launch_defringe(c, cur, cur, w, h, p.defringe_radius, p.defringe_edge_threshold,
                                  p.defringe_chroma_threshold, p.defringe_strength, p.defringe_green != 0,
-                                 p.defringe_green_strength, nullptr));
+                                 p.defringe_green_strength, cur_max_g, out_max));
+    cur_max_g = out_max;
     c->ws.rewind(mark);
     return LRE_OK;
   };

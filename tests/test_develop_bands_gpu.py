@@ -82,3 +82,44 @@ def test_banded_tail_pinned_destination(acc, lre):
     out[:] = 0
     acc.develop(mos, p, out=out)
     assert np.array_equal(out, _device_develop(acc, mos, p))
+
+
+def _standalone_chain(acc, mos, p, w, h):
+    """The 51 MP order as separate device calls, each stage reducing its own
+    input maximum (AMaZE -> defringe -> axial CA -> ACES)."""
+    import torch
+
+    from libraw_enhanced_b200 import scenes as sc
+
+    d_in = torch.from_numpy(mos).cuda()
+    a = torch.empty((h, w, 3), dtype=torch.float32, device="cuda")
+    b = torch.empty_like(a)
+    acc.dev_demosaic_bayer_amaze(d_in, a, w, h, sc.FILTERS["RGGB"], WB, 1.0)
+    if p.defringe:
+        acc.dev_defringe(a, a, w, h)
+    if p.axial_ca_correction:
+        acc.dev_ca_axial_cleanup(a, b, w, h)
+        a, b = b, a
+    if p.tone_mapping == 1:
+        acc.dev_tone_mapping(a, a, w, h, 1.0)
+    acc.synchronize()
+    return a.cpu().numpy()
+
+
+@pytest.mark.parametrize("hw", [(517, 1203), (33, 40), (96, 64)])
+@pytest.mark.parametrize("defringe", [1, 0])
+def test_fused_maxima_match_standalone_stages(acc, lre, hw, defringe):
+    """AMaZE and the defringe main pass hand the next stage its input's max G
+    (reduced in their own kernels, the 4-px border included); the result must
+    equal the stages run one by one, each reducing its own input."""
+    h, w = hw
+    mos = scenes.bayer_scene(h, w, 15)
+    # the brightest samples sit in the border frame, so the border pass's
+    # share of the maximum decides it
+    mos[:2, :] = np.float32(0.97)
+    mos[:, -3:] = np.float32(0.99)
+    p = lre.develop_params(cfa="RGGB", cam_mul=WB, defringe=defringe, axial_ca_correction=1, tone_mapping=1,
+                           stage_order=1)
+    ref = _standalone_chain(acc, mos, p, w, h)
+    assert np.array_equal(_device_develop(acc, mos, p), ref)
+    assert np.array_equal(acc.develop(mos, p), ref)
