@@ -781,8 +781,9 @@ lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, si
     src = tmp;
   }
   // Strip width 128 (4 columns per lane) or 64 (2 per lane); strip height:
-  // enough one-warp strips for ~24 resident warps per SM (the
-  // passes are load-latency bound), but at least 16 rows so the 2r + 1 row
+  // enough one-warp strips for at least 24 per SM (more than the 16-20 that
+  // fit at once, so every SM stays full while the passes, which are
+  // load-latency bound, drain), but at least 16 rows so the 2r + 1 row
   // prologue of a strip stays small; capped by the tuning choice.
   const int WS = c->tune.axial_strip == 64 ? 64 : 128;
   const size_t strips_x = (w + WS - 1) / WS;
