@@ -136,3 +136,25 @@ def test_launch_counter_counts_own_kernels(acc):
     # init + max G + prep, blur with the support seed fused, blur of the
     # seed, line-link, blur of the solo seeds, main pass
     assert acc.launch_count - n0 == 1 + 8
+
+
+def test_defringe_unaligned_views_match(acc):
+    """The defringe main pass reads and writes four pixels per float4 when
+    the RGB buffers are 16-byte aligned and falls back to one pixel per step
+    otherwise (and for the last W*H % 4 pixels); both forms must agree."""
+    torch = pytest.importorskip("torch")
+    h, w = 203, 301  # W*H % 4 == 3: the scalar tail runs too
+    img = torch.from_numpy(oracle.amaze(scenes.sparse_rgb(scenes.bayer_scene(h, w, 5), "RGGB"),
+                                        scenes.FILTERS["RGGB"], WB, 1.0)).cuda()
+    aligned = torch.empty_like(img)
+    acc.dev_defringe(img, aligned, w, h)
+    src_buf = torch.empty(h * w * 3 + 1, device="cuda")
+    dst_buf = torch.empty(h * w * 3 + 1, device="cuda")
+    src = src_buf[1:].view(h, w, 3)  # 4-byte offset: not 16-byte aligned
+    dst = dst_buf[1:].view(h, w, 3)
+    src.copy_(img)
+    acc.synchronize()
+    torch.cuda.synchronize()
+    acc.dev_defringe(src, dst, w, h)
+    acc.synchronize()
+    assert torch.equal(dst, aligned)
