@@ -246,7 +246,6 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
   XtSlab S = make_xt_slab(A.scratch + (size_t)blockIdx.x * kXtSlabBytes);
   __shared__ int s_tile;
   const int W = A.W, H = A.H;
-  const int dirv[4] = {1, ts, ts + 1, ts - 1};
   bool zeroed_once = false;
 
   for (;;) {
@@ -428,34 +427,39 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
             if (!xisgreen(P, row, leftstart)) break;
           int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1 + (xfc(P, row, leftstart + 1) & 1));
           const float2* g = S.gmm + (size_t)(row - top) * (ts / 2);
+          // A site's three directions write three different planes and
+          // read only their own plane, so all fifteen operands are loaded
+          // before the three stores; sites stay in the reference's order.
+          auto site = [&](int col, int f, const short* hex, int flip) {
+            float v[3][5];
+#pragma unroll
+            for (int d = 3; d < 6; d++) {
+              const float* rix = RGB((d - 2) ^ flip, row - top, col - left);
+              const int o1 = hex[d] * 3, o2 = -2 * hex[d] * 3;
+              v[d - 3][0] = rix[o2 + 1];
+              v[d - 3][1] = rix[o1 + 1];
+              v[d - 3][2] = rix[o1 + f];
+              v[d - 3][3] = rix[o2 + f];
+              v[d - 3][4] = rix[f];
+            }
+            const float2 mmv = g[(col - left) >> 1];
+#pragma unroll
+            for (int d = 3; d < 6; d++) {
+              const float* q = v[d - 3];
+              const float val = 0.33333333f * (q[0] + 2 * (q[1] - q[2]) - q[3]) + q[4];
+              RGB((d - 2) ^ flip, row - top, col - left)[1] = LIMf(val, mmv.x, mmv.y);
+            }
+          };
           if (coloffset == 3) {
             int f = xfc(P, row, leftstart);
             const short* hex = P.allhex1[row % 3][leftstart % 3];
-            for (int col = leftstart; col < mcol_g - 2; col += coloffset, f ^= 2) {
-              for (int d = 3; d < 6; d++) {
-                float* rix = RGB(d - 2, row - top, col - left);
-                const int o1 = hex[d] * 3, o2 = -2 * hex[d] * 3;
-                const float val =
-                    0.33333333f * (rix[o2 + 1] + 2 * (rix[o1 + 1] - rix[o1 + f]) - rix[o2 + f]) + rix[f];
-                const float2 mmv = g[(col - left) >> 1];
-                rix[1] = LIMf(val, mmv.x, mmv.y);
-              }
-            }
+            for (int col = leftstart; col < mcol_g - 2; col += coloffset, f ^= 2) site(col, f, hex, 0);
           } else {
             int f = xfc(P, row, leftstart);
             const short* hexmod[2] = {P.allhex1[row % 3][leftstart % 3], P.allhex1[row % 3][(leftstart + coloffset) % 3]};
             for (int col = leftstart, hexindex = 0; col < mcol_g - 2;
-                 col += coloffset, coloffset ^= 3, f = f ^ (coloffset & 2), hexindex ^= 1) {
-              const short* hex = hexmod[hexindex];
-              for (int d = 3; d < 6; d++) {
-                float* rix = RGB((d - 2) ^ 1, row - top, col - left);
-                const int o1 = hex[d] * 3, o2 = -2 * hex[d] * 3;
-                const float val =
-                    0.33333333f * (rix[o2 + 1] + 2 * (rix[o1 + 1] - rix[o1 + f]) - rix[o2 + f]) + rix[f];
-                const float2 mmv = g[(col - left) >> 1];
-                rix[1] = LIMf(val, mmv.x, mmv.y);
-              }
-            }
+                 col += coloffset, coloffset ^= 3, f = f ^ (coloffset & 2), hexindex ^= 1)
+              site(col, f, hexmod[hexindex], 1);
           }
         }
         __syncthreads();
@@ -509,14 +513,34 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
           const int c = ((row - P.sgrow) % 3) ? ts : 1;
           const int h = 3 * (c ^ ts ^ 1);
           const int f = 2 - xfc(P, row, col);
-          float* rix = RGB(0, row - top, col - left);
-          for (int d = 0; d < 4; d++, rix += (size_t)ts * ts * 3) {
-            const int ii = d > 1 || ((d ^ c) & 1) ||
-                                   ((fabsf(rix[1] - rix[c * 3 + 1]) + fabsf(rix[1] - rix[-c * 3 + 1])) <
-                                    2.f * (fabsf(rix[1] - rix[h * 3 + 1]) + fabsf(rix[1] - rix[-h * 3 + 1])))
-                               ? c
-                               : h;
-            rix[f] = rix[1] + 0.5f * (rix[ii * 3 + f] + rix[-ii * 3 + f] - rix[ii * 3 + 1] - rix[-ii * 3 + 1]);
+          float* rix0 = RGB(0, row - top, col - left);
+          // every operand of the four directions is loaded before the first
+          // store (the stores go to this site's own colour f in each plane,
+          // which no load reads), so the loads are in flight together; the
+          // h operands are loaded even where the reference does not need
+          // them (they lie inside the tile plane)
+          float g0[4], gc0[4], gc1[4], gh0[4], gh1[4], fc0[4], fc1[4], fh0[4], fh1[4];
+#pragma unroll
+          for (int d = 0; d < 4; d++) {
+            const float* rix = rix0 + (size_t)d * ts * ts * 3;
+            g0[d] = rix[1];
+            gc0[d] = rix[c * 3 + 1];
+            gc1[d] = rix[-c * 3 + 1];
+            gh0[d] = rix[h * 3 + 1];
+            gh1[d] = rix[-h * 3 + 1];
+            fc0[d] = rix[c * 3 + f];
+            fc1[d] = rix[-c * 3 + f];
+            fh0[d] = rix[h * 3 + f];
+            fh1[d] = rix[-h * 3 + f];
+          }
+#pragma unroll
+          for (int d = 0; d < 4; d++) {
+            const bool use_c = d > 1 || ((d ^ c) & 1) ||
+                               ((fabsf(g0[d] - gc0[d]) + fabsf(g0[d] - gc1[d])) <
+                                2.f * (fabsf(g0[d] - gh0[d]) + fabsf(g0[d] - gh1[d])));
+            const float a0 = use_c ? fc0[d] : fh0[d], a1 = use_c ? fc1[d] : fh1[d];
+            const float b0 = use_c ? gc0[d] : gh0[d], b1 = use_c ? gc1[d] : gh1[d];
+            rix0[(size_t)d * ts * ts * 3 + f] = g0[d] + 0.5f * (a0 + a1 - b0 - b1);
           }
         }
         __syncthreads();
@@ -566,16 +590,34 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
         for (int i = tid; i < (nrows > 0 ? nrows : 0) * (ncols > 0 ? ncols : 0); i += nth) {
           const int q_ = fdf.div(i), row = topstart + q_, col = leftstart + i - q_ * ncols;
           if (!((row - P.sgrow) % 3) || !((col - P.sgcol) % 3)) continue;
-          float* rix = RGB(0, row - top, col - left);
+          float* rix0 = RGB(0, row - top, col - left);
           const short* hex = P.allhex1[row % 3][col % 3];
-          for (int d = 0; d < NDIR; d += 2, rix += (size_t)ts * ts * 3) {
-            const int o0 = hex[d] * 3, o1 = hex[d + 1] * 3;
-            if (hex[d] + hex[d + 1]) {
-              const float g = 3 * rix[1] - 2 * rix[o0 + 1] - rix[o1 + 1];
-              for (int c = 0; c < 4; c += 2) rix[c] = (g + 2 * rix[o0 + c] + rix[o1 + c]) * 0.33333333f;
+          // all loads of the four direction planes first, then the stores
+          // (this site's own R and B, which no load reads)
+          float v1[4], a1[4], b1[4], a0[4], b0[4], a2[4], b2[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const float* rix = rix0 + (size_t)q * ts * ts * 3;
+            const int o0 = hex[2 * q] * 3, o1 = hex[2 * q + 1] * 3;
+            v1[q] = rix[1];
+            a1[q] = rix[o0 + 1];
+            b1[q] = rix[o1 + 1];
+            a0[q] = rix[o0];
+            b0[q] = rix[o1];
+            a2[q] = rix[o0 + 2];
+            b2[q] = rix[o1 + 2];
+          }
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            float* rix = rix0 + (size_t)q * ts * ts * 3;
+            if (hex[2 * q] + hex[2 * q + 1]) {
+              const float g = 3 * v1[q] - 2 * a1[q] - b1[q];
+              rix[0] = (g + 2 * a0[q] + b0[q]) * 0.33333333f;
+              rix[2] = (g + 2 * a2[q] + b2[q]) * 0.33333333f;
             } else {
-              const float g = 2 * rix[1] - rix[o0 + 1] - rix[o1 + 1];
-              for (int c = 0; c < 4; c += 2) rix[c] = (g + rix[o0 + c] + rix[o1 + c]) * 0.5f;
+              const float g = 2 * v1[q] - a1[q] - b1[q];
+              rix[0] = (g + a0[q] + b0[q]) * 0.5f;
+              rix[2] = (g + a2[q] + b2[q]) * 0.5f;
             }
           }
         }
@@ -617,27 +659,46 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
       const int dn = XTS - 10;
       const int rows = mrow - 10, cols = mcol - 10;
       const XDiv fdrc(rows * cols), fdcl(cols);
-      for (int i = tid; i < NDIR * rows * cols; i += nth) {
-        const int d = fdrc.div(i);
-        const int rem = i - d * (rows * cols);
-        const int q_ = fdcl.div(rem);
-        const int row = 5 + q_, col = 5 + rem - q_ * cols;
-        int f = dirv[d & 3];
-        f = f == 1 ? 1 : f - 8;
-        // yuv buffer offset f (width ts-8) -> tile offset
-        const int fr = (f == 1) ? 0 : 1, fc = (f == 1) ? 1 : (f - (XTS - 8));
-        auto yuv = [&](int r, int c, float& y, float& u, float& v) {
-          const float* p = RGB(d, r, c);
-          y = 0.2627f * p[0] + 0.6780f * p[1] + 0.0593f * p[2];
-          u = (p[2] - y) * 0.56433f;
-          v = (p[0] - y) * 0.67815f;
-        };
-        float y0, u0, v0, yp, up, vp, ym, um, vm;
-        yuv(row, col, y0, u0, v0);
-        yuv(row + fr, col + fc, yp, up, vp);
-        yuv(row - fr, col - fc, ym, um, vm);
-        S.drv[((size_t)d * dn + (row - 5)) * dn + (col - 5)] =
-            SQRf(2 * y0 - yp - ym) + SQRf(2 * u0 - up - um) + SQRf(2 * v0 - vp - vm);
+      const int n = NDIR * rows * cols;
+      // four items per thread and step: their 36 loads are issued before the
+      // first store (a store to the derivative planes could otherwise alias
+      // the next item's loads for the compiler)
+      constexpr int U = 4;
+      for (int i0 = tid; i0 < n; i0 += U * nth) {
+        float res[U];
+        int at[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const int i = i0 + u * nth;
+          at[u] = -1;
+          if (i < n) {
+            const int d = fdrc.div(i);
+            const int rem = i - d * (rows * cols);
+            const int q_ = fdcl.div(rem);
+            const int row = 5 + q_, col = 5 + rem - q_ * cols;
+            const int dv = d & 3;
+            // direction steps 1, ts, ts + 1, ts - 1 of directions 0..3 (and 4..7)
+            int f = dv == 0 ? 1 : (dv == 1 ? ts : (dv == 2 ? ts + 1 : ts - 1));
+            f = f == 1 ? 1 : f - 8;
+            // yuv buffer offset f (width ts-8) -> tile offset
+            const int fr = (f == 1) ? 0 : 1, fc = (f == 1) ? 1 : (f - (XTS - 8));
+            auto yuv = [&](int r, int c, float& y, float& uu, float& v) {
+              const float* p = RGB(d, r, c);
+              y = 0.2627f * p[0] + 0.6780f * p[1] + 0.0593f * p[2];
+              uu = (p[2] - y) * 0.56433f;
+              v = (p[0] - y) * 0.67815f;
+            };
+            float y0, u0, v0, yp, up, vp, ym, um, vm;
+            yuv(row, col, y0, u0, v0);
+            yuv(row + fr, col + fc, yp, up, vp);
+            yuv(row - fr, col - fc, ym, um, vm);
+            res[u] = SQRf(2 * y0 - yp - ym) + SQRf(2 * u0 - up - um) + SQRf(2 * v0 - vp - vm);
+            at[u] = (d * dn + (row - 5)) * dn + (col - 5);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+          if (at[u] >= 0) S.drv[at[u]] = res[u];
       }
     }
     __syncthreads();
@@ -652,12 +713,18 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
         float tr = D(0, row, col) < D(1, row, col) ? D(0, row, col) : D(1, row, col);
         for (int d = 2; d < NDIR; d++) tr = (D(d, row, col) < tr ? D(d, row, col) : tr);
         tr *= 8;
+        // all eight counts first, then the stores: a byte store may alias
+        // any load for the compiler, which would otherwise wait for each
+        // direction's loads in turn
+        unsigned char temp[NDIR];
+#pragma unroll
         for (int d = 0; d < NDIR; d++) {
-          unsigned char temp = 0;
+          temp[d] = 0;
           for (int v = -1; v <= 1; v++)
-            for (int h = -1; h <= 1; h++) temp += (D(d, row + v, col + h) <= tr ? 1 : 0);
-          S.homo[((size_t)d * ts + row) * ts + col] = temp;
+            for (int h = -1; h <= 1; h++) temp[d] += (D(d, row + v, col + h) <= tr ? 1 : 0);
         }
+#pragma unroll
+        for (int d = 0; d < NDIR; d++) S.homo[((size_t)d * ts + row) * ts + col] = temp[d];
       }
     }
     __syncthreads();
