@@ -486,7 +486,7 @@ lre_status launch_dcb(Context* c, const float* raw, int raw_c_stride, float* rgb
 
   Geo g{(int)w, (int)h, filters, maximum_value};
   const dim3 blk(32, 8);
-  const dim3 grd((unsigned)std::min<size_t>((w + 31) / 32, 1024), (unsigned)std::min<size_t>((h + 7) / 8, 8192));
+  const dim3 grd((unsigned)std::min<size_t>((w + 63) / 64, 1024), (unsigned)std::min<size_t>((h + 7) / 8, 8192));
   cudaStream_t s = c->stream;
 #define DCB_LAUNCH(k, ...)                              \
   do {                                                  \

@@ -46,10 +46,16 @@ struct Geo {
   __device__ __forceinline__ size_t at(int r, int c) const { return (size_t)r * W + c; }
 };
 
-// 2D launch helper: (32 x 8) threads, grid-strided in y.
-#define GS_FOR_PIXELS(g)                                                             \
-  for (int r = blockIdx.y * blockDim.y + threadIdx.y; r < (g).H; r += gridDim.y * blockDim.y) \
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < (g).W; c += gridDim.x * blockDim.x)
+// 2D launch helper: (32 x 8) threads, grid-strided in y.  Along x a block
+// covers 64 columns and each thread takes two of them of the same parity in
+// two half-passes (lane l: columns 2l, then 2l + 1), so the 32 lanes of a
+// warp see one Bayer colour at a time and do not diverge on it.  Launch with
+// (W + 63) / 64 blocks in x.
+#define GS_FOR_PIXELS(g)                                                                        \
+  for (int r = blockIdx.y * blockDim.y + threadIdx.y; r < (g).H; r += gridDim.y * blockDim.y)   \
+    for (int gs_half = 0; gs_half < 2; gs_half++)                                                \
+      for (int c = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + gs_half; c < (g).W;             \
+           c += 2 * gridDim.x * blockDim.x)
 
 struct SweepArgs {
   float* plane[4];  // state planes first, then read-only inputs
