@@ -71,9 +71,15 @@ struct Aahd {
   }
 };
 
+// One pixel per (i, j), independent of order.  Along x a block covers 64
+// columns and each thread takes two of them of the same parity in two
+// half-passes, so a warp's lanes see one Bayer colour at a time (launch with
+// (W + 63) / 64 blocks in x).
 #define AAHD_FOR_PIXELS(A)                                                                    \
   for (int i = blockIdx.y * blockDim.y + threadIdx.y; i < (A).H; i += gridDim.y * blockDim.y) \
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < (A).W; j += gridDim.x * blockDim.x)
+    for (int aahd_half = 0; aahd_half < 2; aahd_half++)                                        \
+      for (int j = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + aahd_half; j < (A).W;         \
+           j += 2 * gridDim.x * blockDim.x)
 
 __device__ __forceinline__ void atomic_max_f(float* a, float v) {
   int old = __float_as_int(*a);
@@ -431,7 +437,7 @@ lre_status launch_aahd(Context* c, const float* raw, int raw_c_stride, float* rg
   LRE_TRY(check_launch(c, "demosaic_bayer_aahd"));
 
   const dim3 blk(32, 8);
-  const dim3 grd((unsigned)std::min<size_t>((w + 31) / 32, 1024), (unsigned)std::min<size_t>((h + 7) / 8, 8192));
+  const dim3 grd((unsigned)std::min<size_t>((w + 63) / 64, 1024), (unsigned)std::min<size_t>((h + 7) / 8, 8192));
 #define AAHD_LAUNCH(k, ...)                             \
   do {                                                  \
     k<<<grd, blk, 0, s>>>(__VA_ARGS__);                 \
