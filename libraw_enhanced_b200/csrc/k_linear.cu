@@ -8,6 +8,8 @@
 // sample divided by maximum before summing, as the reference does); then the
 // 1-px frame is filled by the LibRaw border interpolation.  One thread per
 // pixel; the interior reads only the mosaic, so there is no ordering.
+#include <algorithm>
+
 #include "common.cuh"
 #include "lre_internal.h"
 
@@ -20,11 +22,17 @@ __device__ __forceinline__ float lin_raw(const float* __restrict__ raw, int cstr
   return cstride == 1 ? raw[i] : raw[i * 3 + c];
 }
 
-__global__ void k_bayer_linear(const float* __restrict__ raw, int cstride, float* __restrict__ rgb, int W, int H,
-                               uint32_t filters, float maximum) {
-  const size_t n = (size_t)W * H;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int row = (int)(i / W), col = (int)(i % W);
+// (32 x 8) threads per block, grid-strided over rows; along x a block
+// covers 64 columns and each thread takes two of them of the same parity in
+// two half-passes, so a warp's lanes see one Bayer colour at a time and take
+// the same branches.
+__global__ void __launch_bounds__(256) k_bayer_linear(const float* __restrict__ raw, int cstride,
+                                                      float* __restrict__ rgb, int W, int H, uint32_t filters,
+                                                      float maximum) {
+  for (int row = blockIdx.y * blockDim.y + threadIdx.y; row < H; row += gridDim.y * blockDim.y)
+  for (int half = 0; half < 2; half++)
+  for (int col = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + half; col < W; col += 2 * gridDim.x * blockDim.x) {
+    const size_t i = (size_t)row * W + col;
     const unsigned color = fcol3((unsigned)row, (unsigned)col, filters);
     float* o = rgb + i * 3;
     o[color] = lin_raw(raw, cstride, col, row, W, color) / maximum;
@@ -61,8 +69,9 @@ __global__ void k_bayer_linear(const float* __restrict__ raw, int cstride, float
 
 lre_status launch_bayer_linear(Context* c, const float* raw, int raw_c_stride, float* rgb, size_t w, size_t h,
                                uint32_t filters, float maximum_value) {
-  k_bayer_linear<<<grid_for(w * h, 256, c->sm_count * 8), 256, 0, c->stream>>>(raw, raw_c_stride, rgb, (int)w, (int)h,
-                                                                              filters, maximum_value);
+  const dim3 blk(32, 8);
+  const dim3 grd((unsigned)std::min<size_t>((w + 63) / 64, 1024), (unsigned)std::min<size_t>((h + 7) / 8, 8192));
+  k_bayer_linear<<<grd, blk, 0, c->stream>>>(raw, raw_c_stride, rgb, (int)w, (int)h, filters, maximum_value);
   count_launch(c);
   LRE_TRY(check_launch(c, "demosaic_bayer_linear"));
   return launch_border_interp(c, rgb, w, h, filters, 1);
