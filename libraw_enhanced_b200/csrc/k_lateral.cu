@@ -12,6 +12,7 @@
 // equations in double with warp shuffles, and thread 0 solves and broadcasts
 // the step, so all LK iterations of a cell stay on chip.  Gate + smoothing
 // run in one small kernel; the remap is a streaming kernel.
+#include <algorithm>
 #include <cmath>
 
 #include "lre_internal.h"
@@ -265,9 +266,10 @@ __device__ __forceinline__ void sample_shift(ShiftMaps m, int map_w, int map_h, 
 __global__ void k_lk_remap(const float* __restrict__ R0, const float* __restrict__ G0, const float* __restrict__ B0,
                            float* __restrict__ dst, int W, int H, ShiftMaps mr, ShiftMaps mb, int map_w, int map_h,
                            float cell, float clamp_shift) {
-  size_t n = (size_t)W * H;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int y = (int)(i / W), x = (int)(i % W);
+  // (32 x 8) threads, 2D grid-stride: no 64-bit index division per pixel
+  for (int y = blockIdx.y * blockDim.y + threadIdx.y; y < H; y += gridDim.y * blockDim.y)
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x) {
+    const size_t i = (size_t)y * W + x;
     float drx, dry, dbx, dby;
     sample_shift(mr, map_w, map_h, cell, clamp_shift, (float)x, (float)y, drx, dry);
     sample_shift(mb, map_w, map_h, cell, clamp_shift, (float)x, (float)y, dbx, dby);
@@ -362,7 +364,8 @@ lre_status launch_lateral_ca(Context* c, const float* in, float* out, size_t w, 
   }
   k_lk_gate_smooth<<<1, 1024, 0, c->stream>>>(maps, map_w, map_h, min_conf, tmp);
   const float clamp_shift = max_shift * (float)(1 << (eff - 1));
-  k_lk_remap<<<grid_for(w * h, 256, c->sm_count * 8), 256, 0, c->stream>>>(
+  k_lk_remap<<<dim3((unsigned)std::min<size_t>((w + 31) / 32, 1024), (unsigned)std::min<size_t>((h + 7) / 8, 8192)),
+               dim3(32, 8), 0, c->stream>>>(
       Rl[0], Gl[0], Bl[0], out, (int)w, (int)h, ShiftMaps{maps.dx[0], maps.dy[0]}, ShiftMaps{maps.dx[1], maps.dy[1]},
       map_w, map_h, (float)cell, clamp_shift);
   count_launch(c, 2);
