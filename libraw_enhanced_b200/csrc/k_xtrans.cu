@@ -96,8 +96,13 @@ __device__ __forceinline__ float xraw(const XtArgs& A, int row, int col) {
 // landing site.
 __device__ __forceinline__ float xraw_hex(const XtArgs& A, int row, int col, int hex) {
   const long long pos = (long long)row * A.W + col + hex;
-  const int r = (int)(pos / A.W), c = (int)(pos % A.W);
-  const float v = A.cstride == 1 ? A.raw[pos] : A.raw[pos * 3 + xfc(A.P, r, c)];
+  float v;
+  if (A.cstride == 1) {
+    v = A.raw[pos];
+  } else {  // the landing site's colour needs its (row, col)
+    const int r = (int)(pos / A.W), c = (int)(pos % A.W);
+    v = A.raw[pos * 3 + xfc(A.P, r, c)];
+  }
   return v / A.maximum;
 }
 
