@@ -484,6 +484,15 @@ __global__ void __launch_bounds__(256) k_df_line(const float* __restrict__ src, 
     int y = y0 + ly, x = x0 + lx;
     if (x >= W || y >= H) continue;
     const int c = (ly + LH) * LE + (lx + LH);
+    const size_t gi = (size_t)y * W + x;
+    // the solo-seed operands are loaded first, so their latency overlaps
+    // the line search (which reads shared memory only); loaded after the
+    // lfs store below, they would wait for it
+    const float* s = src + gi * 3;
+    const float s0 = s[0], s1 = s[1], s2 = s[2];
+    const float blur_guide = P.bg[gi];
+    const float blrg = P.blrg[gi], blbg = P.blbg[gi];
+    const float bfs = P.bfs[gi], be = P.be[gi], ber = P.ber[gi];
     float best = 0.f;
     if (tile_active) {
       // directions and step counts of core/cpu_accelerator.cpp:4290-4318
@@ -496,25 +505,22 @@ __global__ void __launch_bounds__(256) k_df_line(const float* __restrict__ src, 
       line_dir<2, -1, 6>(s_ls, s_fs, c, best);
       line_dir<1, -2, 6>(s_ls, s_fs, c, best);
     }
-    const size_t gi = (size_t)y * W + x;
     P.lfs[gi] = best;
 
     // solo seeds (core/cpu_accelerator.cpp:4325-4374)
-    const float* s = src + gi * 3;
-    const float blur_guide = P.bg[gi];
-    const float g = smax(s[1], 0.f);
-    const float target_r = g * exp_cr(P.blrg[gi]);
-    const float target_b = g * exp_cr(P.blbg[gi]);
-    const float solo_r = smax(0.f, s[0] - target_r) / smax(blur_guide, 0.05f);
-    const float solo_b = smax(0.f, s[2] - target_b) / smax(blur_guide, 0.05f);
-    const float linked_fringe = ssmooth(0.004f, 0.045f, smax(P.bfs[gi], best * 0.90f));
-    const float c_edge_solo = ssmooth(k.edge_thr * 0.35f * inv_s, k.edge_thr * 1.50f * inv_s, P.be[gi]) *
-                              ssmooth(0.55f * inv_s, 1.35f * inv_s, P.ber[gi]);
+    const float g = smax(s1, 0.f);
+    const float target_r = g * exp_cr(blrg);
+    const float target_b = g * exp_cr(blbg);
+    const float solo_r = smax(0.f, s0 - target_r) / smax(blur_guide, 0.05f);
+    const float solo_b = smax(0.f, s2 - target_b) / smax(blur_guide, 0.05f);
+    const float linked_fringe = ssmooth(0.004f, 0.045f, smax(bfs, best * 0.90f));
+    const float c_edge_solo = ssmooth(k.edge_thr * 0.35f * inv_s, k.edge_thr * 1.50f * inv_s, be) *
+                              ssmooth(0.55f * inv_s, 1.35f * inv_s, ber);
     const float c_bright_solo = ssmooth(0.24f * inv_s, 0.52f * inv_s, blur_guide);
     const float solo_enable = ssmooth(1.25f, 3.0f, k.strength);
-    const float r0 = smax(s[0], 0.f);
-    const float g0 = smax(s[1], 0.f);
-    const float b0 = smax(s[2], 0.f);
+    const float r0 = smax(s0, 0.f);
+    const float g0 = smax(s1, 0.f);
+    const float b0 = smax(s2, 0.f);
     const float red_strength_solo = smax(0.f, r0 - smax(g0, b0)) / smax(r0, 1e-4f);
     const float solo_red_guard = 1.f - 0.90f * ssmooth(0.12f, 0.32f, red_strength_solo);
     P.srs[gi] = solo_enable * c_edge_solo * c_bright_solo * linked_fringe * solo_red_guard *
