@@ -19,7 +19,8 @@ Reported (one JSON line from rank 0):
   roofline -- the dominant stage (largest device time) against the measured
             HBM copy bandwidth, from its algorithmic bytes per pixel;
   cpu_baseline -- the reference's own CPU accelerator (oracle/_ref) on this
-            host's cores, same chain on a bounded crop.
+            host's cores: the same chain on the same 8736x5856 mosaic,
+            a bounded number of develops.
 """
 from __future__ import annotations
 
@@ -41,12 +42,23 @@ WB = (2.0, 1.0, 1.5, 1.0)
 METRIC = "develop MP/s on 1 B200 (51 MP Bayer: AMaZE->defringe->axial CA->tone map)"
 # algorithmic bytes per output pixel of each stage (float32 RGB = 12 B/px)
 STAGE_BYTES = {"amaze": 16.0, "defringe": 24.0, "axial": 24.0, "tone": 24.0}
-# From one ncu capture of k_amaze at 4096x3072 (profiles/develop_12mp_full.md):
-# DRAM read+write bytes and executed warp-instructions per output pixel.
+# From one ncu capture of k_amaze at 4096x3072: DRAM read+write bytes and
+# executed warp-instructions per output pixel.
 AMAZE_DRAM_BYTES_PER_PX = (124.060416e6 + 909.380352e6) / (4096 * 3072)
 AMAZE_WARP_INST_PER_PX = 925190063 / (4096 * 3072)
 # issue roofline: 148 SMs x 4 schedulers x 1.965 GHz, one warp-instruction per cycle each
 ISSUE_PEAK_G = 148 * 4 * 1.965
+
+
+def workload_config(world=1):
+    """The `config` object both arms print (same workload, same sizes)."""
+    return {
+        "workload": "51 MP Bayer develop: AMaZE -> defringe(r10,s10) -> axial CA(r6) -> ACES(1.0), f32 RGB out",
+        "width": W,
+        "height": H,
+        "parallelism": f"replicas x{world}",
+        "l2": "inputs 205 MB mosaic + 614 MB RGB exceed the 126 MB L2 (no flush needed)",
+    }
 
 
 def load_peaks():
@@ -196,41 +208,40 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
-def cpu_baseline(seconds=12.0, threads=None):
-    """The reference CPU accelerator on a 1536x1024 crop of the workload."""
-    import numpy as np
-
+def reference_chain(mosaic, threads):
+    """One develop of `mosaic` by the reference's own CPU accelerator
+    (oracle/_ref): AMaZE -> defringe -> axial CA -> ACES, the GPU arm's chain
+    and parameters."""
     import oracle
     from libraw_enhanced_b200 import scenes
 
-    threads = threads or os.cpu_count() or 1
     oracle.set_threads(threads)
-    h, w = 1024, 1536
-    mos = scenes.bayer_scene(h, w, SEED)
-    sp = scenes.sparse_rgb(mos, "RGGB")
+    sp = scenes.sparse_rgb(mosaic, "RGGB")
+    x = oracle.amaze(sp, scenes.FILTERS["RGGB"], WB, 1.0)
+    del sp
+    x = oracle.defringe(x, 10.0, 0.1, 0.15, 10.0, False, 0.3)
+    x = oracle.axial_ca(x, 6, 1e-4, 0.3)
+    return oracle.tone_mapping(x, 1.0)
 
-    def chain():
-        x = oracle.amaze(sp, scenes.FILTERS["RGGB"], WB, 1.0)
-        x = oracle.defringe(x)
-        x = oracle.axial_ca(x, 6, 1e-4, 0.3)
-        return oracle.tone_mapping(x, 1.0)
 
-    chain()  # warm-up
-    n = 0
+def cpu_baseline(mosaic, develops=2, threads=None):
+    """The reference CPU accelerator on the bench's own 8736x5856 mosaic:
+    one untimed develop, then `develops` timed ones (about 8 s each on 16
+    cores)."""
+    threads = threads or os.cpu_count() or 1
+    reference_chain(mosaic, threads)  # warm-up
     t0 = time.perf_counter()
-    while True:
-        chain()
-        n += 1
-        if time.perf_counter() - t0 >= seconds:
-            break
+    for _ in range(develops):
+        reference_chain(mosaic, threads)
     dt = time.perf_counter() - t0
-    mp = h * w / 1e6
+    mp = mosaic.shape[0] * mosaic.shape[1] / 1e6
     return {
-        "value": round(n * mp / dt, 3),
+        "value": round(develops * mp / dt, 3),
         "unit": "MP/s",
         "cores": threads,
         "kind": "reference",
-        "sample": f"{n} develops of a {w}x{h} crop (AMaZE->defringe->axial->ACES), reference CPUAccelerator, {threads} OpenMP threads",
+        "sample": f"{develops} develops of the full {mosaic.shape[1]}x{mosaic.shape[0]} bench mosaic "
+                  f"(AMaZE->defringe->axial->ACES), reference CPUAccelerator, {threads} OpenMP threads",
     }
 
 
@@ -244,30 +255,15 @@ def run_reference(args):
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/liblre_ref.so not built"}))
         return 0
-    import numpy as np
-
-    from libraw_enhanced_b200 import scenes
-
     threads = os.cpu_count() or 1
-    oracle.set_threads(threads)
-    # bounded sample of the same workload: a 2048x2048 crop per step
-    h, w = 2048, 2048
-    mos = scenes.bayer_scene(h, w, SEED)
-    sp = scenes.sparse_rgb(mos, "RGGB")
-
-    def step():
-        x = oracle.amaze(sp, scenes.FILTERS["RGGB"], WB, 1.0)
-        x = oracle.defringe(x)
-        x = oracle.axial_ca(x, 6, 1e-4, 0.3)
-        return oracle.tone_mapping(x, 1.0)
-
+    mosaic = make_mosaic()  # the GPU arm's input, generated outside the timed region
     for _ in range(args.warmup):
-        step()
+        reference_chain(mosaic, threads)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        step()
+        reference_chain(mosaic, threads)
     dt = time.perf_counter() - t0
-    mp = h * w / 1e6 * args.steps
+    mp = H * W / 1e6 * args.steps
     v = mp / dt
     line = {
         "metric": METRIC,
@@ -282,11 +278,11 @@ def run_reference(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic (seeded fringed scene)",
-        "config": {"workload": f"51 MP Bayer develop chain, sampled as a {w}x{h} crop per step on the CPU",
-                   "chain": "AMaZE->defringe->axial->ACES"},
+        "data": f"synthetic (seeded fringed scene, {W}x{H} RGGB)",
+        "config": workload_config(args.gpus),
         "cpu_baseline": {"value": round(v, 3), "unit": "MP/s", "cores": threads, "kind": "reference",
-                         "sample": f"{args.steps} develops of a {w}x{h} crop"},
+                         "sample": f"{args.steps} develops of the full {W}x{H} mosaic, host buffers, "
+                                   f"{threads} OpenMP threads"},
         "e2e": {"value": round(v, 3), "unit": "MP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -360,11 +356,11 @@ def run_ours(args):
 
     # ---------------- end to end through the C ABI with pinned host buffers
     e2e, e_ms = None, None
+    e2p, ep_ms = None, None
     e2s, es_ms, es_lanes = None, None, None
-    if args.no_e2e:
-        h_mos = None
-    else:
+    if not args.no_e2e:
         e2e, e_ms = run_e2e(acc, mosaic, params, args, world, mp)
+        e2p, ep_ms = run_e2e(acc, mosaic, params, args, world, mp, pinned=False)
         e2s, es_ms, es_lanes = run_e2e_served(mosaic, params, args, world, mp, local)
     barrier(world)
 
@@ -409,16 +405,15 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f32",
             "data": f"synthetic (seeded fringed scene, {W}x{H} RGGB)",
-            "config": {
-                "workload": "51 MP Bayer develop: AMaZE -> defringe(r10,s10) -> axial CA(r6) -> ACES(1.0), f32 RGB out",
-                "width": W,
-                "height": H,
-                "parallelism": f"replicas x{world}",
-                "l2": "inputs 205 MB mosaic + 614 MB RGB exceed the 126 MB L2 (no flush needed)",
-            },
+            "config": workload_config(world),
             "e2e": None if e2e is None else {
                 "value": round(e2e, 2), "unit": "MP/s", "ms_per_step": round(e_ms, 3),
                 "h2d_bytes_per_step": H * W * 4, "d2h_bytes_per_step": H * W * 12},
+            "e2e_pageable": None if e2p is None else {
+                "value": round(e2p, 2), "unit": "MP/s", "ms_per_step": round(ep_ms, 3),
+                "h2d_bytes_per_step": H * W * 4, "d2h_bytes_per_step": H * W * 12,
+                "how": "same call with ordinary (pageable) numpy buffers in and out, as the drop-in caller's "
+                       "std::vector-backed ImageBufferFloat passes them"},
             "e2e_served": None if e2s is None else {
                 "value": round(e2s, 2), "unit": "MP/s", "ms_per_request": round(es_ms, 3),
                 "h2d_bytes_per_step": H * W * 4, "d2h_bytes_per_step": H * W * 12, "lanes": es_lanes,
@@ -438,7 +433,7 @@ def run_ours(args):
             line["served"] = run_served(args)
         if not args.no_cpu_baseline and world == 1:
             try:
-                line["cpu_baseline"] = cpu_baseline()
+                line["cpu_baseline"] = cpu_baseline(mosaic)
             except Exception as e:  # the oracle is test infrastructure; report, do not fail the bench
                 line["cpu_baseline"] = {"value": None, "error": str(e)}
         print(json.dumps(line))
@@ -450,15 +445,20 @@ def run_ours(args):
     return 0
 
 
-def run_e2e(acc, mosaic, params, args, world, mp):
-    """MP/s through lre_develop with pinned host buffers: the H2D copy of the
-    mosaic and the D2H copy of the RGB result are inside every timed step."""
+def run_e2e(acc, mosaic, params, args, world, mp, pinned=True):
+    """MP/s through lre_develop with host buffers (page-locked, or ordinary
+    pageable numpy arrays with pinned=False): the H2D copy of the mosaic and
+    the D2H copy of the RGB result are inside every timed step."""
+    import numpy as np
     import torch
 
-    h_mos = torch.from_numpy(mosaic).pin_memory()
-    h_out = torch.empty((H, W, 3), dtype=torch.float32).pin_memory()
-    h_mos_np = h_mos.numpy()
-    h_out_np = h_out.numpy()
+    if pinned:
+        h_mos_np = torch.from_numpy(mosaic).pin_memory().numpy()
+        h_out_np = torch.empty((H, W, 3), dtype=torch.float32).pin_memory().numpy()
+    else:
+        h_mos_np = np.array(mosaic, dtype=np.float32, copy=True)
+        h_out_np = np.empty((H, W, 3), np.float32)
+        h_out_np.fill(0.0)  # touch the pages, as a caller's filled buffer would be
     acc.set_stream(None)
     for _ in range(max(1, args.warmup // 2)):
         acc.develop(h_mos_np, params, out=h_out_np)
@@ -726,7 +726,7 @@ def run_served(args):
         p.axial_ca_correction = int(rng.random() < 0.5)
         p.lateral_ca_correction = int(rng.random() < 0.2)
         p.tone_mapping = 1 if rng.random() < 0.3 else 0
-        return m, p
+        return ki, m, p
 
     srv = lre.Server(0, lanes=4, budget_bytes=150 * 10**9)
 
@@ -749,7 +749,7 @@ def run_served(args):
         wt.start()
         t0 = time.perf_counter()
         t_next = t0
-        for k, (m, p) in enumerate(reqs):
+        for k, (_, m, p) in enumerate(reqs):
             t_next += gaps[k]
             dly = t_next - time.perf_counter()
             if dly > 0:
@@ -762,12 +762,22 @@ def run_served(args):
         wt.join()
         t_end = time.perf_counter()
         lat = np.array([s["total_ms"] for s in stats])
-        mp = sum(m.shape[0] * m.shape[1] for m, _ in reqs) / 1e6
+        mp = sum(m.shape[0] * m.shape[1] for _, m, _ in reqs) / 1e6
+        per_kind = {}
+        for ki, (kind, kh, kw, _) in enumerate(kinds):
+            lk = np.array([lat[k] for k in range(n) if reqs[k][0] == ki])
+            if lk.size:
+                per_kind[f"{kind}_{kw}x{kh}"] = {
+                    "n": int(lk.size),
+                    "p50_ms": round(float(np.percentile(lk, 50)), 1),
+                    "p99_ms": round(float(np.percentile(lk, 99)), 1),
+                }
         return {
             "lambda": lam if lam else "saturated",
             "n": n,
             "p50_ms": round(float(np.percentile(lat, 50)), 1),
             "p99_ms": round(float(np.percentile(lat, 99)), 1),
+            "per_kind": per_kind,
             "mean_queue_ms": round(float(np.mean([s["queue_ms"] for s in stats])), 1),
             "mp_s": round(mp / (t_end - t0), 1),
             "mp_per_request": round(mp / n, 2),
@@ -795,8 +805,8 @@ def run_served(args):
     run_stream(8, 0)
     rates = []
     for lam in (5, 10, 20, 30, 45, 60):
-        rates.append(run_stream(48, lam))
-    sat = run_stream(48, 0)
+        rates.append(run_stream(64, lam))
+    sat = run_stream(64, 0)
     _, peak = srv.memory()
     srv.close()
     del ring, pool
@@ -806,12 +816,14 @@ def run_served(args):
         "saturated_mp_s": sat["mp_s"],
         "saturated_p50_ms": sat["p50_ms"],
         "saturated_p99_ms": sat["p99_ms"],
+        "saturated_per_kind": sat["per_kind"],
         "lanes": 4,
         "budget_gb": 150,
         "peak_device_gb": round(peak / 1e9, 2),
-        "workload": "Poisson arrivals, 48 requests per rate: 60% 6000x4000 Bayer, 25% 8256x5504 Bayer, "
+        "workload": "Poisson arrivals, 64 requests per rate: 60% 6000x4000 Bayer, 25% 8256x5504 Bayer, "
                     "15% 6240x4160 X-Trans; defringe .5, axial .5, lateral .2, ACES .3; u16 out; "
-                    "latency = submit -> result in page-locked host memory; warm-up: every kind with every "
+                    "latency = submit -> result in page-locked host memory, overall and per request kind "
+                    "(bayer_6000x4000 is the 24 MP class); warm-up: every kind with every "
                     "option twice per lane before the timed rates",
     }
 

@@ -188,17 +188,23 @@ lre_status lre_dev_quantize_u16(lre_ctx* ctx, const float* in, uint16_t* out, si
  * (which synchronises the device), an application whose memory budget is
  * already committed.  It needs no lre_ctx.
  *
- * Arguments and arithmetic are those of lre_dev_ca_axial_cleanup (device
- * pointers; `in == out` allowed), enqueued on `cuda_stream` (NULL = legacy
- * default stream).  Its scratch (the max-G normaliser and, for in-place calls,
- * a copy of the input) is one file-scope device array sized for images of at
- * most 2,097,152 pixels (1920x1080 fits); larger images, radius > 16 or null
- * pointers return LRE_ERR_INVALID_ARGUMENT before any work.  Every GPU that
- * loads the library keeps the array (about 24 MiB) until the process exits.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  All calls share the one array: the
- * scratch is re-initialised by every call, but calls that overlap on the GPU
- * (different streams, or several host threads) race on it, so serialise them. */
+ * Arguments are those of lre_dev_ca_axial_cleanup (device pointers; `in ==
+ * out` allowed), enqueued on `cuda_stream` (NULL = legacy default stream),
+ * which must belong to the current device (else LRE_ERR_INVALID_ARGUMENT).
+ * It runs a different kernel (one fused tile pass instead of the two-pass
+ * stream), so its output matches lre_dev_ca_axial_cleanup's within the
+ * float-stage tolerance (max-abs 1e-4), not bit for bit.  Its scratch (the
+ * max-G normaliser and, for in-place calls, a copy of the input) is one
+ * file-scope device array sized for images of at most 2,097,152 pixels
+ * (1920x1080 and 2048x1024 fit); larger images, radius > 16 or null pointers
+ * return LRE_ERR_INVALID_ARGUMENT before any work.  Every GPU that loads the
+ * library keeps the array (about 24 MiB) until the process exits.  The first
+ * call on a device looks up the array's device address; make that first call
+ * before any stream capture.  All calls share the one array: the scratch is
+ * re-initialised by every call, but calls that overlap on the GPU (different
+ * streams, or several host threads) race on it, so serialise them.  A CUDA
+ * error already pending when it is called is left in place and reported as
+ * LRE_ERR_CUDA, with nothing enqueued. */
 lre_status lre_dev_ca_axial_cleanup_noalloc(const float* in, float* out, size_t width, size_t height,
                                             int radius, float epsilon, float strength,
                                             void* cuda_stream);

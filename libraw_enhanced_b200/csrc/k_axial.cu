@@ -844,9 +844,24 @@ extern "C" lre_status lre_dev_ca_axial_cleanup_noalloc(const float* in, float* o
   strength = fminf(fmaxf(strength, 0.f), 1.f);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
 
-  // One-time set-up per device: the device address of the scratch array.
+  // An error the caller's own earlier work left pending is theirs: report
+  // it without consuming it, and enqueue nothing.
+  if (cudaPeekAtLastError() != cudaSuccess) return LRE_ERR_CUDA;
+
+  // The scratch address below belongs to the current device, so the stream
+  // must be one of that device's streams (the legacy default stream is).
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return LRE_ERR_CUDA;
+  if (s != nullptr) {
+    int sdev = -1;
+    if (cudaStreamGetDevice(s, &sdev) != cudaSuccess) {
+      cudaGetLastError();
+      return LRE_ERR_INVALID_ARGUMENT;
+    }
+    if (sdev != dev) return LRE_ERR_INVALID_ARGUMENT;
+  }
+
+  // One-time set-up per device: the device address of the scratch array.
   float* base = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
@@ -863,15 +878,29 @@ extern "C" lre_status lre_dev_ca_axial_cleanup_noalloc(const float* in, float* o
   float* d_max = base;                 // cleared below on every call
   float* staging = base + kNoAllocHead;
 
+  // Any error from here on comes from this call's own work (none was pending
+  // on entry): take it off the error state and report it.
+  auto failed = [] {
+    if (cudaPeekAtLastError() == cudaSuccess) return false;
+    cudaGetLastError();
+    return true;
+  };
   const size_t n = w * h;
   k_noalloc_zero<<<1, 1, 0, s>>>(d_max);
+  if (failed()) return LRE_ERR_CUDA;
   k_noalloc_max_g<<<grid_for(n, 256, 148u * 4u), 256, 0, s>>>(in, n, d_max);
+  if (failed()) return LRE_ERR_CUDA;
   const float* src = in;
   if (in == out) {
-    if (cudaMemcpyAsync(staging, in, n * 3 * sizeof(float), cudaMemcpyDeviceToDevice, s) != cudaSuccess) return LRE_ERR_CUDA;
+    if (cudaMemcpyAsync(staging, in, n * 3 * sizeof(float), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+      cudaGetLastError();
+      return LRE_ERR_CUDA;
+    }
     src = staging;
   }
-  if (axial_dispatch(pick_tile(radius, 32), 512, w, h, s, src, out, radius, epsilon, strength, d_max) != cudaSuccess)
+  if (axial_dispatch(pick_tile(radius, 32), 512, w, h, s, src, out, radius, epsilon, strength, d_max) != cudaSuccess) {
+    cudaGetLastError();
     return LRE_ERR_CUDA;
-  return cudaGetLastError() == cudaSuccess ? LRE_OK : LRE_ERR_CUDA;
+  }
+  return LRE_OK;
 }

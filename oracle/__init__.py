@@ -131,12 +131,49 @@ def num_threads() -> int:
     return int(ref().ref_num_threads())
 
 
-def amaze(raw_sparse, filters, cam_mul=(2.0, 1.0, 1.5, 1.0), maximum=1.0):
+def amaze_tiles(h: int, w: int) -> int:
+    """Tiles of the reference AMaZE tile loop (core/cpu_accelerator.cpp:1244-1245):
+    160x160 tiles stepping by 128 from -16 in both directions."""
+    return len(range(-16, h, 128)) * len(range(-16, w, 128))
+
+
+def xtrans_tiles(h: int, w: int) -> int:
+    """Tiles of the reference X-Trans 3-pass tile loop (core/cpu_accelerator.cpp:1968-1969):
+    114x114 tiles stepping by 98 from 3 while below the size minus 19."""
+    return len(range(3, h - 19, 98)) * len(range(3, w - 19, 98))
+
+
+class _Threads:
+    """Temporarily run the reference with `n` OpenMP threads."""
+
+    def __init__(self, n):
+        self.n = n
+
+    def __enter__(self):
+        self.saved = num_threads()
+        if self.n:
+            set_threads(self.n)
+
+    def __exit__(self, *exc):
+        set_threads(self.saved)
+
+
+def amaze(raw_sparse, filters, cam_mul=(2.0, 1.0, 1.5, 1.0), maximum=1.0, fresh_tiles=False):
+    """The reference AMaZE (core/cpu_accelerator.cpp:1145-1653).
+
+    The reference allocates its tile scratch once per OpenMP thread
+    (:1217-1218) and never fills the apron corners of tiles that touch two
+    image edges (:1326), so those cells hold what the thread's previous tile
+    left.  ``fresh_tiles=True`` runs one thread per tile (the static
+    ``omp for`` then gives every thread exactly one tile), so every tile
+    starts from a zero-filled buffer and the result is a function of the
+    input alone -- the semantics the CUDA path implements."""
     raw = _img(raw_sparse)
     h, w, _ = raw.shape
     out = np.zeros_like(raw)
     cm = np.asarray(cam_mul, dtype=np.float32)
-    ok = ref().ref_demosaic_bayer_amaze(_ptr(raw), _ptr(out), w, h, int(filters), _ptr(cm), float(maximum))
+    with _Threads(amaze_tiles(h, w) if fresh_tiles else 0):
+        ok = ref().ref_demosaic_bayer_amaze(_ptr(raw), _ptr(out), w, h, int(filters), _ptr(cm), float(maximum))
     assert ok
     return out
 
@@ -170,7 +207,26 @@ def bayer_dcb(raw_sparse, filters, maximum=1.0, iterations=1, enhance=True, thre
 
 
 REF_HL_SO = os.path.join(HERE, "_ref", "liblre_ref_hl.so")
+REF_DT_SO = os.path.join(HERE, "_ref", "liblre_ref_dt.so")
 _ref_hl = None
+_ref_dt = None
+
+
+def ref_detail_tonemap(img):
+    """The reference's detail-preserving tone map, compiled from its own lines
+    (core/libraw_wrapper.cpp:45-116 box_filter_normalized and :1389-1471
+    aces_tone_map_scalar + apply_detail_preserving_tonemap) into
+    oracle/_ref/liblre_ref_dt.so.  Returns the tone-mapped copy."""
+    global _ref_dt
+    if _ref_dt is None:
+        if not os.path.exists(REF_DT_SO):
+            raise FileNotFoundError(f"oracle library missing: {REF_DT_SO} (run `make -C oracle ref`)")
+        _ref_dt = C.CDLL(REF_DT_SO)
+        _ref_dt.ref_detail_tonemap.restype = C.c_int
+        _ref_dt.ref_detail_tonemap.argtypes = [_p, _sz, _sz]
+    a = _img(img).copy()
+    _ref_dt.ref_detail_tonemap(_ptr(a), a.shape[1], a.shape[0])
+    return a
 
 
 def recover_highlights(rgb, saturation_threshold, want_mask=False, wb_rgb=None):
@@ -206,13 +262,21 @@ def bayer_aahd(raw_sparse, filters, maximum=1.0, threads=1):
     return out
 
 
-def xtrans(raw_sparse, xtrans_pattern, passes=3, maximum=1.0, color_matrix=None):
+def xtrans(raw_sparse, xtrans_pattern, passes=3, maximum=1.0, color_matrix=None, fresh_tiles=False):
+    """The reference X-Trans demosaic (core/cpu_accelerator.cpp:1870-2762).
+
+    The 3-pass tile buffers are allocated once per OpenMP thread (:1953-1959)
+    and the homogeneity maps of edge tiles read cells their tile never
+    writes; ``fresh_tiles=True`` runs one thread per tile so that every tile
+    starts from zero-filled buffers (see :func:`amaze`)."""
     raw = _img(raw_sparse)
     h, w, _ = raw.shape
     out = np.zeros_like(raw)
     cm = np.zeros(12, np.float32) if color_matrix is None else np.asarray(color_matrix, np.float32).reshape(12)
     xt = _xt(xtrans_pattern)
-    ok = ref().ref_demosaic_xtrans(_ptr(raw), _ptr(out), w, h, _ptr(xt), _ptr(cm), float(maximum), int(passes))
+    n = xtrans_tiles(h, w) if (fresh_tiles and passes != 1) else 0
+    with _Threads(n):
+        ok = ref().ref_demosaic_xtrans(_ptr(raw), _ptr(out), w, h, _ptr(xt), _ptr(cm), float(maximum), int(passes))
     assert ok
     return out
 

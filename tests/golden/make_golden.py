@@ -2,9 +2,11 @@
 
     make -C oracle && python tests/golden/make_golden.py
 
-Every output is produced by uniuyuni/libraw_enhanced's own CPU accelerator
-(compiled from the reference sources into oracle/_ref/liblre_ref.so) or, for
-the LibRaw-dependent pieces, by the oracle's C restatement.  Inputs are small
+Every output is produced by uniuyuni/libraw_enhanced's own code: its CPU
+accelerator (compiled from the reference sources into
+oracle/_ref/liblre_ref.so), its detail-preserving tone map (the reference's
+own lines compiled into oracle/_ref/liblre_ref_dt.so) or, for the
+LibRaw-dependent integer pieces, the oracle's C restatement.  Inputs are small
 seeded synthetic scenes and are stored beside the outputs, so the fixtures do
 not depend on the scene generator staying unchanged.
 """
@@ -36,7 +38,7 @@ def main():
     out["defringe_green_s4"] = oracle.defringe(rgb, strength=4.0, green=True)
     out["axial"] = oracle.axial_ca(rgb)
     out["tone"] = oracle.tone_mapping(rgb, 1.0)
-    out["detail"] = oracle.detail_tonemap(rgb)
+    out["detail"] = oracle.ref_detail_tonemap(rgb)
     out["micro"] = oracle.micro_contrast(rgb, 0.6, 8.0, 0.04)
     lat_in = scenes.radial_ca(scenes.scene_rgb(h, w, 102), 1.004, 0.996)
     out["lateral_in"] = lat_in

@@ -107,6 +107,32 @@ def test_reference_build_reproduces_golden(gold, key, fn):
     assert np.array_equal(got, gold[key]), key
 
 
+needs_ref_dt = pytest.mark.skipif(not os.path.exists(oracle.REF_DT_SO), reason="oracle/_ref not built (make -C oracle)")
+
+
+@needs_ref_dt
+def test_detail_tonemap_reference_lines_reproduce_golden(gold):
+    """The golden `detail` vector is written by the reference's own lines
+    (core/libraw_wrapper.cpp:45-116, :1389-1471 compiled into
+    oracle/_ref/liblre_ref_dt.so); rebuilding them reproduces it."""
+    assert np.array_equal(oracle.ref_detail_tonemap(gold["amaze_rggb"]), gold["detail"])
+
+
+@needs_ref_dt
+@pytest.mark.parametrize("threads", [1, 3, 8])
+def test_detail_tonemap_restatement_matches_reference_lines(threads):
+    """The C restatement of the detail tone map equals the reference's own
+    compiled lines bit for bit, at several OpenMP thread counts (the
+    reference's sliding box sums run per row / per column, so its result does
+    not depend on the thread split)."""
+    img = np.random.default_rng(40).random((83, 131, 3), dtype=np.float32) * np.float32(1.3)
+    oracle.set_threads(threads)
+    try:
+        assert np.array_equal(oracle.detail_tonemap(img), oracle.ref_detail_tonemap(img))
+    finally:
+        oracle.set_threads(4)
+
+
 def test_restatement_reproduces_golden(gold):
     assert np.array_equal(oracle.detail_tonemap(gold["amaze_rggb"]), gold["detail"])
     assert np.array_equal(oracle.quantize_u16(gold["tone"]), gold["u16"])
@@ -136,3 +162,66 @@ def test_reference_dcb_flat_field_and_thread_dependence():
     a = oracle.bayer_dcb(sp, f, 4095.0, threads=1)
     b = oracle.bayer_dcb(sp, f, 4095.0, threads=1)
     assert np.array_equal(a, b) and np.isfinite(a).all()
+
+
+@needs_ref
+def test_reference_amaze_depends_on_thread_split_only_in_stale_cells():
+    """The reference AMaZE is not a function of its input near image corners:
+    its tile scratch is allocated once per OpenMP thread
+    (core/cpu_accelerator.cpp:1217-1218) and the apron corners of tiles that
+    touch two image edges are never filled (:1326).  Between thread splits
+    the output moves inside tests._util.amaze_stale_mask and nowhere else;
+    with one thread per tile (every tile starts from a zeroed buffer, the
+    semantics the CUDA path implements) the result is reproducible."""
+    from tests._util import amaze_stale_mask
+
+    h, w = 1024, 1536
+    sp = scenes.sparse_rgb(scenes.bayer_scene(h, w, 1), "RGGB")
+    f = scenes.FILTERS["RGGB"]
+    saved = oracle.num_threads()
+    try:
+        outs = {}
+        for t in (1, 9, oracle.amaze_tiles(h, w)):
+            oracle.set_threads(t)
+            outs[t] = oracle.amaze(sp, f, WB, 1.0)
+        fresh = oracle.amaze(sp, f, WB, 1.0, fresh_tiles=True)
+    finally:
+        oracle.set_threads(saved)
+    stale = amaze_stale_mask(h, w)
+    assert np.array_equal(fresh, outs[oracle.amaze_tiles(h, w)])
+    moved_anywhere = False
+    for t in (1, 9):
+        d = np.abs(outs[t] - fresh).max(axis=2)
+        assert d[~stale].max() == 0.0, t
+        moved_anywhere |= bool(d[stale].max() > 0)
+    assert moved_anywhere  # the thread split does change the stale cells
+
+
+@needs_ref
+def test_reference_xtrans_depends_on_thread_split_only_in_frame():
+    """The reference X-Trans 3-pass reads per-thread tile buffers
+    (core/cpu_accelerator.cpp:1953-1959) in cells its edge tiles never write,
+    so the thread split moves the output within 12 px of the image edge and
+    nowhere else; one thread per tile makes it reproducible."""
+    h, w = 240, 360
+    rgb = scenes.scene_rgb(h, w, 21)
+    sp = scenes.sparse_rgb(scenes.mosaic(rgb, scenes.XTRANS_STD, (1.8, 1.0, 1.6, 1.0), 21), scenes.XTRANS_STD)
+    saved = oracle.num_threads()
+    try:
+        outs = {}
+        for t in (1, 4):
+            oracle.set_threads(t)
+            outs[t] = oracle.xtrans(sp, scenes.XTRANS_STD, 3)
+        fresh = oracle.xtrans(sp, scenes.XTRANS_STD, 3, fresh_tiles=True)
+        fresh2 = oracle.xtrans(sp, scenes.XTRANS_STD, 3, fresh_tiles=True)
+    finally:
+        oracle.set_threads(saved)
+    assert np.array_equal(fresh, fresh2)
+    inner = np.zeros((h, w), bool)
+    inner[12:-12, 12:-12] = True
+    moved = False
+    for t in (1, 4):
+        d = np.abs(outs[t] - fresh).max(axis=2)
+        assert d[inner].max() == 0.0, t
+        moved |= bool(d[~inner].max() > 0)
+    assert moved
