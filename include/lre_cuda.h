@@ -85,6 +85,18 @@ lre_status lre_host_free(lre_ctx* ctx, void* p);
  * device operation on this context fails with LRE_ERR_INJECTED before any
  * work is enqueued (0 disables).  Never touches the GPU. */
 void lre_inject_fault(lre_ctx* ctx, int countdown);
+/* Bound of every device-side wait of the in-order sweeps (DCB, AAHD,
+ * highlight recovery: a band waits for the band above to publish its
+ * columns), in SM clock cycles; cycles <= 0 restores the default (~2 s).
+ * A wait that runs out sets an error flag, stops waiting and lets the kernel
+ * finish; the call then returns LRE_ERR_TIMEOUT and the context stays
+ * usable.  No counterpart in the reference (its loops run on the CPU). */
+lre_status lre_set_wait_limit(lre_ctx* ctx, long long cycles);
+/* Host-side fault injection for the bounded waits: in the next in-order
+ * sweep, band `band` (32 rows each, from the top) never publishes its
+ * progress -- a message that is dropped -- so the band below it waits until
+ * its bound runs out.  One-shot; band < 0 clears it.  No device fault. */
+void lre_inject_sweep_stall(lre_ctx* ctx, int band);
 
 /* ------------------------------------------------ stages, host buffers */
 /* GPUAccelerator::demosaic_bayer_amaze (core/gpu_accelerator.h:35-39;
@@ -353,6 +365,62 @@ lre_status lre_dev_output_epilogue(lre_ctx* ctx, const float* in, void* out, siz
                                    size_t height, const float transform[12], float gamma_power,
                                    float gamma_slope, int output_color_space, int bits);
 
+/* ------------------------------------------------------ white balance */
+/* The inputs of LibRaw's white-balance multiplier derivation, as the
+ * reference's scale_colors reads them (core/libraw_wrapper.cpp:602-845):
+ * imgdata.params, imgdata.color and imgdata.idata fields. */
+typedef struct lre_wb_inputs {
+  float user_mul[4];               /* params.user_mul; user_mul[0] != 0 replaces pre_mul */
+  float pre_mul[4];                /* color.pre_mul (daylight multipliers)              */
+  float cam_mul[4];                /* color.cam_mul (as-shot multipliers)               */
+  unsigned short white[8][8];      /* color.white                                       */
+  unsigned cblack[4];              /* color.cblack[0..3]                                */
+  int use_auto_wb;                 /* params.use_auto_wb                                */
+  int use_camera_wb;               /* params.use_camera_wb                              */
+  int camerawb_fallback_to_daylight; /* rawparams.options has
+                                      LIBRAW_RAWOPTIONS_CAMERAWB_FALLBACK_TO_DAYLIGHT   */
+  int as_shot_wb_applied;          /* color.as_shot_wb_applied                          */
+  int colors;                      /* idata.colors                                      */
+  int no_auto_scale;               /* params.no_auto_scale: multipliers all 1           */
+} lre_wb_inputs;
+
+/* What the derivation produces. */
+typedef struct lre_wb_result {
+  float scale_mul[4];  /* the multipliers apply_white_balance uses (effective_wb)   */
+  float pre_mul[4];    /* color.pre_mul after the derivation                       */
+  unsigned maximum;    /* color.maximum - color.black (scale_colors' unsigned update) */
+  int auto_wb;         /* 1: the grey-world (auto-WB) branch ran                    */
+  int bad_camera_wb;   /* 1: LibRaw would raise LIBRAW_WARN_BAD_CAMERA_WB           */
+} lre_wb_result;
+
+/* 1 when `in` selects the grey-world (auto-WB) branch, which needs the
+ * per-channel sums of the black-subtracted image; 0 otherwise.  Replaces
+ * should_use_auto_wb in core/libraw_wrapper.cpp:623-632. */
+int lre_wb_needs_channel_sums(const lre_wb_inputs* in);
+
+/* scale_colors' multiplier logic (core/libraw_wrapper.cpp:612-845: user
+ * multipliers, auto-WB, camera WB from color.white, the Nikon sRAW daylight
+ * case, pre_mul[1]/[3] defaults, maximum -= black, normalisation by the
+ * smallest multiplier) on the host, bit-exact.  `channel_sums` /
+ * `channel_counts` are the per-native-colour (0..3) sums and counts of the
+ * uint16[4] image (lre_channel_sums); they are read only when
+ * lre_wb_needs_channel_sums(in) is 1 and may be NULL otherwise
+ * (LRE_ERR_INVALID_ARGUMENT if needed and NULL).  No device work. */
+lre_status lre_wb_multipliers(const lre_wb_inputs* in, uint32_t filters, unsigned maximum, unsigned black,
+                              const uint64_t channel_sums[4], const uint64_t channel_counts[4],
+                              lre_wb_result* out);
+/* The grey-world statistics of the auto-WB branch (core/libraw_wrapper.cpp:
+ * 632-661): for each native colour c (fcol_xtrans, or fcol_bayer_native
+ * 0..3), the sum of image[i][c] over the sites of colour c and their count,
+ * as exact 64-bit integers (the reference's double sums of 16-bit values
+ * are exact below 2^53).  `raw4` is width*height uint16[4] pixels in host
+ * memory (lre_channel_sums) or device memory (lre_dev_channel_sums); both
+ * return after the sums are in host memory. */
+lre_status lre_channel_sums(lre_ctx* ctx, const uint16_t* raw4, size_t width, size_t height, uint32_t filters,
+                            const char xtrans[36], uint64_t sums[4], uint64_t counts[4]);
+lre_status lre_dev_channel_sums(lre_ctx* ctx, const uint16_t* raw4, size_t width, size_t height,
+                                uint32_t filters, const char xtrans[36], uint64_t sums[4], uint64_t counts[4]);
+
 /* ------------------------------------------------------ on-device ingest */
 /* The LibRaw-side frame description the raw ingest reads (imgdata.sizes and
  * imgdata.color fields, plus the pipeline's WB and adjust_maximum inputs). */
@@ -371,6 +439,11 @@ typedef struct lre_raw_frame {
   float wb[4];                    /* effective WB multipliers (scale_colors)           */
   float adjust_maximum_thr;       /* params.adjust_maximum_thr; 0: keep `maximum`       */
   float data_maximum;             /* color.data_maximum; 0: scanned on the device       */
+  int derive_wb;                  /* 1: derive the WB multipliers from wb_in as the
+                                     pipeline's scale_colors does (after black level and
+                                     green matching; wb[] is then ignored, and adjust_maximum
+                                     compares against maximum - black); 0: use wb[]       */
+  lre_wb_inputs wb_in;            /* scale_colors inputs when derive_wb == 1              */
 } lre_raw_frame;
 
 /* raw2image (core/libraw_wrapper.cpp:2299-2438, copy_bayer_image standard
@@ -386,7 +459,9 @@ lre_status lre_green_matching(lre_ctx* ctx, uint16_t* raw4, size_t width, size_t
                               uint32_t filters, unsigned maximum);
 /* process_raw_to_rgb from the decoded raw_image to the developed image
  * (core/libraw_wrapper.cpp:1477-1853 order): raw2image, black level, green
- * matching, white balance, adjust_maximum, then the develop chain of
+ * matching, the WB multipliers (frame->derive_wb: derived on the device and
+ * host as scale_colors does; else frame->wb), white balance,
+ * adjust_maximum, then the develop chain of
  * `params` (its filters/xtrans/maximum_value are taken from the frame and
  * the adopted maximum).  The frame crosses PCIe as 16-bit samples.
  * *maximum_used (may be NULL) receives the maximum handed to the demosaic. */

@@ -48,6 +48,9 @@ __all__ = [
     "Server",
     "develop_params",
     "raw_frame",
+    "wb_inputs",
+    "wb_multipliers",
+    "wb_needs_channel_sums",
 ]
 
 # LibRaw `filters` words of the four Bayer layouts.
@@ -152,6 +155,14 @@ class CudaAccelerator:
     def inject_fault(self, countdown: int) -> None:
         """Host-side fault injection: the countdown-th next call fails."""
         self._lib.lre_inject_fault(self._h, int(countdown))
+
+    def set_wait_limit(self, cycles: int = 0) -> None:
+        """Bound of the in-order sweeps' device-side waits in SM cycles (0: default ~2 s)."""
+        self._check(self._lib.lre_set_wait_limit(self._h, int(cycles)))
+
+    def inject_sweep_stall(self, band: int) -> None:
+        """Fault injection: in the next in-order sweep, `band` never reports progress."""
+        self._lib.lre_inject_sweep_stall(self._h, int(band))
 
     # ------------------------------------------------------------ stages (host)
     def demosaic_bayer_amaze(self, raw_rgb, filters: int, cam_mul=(1.0, 1.0, 1.0, 1.0), maximum_value: float = 1.0):
@@ -417,6 +428,25 @@ class CudaAccelerator:
         self._check(self._lib.lre_raw2image(self._h, _ptr(r), C.byref(frame), _ptr(out)))
         return out
 
+    def channel_sums(self, raw4, filters: int, xtrans=None):
+        """Per-native-colour sums and counts of a uint16 (H, W, 4) image
+        (the auto-WB statistics of scale_colors), reduced on the device."""
+        a = np.ascontiguousarray(raw4, dtype=np.uint16)
+        sums = np.zeros(4, np.uint64)
+        counts = np.zeros(4, np.uint64)
+        self._check(self._lib.lre_channel_sums(self._h, _ptr(a), a.shape[1], a.shape[0], int(filters),
+                                               _xtrans_bytes(xtrans), _ptr(sums), _ptr(counts)))
+        return sums, counts
+
+    def scale_colors(self, raw4, filters: int, inputs, maximum: int, black: int, xtrans=None) -> dict:
+        """scale_colors' multipliers for a black-subtracted uint16 (H, W, 4)
+        image: the channel sums on the device when auto-WB needs them, then
+        :func:`wb_multipliers`."""
+        if wb_needs_channel_sums(inputs) and not inputs.no_auto_scale:
+            sums, counts = self.channel_sums(raw4, filters, xtrans)
+            return wb_multipliers(inputs, filters, maximum, black, sums, counts)
+        return wb_multipliers(inputs, filters, maximum, black)
+
     def green_matching(self, raw4, filters: int, maximum: int):
         a = np.ascontiguousarray(raw4, dtype=np.uint16).copy()
         self._check(self._lib.lre_green_matching(self._h, _ptr(a), a.shape[1], a.shape[0], int(filters), int(maximum)))
@@ -588,10 +618,59 @@ class Server:
         return a.value, b.value
 
 
+def wb_inputs(user_mul=(0.0, 0.0, 0.0, 0.0), pre_mul=(1.0, 1.0, 1.0, 1.0), cam_mul=(0.0, 0.0, 0.0, 0.0),
+              white=None, cblack=(0, 0, 0, 0), use_auto_wb=False, use_camera_wb=False,
+              camerawb_fallback_to_daylight=False, as_shot_wb_applied=False, colors=3,
+              no_auto_scale=False) -> "_lib.WbInputs":
+    """The imgdata fields LibRaw's scale_colors reads to choose the WB
+    multipliers (core/libraw_wrapper.cpp:602-845)."""
+    w = _lib.WbInputs()
+    for i in range(4):
+        w.user_mul[i] = float(user_mul[i])
+        w.pre_mul[i] = float(pre_mul[i])
+        w.cam_mul[i] = float(cam_mul[i])
+        w.cblack[i] = int(cblack[i])
+    if white is not None:
+        wh = np.asarray(white, dtype=np.uint16).reshape(8, 8)
+        for r in range(8):
+            for c in range(8):
+                w.white[r][c] = int(wh[r, c])
+    w.use_auto_wb, w.use_camera_wb = int(bool(use_auto_wb)), int(bool(use_camera_wb))
+    w.camerawb_fallback_to_daylight = int(bool(camerawb_fallback_to_daylight))
+    w.as_shot_wb_applied, w.colors, w.no_auto_scale = int(bool(as_shot_wb_applied)), int(colors), int(bool(no_auto_scale))
+    return w
+
+
+def wb_multipliers(inputs: "_lib.WbInputs", filters: int, maximum: int, black: int, channel_sums=None,
+                   channel_counts=None) -> dict:
+    """scale_colors' multiplier logic (host, bit-exact): returns scale_mul,
+    pre_mul, maximum - black, and the auto-WB / bad-camera-WB flags.  The
+    channel sums (:meth:`CudaAccelerator.channel_sums`) are needed only when
+    the inputs select auto-WB."""
+    lib = _lib.load()
+    r = _lib.WbResult()
+    sp = cp = None
+    if channel_sums is not None:
+        sums = np.ascontiguousarray(channel_sums, dtype=np.uint64)
+        counts = np.ascontiguousarray(channel_counts, dtype=np.uint64)
+        sp, cp = _ptr(sums), _ptr(counts)
+    st = lib.lre_wb_multipliers(C.byref(inputs), int(filters), int(maximum), int(black), sp, cp, C.byref(r))
+    if st != _lib.LRE_OK:
+        raise LibRawError(st, "wb_multipliers: the inputs select auto-WB, which needs the channel sums")
+    return {"scale_mul": np.array(r.scale_mul, np.float32), "pre_mul": np.array(r.pre_mul, np.float32),
+            "maximum": int(r.maximum), "auto_wb": bool(r.auto_wb), "bad_camera_wb": bool(r.bad_camera_wb)}
+
+
+def wb_needs_channel_sums(inputs: "_lib.WbInputs") -> bool:
+    return bool(_lib.load().lre_wb_needs_channel_sums(C.byref(inputs)))
+
+
 def raw_frame(raw_width, raw_height, width, height, filters, raw_pitch=None, top_margin=0, left_margin=0,
               shrink=0, xtrans=None, cblack=(), black=0, maximum=65535, green_matching=0, wb=(1.0, 1.0, 1.0, 1.0),
-              adjust_maximum_thr=0.0, data_maximum=0.0) -> "_lib.RawFrame":
-    """A LibRaw-style frame description for the raw ingest entry points."""
+              adjust_maximum_thr=0.0, data_maximum=0.0, wb_in=None) -> "_lib.RawFrame":
+    """A LibRaw-style frame description for the raw ingest entry points.
+    With ``wb_in`` (:func:`wb_inputs`) the develop derives the WB multipliers
+    on the device as scale_colors does and ``wb`` is ignored."""
     f = _lib.RawFrame()
     f.raw_width, f.raw_height = int(raw_width), int(raw_height)
     f.raw_pitch = int(raw_pitch if raw_pitch is not None else 2 * raw_width)
@@ -610,6 +689,9 @@ def raw_frame(raw_width, raw_height, width, height, filters, raw_pitch=None, top
         f.wb[i] = float(v)
     f.adjust_maximum_thr = float(adjust_maximum_thr)
     f.data_maximum = float(data_maximum)
+    if wb_in is not None:
+        f.derive_wb = 1
+        f.wb_in = wb_in
     return f
 
 

@@ -70,6 +70,32 @@ class DevelopParams(C.Structure):
     ]
 
 
+class WbInputs(C.Structure):
+    _fields_ = [
+        ("user_mul", C.c_float * 4),
+        ("pre_mul", C.c_float * 4),
+        ("cam_mul", C.c_float * 4),
+        ("white", (C.c_ushort * 8) * 8),
+        ("cblack", C.c_uint * 4),
+        ("use_auto_wb", C.c_int),
+        ("use_camera_wb", C.c_int),
+        ("camerawb_fallback_to_daylight", C.c_int),
+        ("as_shot_wb_applied", C.c_int),
+        ("colors", C.c_int),
+        ("no_auto_scale", C.c_int),
+    ]
+
+
+class WbResult(C.Structure):
+    _fields_ = [
+        ("scale_mul", C.c_float * 4),
+        ("pre_mul", C.c_float * 4),
+        ("maximum", C.c_uint),
+        ("auto_wb", C.c_int),
+        ("bad_camera_wb", C.c_int),
+    ]
+
+
 class RawFrame(C.Structure):
     _fields_ = [
         ("raw_width", C.c_size_t),
@@ -89,6 +115,8 @@ class RawFrame(C.Structure):
         ("wb", C.c_float * 4),
         ("adjust_maximum_thr", C.c_float),
         ("data_maximum", C.c_float),
+        ("derive_wb", C.c_int),
+        ("wb_in", WbInputs),
     ]
 
 
@@ -158,6 +186,8 @@ SIGNATURES = {
     "lre_host_alloc": (_st, [_p, _sz, C.POINTER(_p)]),
     "lre_host_free": (_st, [_p, _p]),
     "lre_inject_fault": (None, [_p, _i]),
+    "lre_set_wait_limit": (_st, [_p, C.c_longlong]),
+    "lre_inject_sweep_stall": (None, [_p, _i]),
     "lre_demosaic_bayer_amaze": (_st, [_p, _p, _p, _sz, _sz, C.c_uint32, _p, _f]),
     "lre_demosaic_xtrans_1pass": (_st, [_p, _p, _p, _sz, _sz, _p, _p, _f]),
     "lre_demosaic_xtrans_3pass": (_st, [_p, _p, _p, _sz, _sz, _p, _p, _f]),
@@ -203,6 +233,10 @@ SIGNATURES = {
     "lre_green_matching": (_st, [_p, _p, _sz, _sz, C.c_uint32, C.c_uint]),
     "lre_develop_raw": (_st, [_p, _p, C.POINTER(RawFrame), _p, C.POINTER(DevelopParams), C.POINTER(_f)]),
     "lre_dev_develop_raw": (_st, [_p, _p, C.POINTER(RawFrame), _p, C.POINTER(DevelopParams), C.POINTER(_f)]),
+    "lre_wb_needs_channel_sums": (_i, [C.POINTER(WbInputs)]),
+    "lre_wb_multipliers": (_st, [C.POINTER(WbInputs), C.c_uint32, C.c_uint, C.c_uint, _p, _p, C.POINTER(WbResult)]),
+    "lre_channel_sums": (_st, [_p, _p, _sz, _sz, C.c_uint32, _p, _p, _p]),
+    "lre_dev_channel_sums": (_st, [_p, _p, _sz, _sz, C.c_uint32, _p, _p, _p]),
     "lre_set_tuning": (_st, [_p, C.POINTER(Tuning)]),
     "lre_get_tuning": (_st, [_p, C.POINTER(Tuning)]),
     "lre_batch_create": (_st, [C.POINTER(BatchConfig), C.POINTER(_p)]),

@@ -235,4 +235,16 @@ void lre_inject_fault(lre_ctx* ctx, int countdown) {
   if (c) c->inject_countdown = countdown > 0 ? countdown : 0;
 }
 
+lre_status lre_set_wait_limit(lre_ctx* ctx, long long cycles) {
+  Context* c = reinterpret_cast<Context*>(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  c->sweep_wait_cycles = cycles > 0 ? cycles : 0;
+  return LRE_OK;
+}
+
+void lre_inject_sweep_stall(lre_ctx* ctx, int band) {
+  Context* c = reinterpret_cast<Context*>(ctx);
+  if (c) c->sweep_hold_band = band >= 0 ? band : -1;
+}
+
 }  // extern "C"

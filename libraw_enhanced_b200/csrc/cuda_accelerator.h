@@ -118,8 +118,9 @@ class CudaAccelerator {
     if (!same(in, out)) return bad("convert_color_space: buffer size mismatch");
     return ok(lre_convert_color_space(ctx_, f(in), f(out), in.width, in.height, &transform[0][0]));
   }
-  bool gamma_correct(const ImageBufferFloat& in, ImageBufferFloat& out, float gamma_power, float gamma_slope,
-                     int output_color_space) {
+  // defaults as GPUAccelerator::gamma_correct (core/gpu_accelerator.h:70-74)
+  bool gamma_correct(const ImageBufferFloat& in, ImageBufferFloat& out, float gamma_power = 0.f,
+                     float gamma_slope = 0.f, int output_color_space = 1) {
     if (!same(in, out)) return bad("gamma_correct: buffer size mismatch");
     return ok(lre_gamma_correct(ctx_, f(in), f(out), in.width, in.height, gamma_power, gamma_slope, output_color_space));
   }

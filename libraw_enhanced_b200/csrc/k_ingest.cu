@@ -243,8 +243,18 @@ lre_status develop_raw_device(Context* c, const uint16_t* d_raw, const lre_raw_f
   LRE_TRY(lre::launch_raw2image(c, d_raw, f, img4));
   LRE_TRY(lre::launch_black_level(c, img4, iw, ih, f.cblack, 6 + (size_t)f.cblack[4] * f.cblack[5], f.black, f.maximum));
   if (f.green_matching) LRE_TRY(lre::launch_green_matching(c, img4, copy, iw, ih, f.filters, f.maximum));
-  LRE_TRY(lre::launch_wb_dense(c, img4, dense, iw, ih, f.wb, f.filters, f.xtrans));
+  // scale_colors (core/libraw_wrapper.cpp:1545-1553) sits between green
+  // matching and the white balance; it also lowers color.maximum by black,
+  // which adjust_maximum then compares against
+  float wb[4] = {f.wb[0], f.wb[1], f.wb[2], f.wb[3]};
   float maximum = (float)f.maximum;
+  if (f.derive_wb) {
+    lre_wb_result r;
+    LRE_TRY(lre::derive_wb_device(c, img4, iw, ih, f.filters, f.xtrans, f.maximum, f.black, f.wb_in, &r));
+    for (int k = 0; k < 4; k++) wb[k] = r.scale_mul[k];
+    maximum = (float)r.maximum;
+  }
+  LRE_TRY(lre::launch_wb_dense(c, img4, dense, iw, ih, wb, f.filters, f.xtrans));
   if (f.adjust_maximum_thr >= 0.00001f) {
     float real_max = f.data_maximum;
     if (real_max == 0.f) {

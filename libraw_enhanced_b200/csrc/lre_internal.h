@@ -82,6 +82,11 @@ struct Context {
   cudaEvent_t tail_ev[8] = {};  // rows of the final RGB ready for download
   std::mutex mu;               // one host-buffer call at a time per context
   int sm_count = 148;
+  // Bound of each device-side wait of the in-order sweeps, in SM clock
+  // cycles (0: the default, ~2 s), and a one-shot host-side fault injection:
+  // the next sweep's band `sweep_hold_band` never reports its progress.
+  long long sweep_wait_cycles = 0;
+  int sweep_hold_band = -1;
 };
 
 // Status helpers.
@@ -192,6 +197,14 @@ lre_status launch_wb_dense(Context* c, const uint16_t* raw4, float* dense, size_
                            uint32_t filters, const char* xtrans);
 lre_status launch_cfa_max_dense(Context* c, const float* dense, size_t w, size_t h, uint32_t filters,
                                 const char* xtrans, float* d_out);
+// scale_colors' multipliers (k_wb.cu): the auto-WB channel sums of the
+// device uint16[4] image when needed (synchronises), then the host logic.
+bool wb_needs_sums(const lre_wb_inputs& in);
+lre_status wb_multipliers(const lre_wb_inputs& in, uint32_t filters, unsigned maximum, unsigned black,
+                          const uint64_t* sums, const uint64_t* counts, lre_wb_result* out);
+lre_status derive_wb_device(Context* c, const uint16_t* d_raw4, size_t w, size_t h, uint32_t filters,
+                            const char* xtrans, unsigned maximum, unsigned black, const lre_wb_inputs& in,
+                            lre_wb_result* out);
 }  // namespace lre
 
 namespace lre {

@@ -65,6 +65,8 @@ struct SweepArgs {
   int* err;
   int* progress;  // per band: columns < progress[b] of band b are final in HBM
   const int* skip_if_zero;  // optional: every band returns at once when *skip_if_zero == 0
+  long long wait_cycles;    // bound of one wait for the band above (SM clock cycles)
+  int hold_ticket;          // fault injection: this band never publishes (-1: none)
 };
 
 // The sweep's shared-memory ring, addressed through the __shared__ symbol
@@ -100,7 +102,7 @@ __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
+constexpr long long kWaitCycles = 4000000000LL;  // default wait bound: ~2 s at 1.9 GHz
 
 __device__ __forceinline__ void cp_async4(float* s, const float* g) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(kSweepWarps * 32) k_gs_sweep(SweepArgs a) {
       const long long start = clock64();
       while ((above = ld_acquire(a.progress + ticket - NCH)) < need) {
         __nanosleep(32);
-        if (clock64() - start > kWaitCycles) {
+        if (clock64() - start > a.wait_cycles) {
           atomicExch(a.err, 1);
           ok = 0;
           break;
@@ -266,7 +268,7 @@ __global__ void __launch_bounds__(kSweepWarps * 32) k_gs_sweep(SweepArgs a) {
   auto publish = [&](int upto) {
     if (upto <= published) return;
     __syncwarp();
-    if (lane == 0) st_release(a.progress + ticket, upto > a.c_hi ? INT_MAX : upto);
+    if (lane == 0 && ticket != a.hold_ticket) st_release(a.progress + ticket, upto > a.c_hi ? INT_MAX : upto);
     published = upto;
   };
 
@@ -294,6 +296,11 @@ lre_status sweep(Context* c, const SweepArgs& base, int* sync, int nb_max, const
   SweepArgs a = base;
   a.ticket = sync;
   a.progress = sync + 64;
+  a.wait_cycles = c->sweep_wait_cycles > 0 ? c->sweep_wait_cycles : kWaitCycles;
+  // a held band (host-side fault injection, one sweep only) never reports
+  // its progress, so the band below it waits until its bound runs out
+  a.hold_ticket = c->sweep_hold_band >= 0 ? c->sweep_hold_band * Op::NCH : -1;
+  c->sweep_hold_band = -1;
   LRE_CUDA_TRY(c, cudaMemsetAsync(sync, 0, sizeof(int), c->stream));
   LRE_CUDA_TRY(c, cudaMemsetAsync(a.progress, 0, (size_t)nb * sizeof(int), c->stream));
   LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_gs_sweep<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R::BYTES));

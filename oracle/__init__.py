@@ -92,6 +92,8 @@ _PORT_SIGS = {
     "port_scale_mul": (None, [_p, C.c_int, _f, _p]),
     "port_auto_wb": (None, [_p, _sz, _sz, C.c_uint32, _p, _p]),
     "port_border_interpolate": (None, [_p, _sz, _sz, C.c_uint32, _sz]),
+    "port_scale_colors": (C.c_int, [_p, _sz, _sz, C.c_uint32, _p, _p, _p, _p, _p, _p, C.c_int, C.c_int,
+                                    C.POINTER(C.c_uint), C.c_uint, _p, _p]),
 }
 
 _ref = None
@@ -435,6 +437,29 @@ def auto_wb(raw4, filters, xtrans_pattern=None):
     out = np.empty(4, np.float32)
     port().port_auto_wb(_ptr(a), a.shape[1], a.shape[0], int(filters), _ptr(_xt(xtrans_pattern)), _ptr(out))
     return out
+
+
+def scale_colors(raw4, filters, xtrans_pattern=None, *, user_mul=(0, 0, 0, 0), pre_mul=(1, 1, 1, 1),
+                 cam_mul=(0, 0, 0, 0), white=None, cblack=(0, 0, 0, 0), colors=3, use_auto_wb=False,
+                 use_camera_wb=False, fallback_daylight=False, as_shot_wb_applied=False, no_auto_scale=False,
+                 maximum=16383, black=0):
+    """scale_colors' multiplier derivation (core/libraw_wrapper.cpp:602-845).
+    Returns (scale_mul[4], pre_mul[4], maximum - black, bad_camera_wb)."""
+    a = np.zeros((1, 1, 4), np.uint16) if raw4 is None else np.ascontiguousarray(raw4, dtype=np.uint16)
+    h, w = a.shape[:2]
+    f4 = lambda v: np.ascontiguousarray(np.asarray(v, np.float32).reshape(4))  # noqa: E731
+    um, pm, cm = f4(user_mul), f4(pre_mul), f4(cam_mul)
+    wh = np.zeros(64, np.uint16) if white is None else np.ascontiguousarray(np.asarray(white, np.uint16).reshape(64))
+    cb = np.ascontiguousarray(np.asarray(cblack, np.uint32).reshape(4))
+    flags = (int(bool(use_auto_wb)) | int(bool(use_camera_wb)) << 1 | int(bool(fallback_daylight)) << 2
+             | int(bool(as_shot_wb_applied)) << 3 | int(bool(no_auto_scale)) << 4)
+    mx = C.c_uint(int(maximum))
+    sm = np.empty(4, np.float32)
+    po = np.empty(4, np.float32)
+    warn = port().port_scale_colors(_ptr(a), w, h, int(filters), _ptr(_xt(xtrans_pattern)), _ptr(um), _ptr(pm),
+                                    _ptr(cm), _ptr(wh), _ptr(cb), int(colors), flags, C.byref(mx), int(black),
+                                    _ptr(sm), _ptr(po))
+    return sm, po, int(mx.value), bool(warn)
 
 
 def border_interpolate(rgb, filters, border=4):

@@ -249,6 +249,100 @@ void port_scale_mul(const float pre_mul_in[4], int colors, float maximum, float 
 }
 
 /*
+ * core/libraw_wrapper.cpp:602-845 (scale_colors), the whole multiplier
+ * derivation, in the reference's statement order and types:
+ *   :612-618  user_mul replaces pre_mul when user_mul[0] != 0;
+ *   :623-632  should_use_auto_wb;
+ *   :633-664  auto-WB from the raw image (double sums of the samples,
+ *             pow(., 1.0) identities, G2 folded into G);
+ *   :740-772  camera WB from the 8x8 white block (unsigned sums; the
+ *             white - cblack difference wraps as unsigned into an int);
+ *   :774-784  Nikon sRAW daylight division;
+ *   :786-792  pre_mul[1] / pre_mul[3] defaults;
+ *   :800      maximum -= black (unsigned);
+ *   :802-826  scale_mul = pre_mul / min(pre_mul) unless auto-WB ran;
+ * plus the pipeline's no_auto_scale override (:1545-1553).
+ * `raw4` (w*h uint16[4]) is read only when the auto-WB branch runs.
+ * flags: bit0 use_auto_wb, bit1 use_camera_wb, bit2 camera-WB fallback to
+ * daylight, bit3 as_shot_wb_applied, bit4 no_auto_scale.
+ * out: scale_mul[4], pre_mul[4]; *maximum_io is updated; returns 1 when the
+ * bad-camera-WB warning would be raised.
+ */
+int port_scale_colors(const uint16_t* raw4, size_t w, size_t h, uint32_t filters, const char xtrans[36],
+                      const float user_mul[4], const float pre_mul_in[4], const float cam_mul[4],
+                      const unsigned short white[64], const unsigned cblack[4], int colors, int flags,
+                      unsigned* maximum_io, unsigned black, float scale_mul[4], float pre_mul_out[4]) {
+  const int use_auto_wb = flags & 1, use_camera_wb = (flags >> 1) & 1, fallback = (flags >> 2) & 1;
+  const int as_shot = (flags >> 3) & 1, no_auto_scale = (flags >> 4) & 1;
+  float pre_mul[4];
+  int warn = 0;
+  memcpy(pre_mul, pre_mul_in, sizeof(pre_mul));
+  if (user_mul[0]) memcpy(pre_mul, user_mul, sizeof(pre_mul));
+  const int auto_wb = use_auto_wb || (use_camera_wb && (cam_mul[0] < -0.5 || (cam_mul[0] <= 0.00001f && !fallback)));
+  if (auto_wb) {
+    double p = 1.0;
+    double norm[4] = {0.0, 0.0, 0.0, 0.0};
+    double count[4] = {0.0, 0.0, 0.0, 0.0};
+    for (size_t row = 0; row < h; ++row)
+      for (size_t col = 0; col < w; ++col) {
+        unsigned cc = filters == 9 ? port_fcol_xtrans((unsigned)row, (unsigned)col, xtrans)
+                                   : port_fcol_bayer_native((unsigned)row, (unsigned)col, filters);
+        norm[cc] += pow(raw4[(row * w + col) * 4 + cc], p);
+        count[cc] += 1;
+      }
+    norm[1] += norm[3];
+    count[1] += count[3];
+    for (unsigned cc = 0; cc < 3; ++cc) norm[cc] = pow(norm[cc] / count[cc], 1.0 / p);
+    pre_mul[0] = norm[1] / norm[0];
+    pre_mul[1] = 1.0;
+    pre_mul[2] = norm[1] / norm[2];
+    pre_mul[3] = 1.0;
+  }
+  if (use_camera_wb && cam_mul[0] > 0.00001f) {
+    unsigned sum[8];
+    int val;
+    memset(sum, 0, sizeof(sum));
+    for (unsigned row = 0; row < 8; row++)
+      for (unsigned col = 0; col < 8; col++) {
+        unsigned c = port_fcol_bayer_native(row, col, filters);
+        if ((val = white[row * 8 + col] - cblack[c]) > 0) sum[c] += val;
+        sum[c + 4]++;
+      }
+    if (as_shot) {
+      pre_mul[0] = pre_mul[1] = pre_mul[2] = pre_mul[3] = 1.0;
+    } else if (sum[0] && sum[1] && sum[2] && sum[3]) {
+      for (unsigned c = 0; c < 4; c++) pre_mul[c] = (float)sum[c + 4] / sum[c];
+    } else if (cam_mul[0] > 0.00001f && cam_mul[2] > 0.00001f) {
+      memcpy(pre_mul, cam_mul, sizeof(pre_mul));
+    } else {
+      warn = 1;
+    }
+  }
+  if (as_shot && !use_camera_wb && !use_auto_wb && cam_mul[0] > 0.00001f && cam_mul[1] > 0.00001f &&
+      cam_mul[2] > 0.00001f)
+    for (unsigned c = 0; c < 3; c++) pre_mul[c] /= cam_mul[c];
+  if (pre_mul[1] == 0) pre_mul[1] = 1;
+  if (pre_mul[3] == 0) pre_mul[3] = colors < 4 ? pre_mul[1] : 1;
+  *maximum_io -= black;
+  if (!auto_wb) {
+    double dmin = 1.7976931348623157e308;
+    for (unsigned c = 0; c < 4; c++)
+      if (dmin > pre_mul[c]) dmin = pre_mul[c];
+    if (dmin > 0.00001 && *maximum_io > 0) {
+      for (unsigned c = 0; c < 4; c++) scale_mul[c] = pre_mul[c] / dmin;
+    } else {
+      for (unsigned c = 0; c < 4; c++) scale_mul[c] = 1.0;
+    }
+  } else {
+    for (unsigned c = 0; c < 4; c++) scale_mul[c] = pre_mul[c];
+  }
+  if (no_auto_scale)
+    for (unsigned c = 0; c < 4; c++) scale_mul[c] = 1.0;
+  memcpy(pre_mul_out, pre_mul, sizeof(pre_mul));
+  return warn;
+}
+
+/*
  * core/libraw_wrapper.cpp:632-661 (scale_colors, auto-WB branch, p = 1):
  * per-CFA-channel means of the uint16[4] samples, G2 folded into G,
  * pre_mul = (G/R, 1, G/B, 1).  Double accumulation as in the reference.

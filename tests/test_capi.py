@@ -73,3 +73,22 @@ def test_cpp_adapter_compiles_and_links(tmp_path):
     r = subprocess.run([cxx, "-std=c++17", "-I", ROOT, str(src), "-o", str(tmp_path / "adapter"), "-L", lib_dir,
                         "-l:liblre_cuda.so", "-Wl,-rpath," + lib_dir], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_cpp_adapter_compiles_against_reference_types(tmp_path):
+    """With LRE_USE_REFERENCE_TYPES the adapter takes libraw_enhanced's own
+    ImageBuffer / ImageBufferFloat (core/accelerator.h) -- the build a
+    maintainer makes inside the reference.  Compiles the device harness that
+    way (no device call is made here)."""
+    import shutil
+    import subprocess
+
+    ref = os.environ.get("LRE_REFERENCE_DIR") or os.path.join(os.path.dirname(ROOT), "reference")
+    if not os.path.exists(os.path.join(ref, "core", "accelerator.h")):
+        pytest.skip("reference checkout not present")
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    r = subprocess.run([cxx, "-std=c++17", "-fsyntax-only", "-DLRE_USE_REFERENCE_TYPES", "-I", os.path.join(ref, "core"),
+                        "-I", ROOT, os.path.join(ROOT, "tests", "adapter_harness.cpp")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -107,3 +107,24 @@ def test_dcb_rejects_non_bayer(lre, acc):
         assert ei.value.status == 1
     with pytest.raises(lre.LibRawError):
         acc.demosaic_bayer_dcb(sp, scenes.FILTERS["RGGB"], 1.0, iterations=-1)
+
+
+def test_sweep_wait_runs_out_and_context_recovers(lre, acc):
+    """The in-order sweeps' bounded wait, driven to its limit without any GPU
+    fault: host-side injection makes band 0 of the next sweep drop its
+    progress reports, so band 1 waits until a short bound (2e7 SM cycles,
+    ~10 ms) runs out, raises the error flag and finishes; the call returns
+    LRE_ERR_TIMEOUT.  The next call, with the default bound, is bit-exact."""
+    _, sp = _raw(128, 96, 45, "RGGB", 4095.0)  # 4 bands of 32 rows
+    f = scenes.FILTERS["RGGB"]
+    acc.set_wait_limit(20_000_000)
+    acc.inject_sweep_stall(0)
+    try:
+        with pytest.raises(lre.LibRawError) as e:
+            acc.demosaic_bayer_dcb(sp, f, 4095.0)
+        assert e.value.status == 5  # LRE_ERR_TIMEOUT
+    finally:
+        acc.set_wait_limit(0)
+        acc.inject_sweep_stall(-1)
+    got = acc.demosaic_bayer_dcb(sp, f, 4095.0)
+    assert np.array_equal(got, oracle.bayer_dcb(sp, f, 4095.0, threads=1))

@@ -101,3 +101,61 @@ def test_develop_raw_rejects_bad_frames(lre, acc):
     f = lre.raw_frame(40, 40, 40, 40, RGGB, top_margin=40)
     with pytest.raises(lre.LibRawError):
         acc.develop_raw(raw, f, lre.develop_params())
+
+
+@pytest.mark.parametrize("filters", [RGGB_G2, "xtrans"])
+def test_channel_sums_match_numpy(lre, acc, filters):
+    """The auto-WB statistics (core/libraw_wrapper.cpp:632-661) reduced on
+    the device: exact 64-bit sums and counts per native colour."""
+    rng = np.random.default_rng(21)
+    raw4 = rng.integers(0, 65536, size=(301, 517, 4), dtype=np.uint16)
+    xt = scenes.XTRANS_STD if filters == "xtrans" else None
+    filt = 9 if filters == "xtrans" else filters
+    sums, counts = acc.channel_sums(raw4, filt, xt)
+    idx = scenes.cfa_map(301, 517, xt if xt is not None else filt)
+    vals = np.take_along_axis(raw4.astype(np.uint64), idx[:, :, None], axis=2)[:, :, 0]
+    assert sums.tolist() == [int(vals[idx == c].sum()) for c in range(4)]
+    assert counts.tolist() == [int((idx == c).sum()) for c in range(4)]
+
+
+@pytest.mark.parametrize("mode", ["auto", "camera", "daylight"])
+def test_develop_raw_derives_wb_like_scale_colors(lre, acc, mode):
+    """develop_raw with frame.wb_in: the multipliers come from scale_colors'
+    logic (core/libraw_wrapper.cpp:602-845) after black level and green
+    matching, and adjust_maximum compares against maximum - black, as the
+    reference pipeline does (:1515-1575)."""
+    h, w = 256, 384
+    raw, rw, rh, pitch, top, left = _raw_from_scene(h, w, "RGGB", 14)
+    cblack = (10, 4, 12, 6, 0, 0)
+    black, maximum = 256, 16383
+    white = np.full((8, 8), 900, np.uint16)
+    white[::2, ::2] = 500  # R sites of RGGB
+    kw = {"auto": dict(use_auto_wb=True),
+          "camera": dict(use_camera_wb=True, cam_mul=(2.0, 1.0, 1.5, 0.0), white=white, cblack=cblack[:4]),
+          "daylight": dict(pre_mul=(2.2, 1.0, 1.4, 0.0))}[mode]
+    inputs = lre.wb_inputs(**kw)
+    f = lre.raw_frame(rw, rh, w, h, RGGB_G2, raw_pitch=pitch, top_margin=top, left_margin=left, cblack=cblack,
+                      black=black, maximum=maximum, green_matching=1, adjust_maximum_thr=0.75, wb_in=inputs)
+    p = lre.develop_params(cam_mul=(2.0, 1.0, 1.5, 1.0), defringe=1, axial_ca_correction=1, stage_order=1)
+    got, used = acc.develop_raw(raw, f, p)
+    # the reference's steps, restated on the CPU
+    img = oracle.raw2image(raw, pitch, top, left, w, h, RGGB_G2)
+    img = oracle.black_level(img, cblack, black, maximum)
+    img = oracle.green_matching(img, RGGB_G2, maximum)
+    okw = dict(kw)
+    if "cblack" in okw:
+        okw["cblack"] = tuple(okw["cblack"])
+    scale_mul, _, mx_after, _ = oracle.scale_colors(img, RGGB_G2, maximum=maximum, black=black, **okw)
+    sparse = oracle.port_white_balance(img, scale_mul, RGGB_G2)
+    adopted, _ = oracle.adjust_maximum(sparse, RGGB_G2, 0.75, 0.0, float(mx_after))
+    assert used == adopted
+    # the same multipliers through the standalone entry points
+    r = acc.scale_colors(img, RGGB_G2, inputs, maximum, black)
+    assert r["scale_mul"].view(np.uint32).tolist() == scale_mul.view(np.uint32).tolist()
+    ch = scenes.cfa_map(h, w, RGGB_G2)
+    ch = np.where(ch == 3, 1, ch)
+    dense = np.take_along_axis(sparse, ch[:, :, None], axis=2)[:, :, 0]
+    p.filters = RGGB_G2
+    p.maximum_value = adopted
+    ref = acc.develop(np.ascontiguousarray(dense), p)
+    assert np.array_equal(got, ref)
