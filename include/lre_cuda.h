@@ -444,13 +444,19 @@ typedef struct lre_raw_frame {
                                      green matching; wb[] is then ignored, and adjust_maximum
                                      compares against maximum - black); 0: use wb[]       */
   lre_wb_inputs wb_in;            /* scale_colors inputs when derive_wb == 1              */
+  int fuji_width;                 /* rawdata.ioparams.fuji_width; > 0 with a Bayer word:
+                                     Fuji SuperCCD honeycomb raw2image                    */
+  int fuji_layout;                /* unpacker_data.fuji_layout                           */
 } lre_raw_frame;
 
 /* raw2image (core/libraw_wrapper.cpp:2299-2438, copy_bayer_image standard
- * path and copy_xtrans_image): the uint16 raw_image into zero-initialised
- * uint16[4] pixels (ImageBuffer), each sample in its CFA channel, a Bayer
- * colour-3 sample also in channel 1; half-size frames keep the last sample
- * of each 2x2 cell per channel, as the reference's scan order does. */
+ * and Fuji honeycomb paths, copy_xtrans_image): the uint16 raw_image into
+ * zero-initialised uint16[4] pixels (ImageBuffer), each sample in its CFA
+ * channel, a Bayer colour-3 sample also in channel 1; half-size frames keep
+ * the last sample of each 2x2 cell per channel, as the reference's scan
+ * order does.  With frame->fuji_width > 0 and a Bayer filters word the raw
+ * rows and columns are mapped onto the 45-degree SuperCCD frame
+ * (:2342-2392). */
 lre_status lre_raw2image(lre_ctx* ctx, const uint16_t* raw_image, const lre_raw_frame* frame,
                          uint16_t* image4);
 /* apply_green_matching (core/libraw_wrapper.cpp:496-585), in place on
@@ -467,6 +473,20 @@ lre_status lre_green_matching(lre_ctx* ctx, uint16_t* raw4, size_t width, size_t
  * *maximum_used (may be NULL) receives the maximum handed to the demosaic. */
 lre_status lre_develop_raw(lre_ctx* ctx, const uint16_t* raw_image, const lre_raw_frame* frame,
                            void* out, const lre_develop_params* params, float* maximum_used);
+/* The Fuji SuperCCD rotate after demosaic (core/libraw_wrapper.cpp:1709-1750,
+ * use_fuji_rotate): the demosaiced width x height image, sampled bilinearly
+ * along the 45-degree grid, becomes *out_w x *out_h (wide = fuji_width' /
+ * sqrt(0.5), high = (height - fuji_width') / sqrt(0.5), fuji_width' =
+ * (fuji_width - 1 + shrink) >> shrink); pixels whose sample falls outside
+ * stay 0.  lre_fuji_rotate_size gives the output size (0 x 0 when the
+ * reference leaves the image unrotated).  `out` holds out_w * out_h * 3
+ * floats; host buffers for lre_fuji_rotate, device for lre_dev_fuji_rotate. */
+lre_status lre_fuji_rotate_size(int fuji_width, int shrink, size_t width, size_t height, size_t* out_w,
+                                size_t* out_h);
+lre_status lre_fuji_rotate(lre_ctx* ctx, const float* in, size_t width, size_t height, int fuji_width, int shrink,
+                           float* out);
+lre_status lre_dev_fuji_rotate(lre_ctx* ctx, const float* in, size_t width, size_t height, int fuji_width,
+                               int shrink, float* out);
 /* Same on device buffers; synchronises the context stream once when the
  * maximum has to be scanned. */
 lre_status lre_dev_develop_raw(lre_ctx* ctx, const uint16_t* raw_image, const lre_raw_frame* frame,

@@ -51,6 +51,7 @@ __all__ = [
     "wb_inputs",
     "wb_multipliers",
     "wb_needs_channel_sums",
+    "fuji_rotate_size",
 ]
 
 # LibRaw `filters` words of the four Bayer layouts.
@@ -447,6 +448,18 @@ class CudaAccelerator:
             return wb_multipliers(inputs, filters, maximum, black, sums, counts)
         return wb_multipliers(inputs, filters, maximum, black)
 
+    def fuji_rotate(self, image, fuji_width: int, shrink: int = 0):
+        """The 45-degree Fuji SuperCCD rotate after demosaic
+        (core/libraw_wrapper.cpp:1709-1750)."""
+        img = _rgb(image, "fuji_rotate")
+        h, w = img.shape[:2]
+        size = fuji_rotate_size(fuji_width, shrink, w, h)
+        if size is None:
+            raise ValueError("fuji_rotate: the reference leaves this image unrotated")
+        out = np.empty((size[1], size[0], 3), np.float32)
+        self._check(self._lib.lre_fuji_rotate(self._h, _ptr(img), w, h, int(fuji_width), int(shrink), _ptr(out)))
+        return out
+
     def green_matching(self, raw4, filters: int, maximum: int):
         a = np.ascontiguousarray(raw4, dtype=np.uint16).copy()
         self._check(self._lib.lre_green_matching(self._h, _ptr(a), a.shape[1], a.shape[0], int(filters), int(maximum)))
@@ -667,7 +680,8 @@ def wb_needs_channel_sums(inputs: "_lib.WbInputs") -> bool:
 
 def raw_frame(raw_width, raw_height, width, height, filters, raw_pitch=None, top_margin=0, left_margin=0,
               shrink=0, xtrans=None, cblack=(), black=0, maximum=65535, green_matching=0, wb=(1.0, 1.0, 1.0, 1.0),
-              adjust_maximum_thr=0.0, data_maximum=0.0, wb_in=None) -> "_lib.RawFrame":
+              adjust_maximum_thr=0.0, data_maximum=0.0, wb_in=None, fuji_width=0,
+              fuji_layout=0) -> "_lib.RawFrame":
     """A LibRaw-style frame description for the raw ingest entry points.
     With ``wb_in`` (:func:`wb_inputs`) the develop derives the WB multipliers
     on the device as scale_colors does and ``wb`` is ignored."""
@@ -692,7 +706,16 @@ def raw_frame(raw_width, raw_height, width, height, filters, raw_pitch=None, top
     if wb_in is not None:
         f.derive_wb = 1
         f.wb_in = wb_in
+    f.fuji_width, f.fuji_layout = int(fuji_width), int(fuji_layout)
     return f
+
+
+def fuji_rotate_size(fuji_width: int, shrink: int, width: int, height: int):
+    """Output (width, height) of the Fuji SuperCCD rotate, or None when the
+    reference leaves the image unrotated (core/libraw_wrapper.cpp:1709-1718)."""
+    ow, oh = C.c_size_t(), C.c_size_t()
+    _lib.load().lre_fuji_rotate_size(int(fuji_width), int(shrink), int(width), int(height), C.byref(ow), C.byref(oh))
+    return None if ow.value == 0 else (ow.value, oh.value)
 
 
 def develop_params(**kw) -> DevelopParams:

@@ -117,6 +117,8 @@ class RawFrame(C.Structure):
         ("data_maximum", C.c_float),
         ("derive_wb", C.c_int),
         ("wb_in", WbInputs),
+        ("fuji_width", C.c_int),
+        ("fuji_layout", C.c_int),
     ]
 
 
@@ -237,6 +239,9 @@ SIGNATURES = {
     "lre_wb_multipliers": (_st, [C.POINTER(WbInputs), C.c_uint32, C.c_uint, C.c_uint, _p, _p, C.POINTER(WbResult)]),
     "lre_channel_sums": (_st, [_p, _p, _sz, _sz, C.c_uint32, _p, _p, _p]),
     "lre_dev_channel_sums": (_st, [_p, _p, _sz, _sz, C.c_uint32, _p, _p, _p]),
+    "lre_fuji_rotate_size": (_st, [_i, _i, _sz, _sz, C.POINTER(_sz), C.POINTER(_sz)]),
+    "lre_fuji_rotate": (_st, [_p, _p, _sz, _sz, _i, _i, _p]),
+    "lre_dev_fuji_rotate": (_st, [_p, _p, _sz, _sz, _i, _i, _p]),
     "lre_set_tuning": (_st, [_p, C.POINTER(Tuning)]),
     "lre_get_tuning": (_st, [_p, C.POINTER(Tuning)]),
     "lre_batch_create": (_st, [C.POINTER(BatchConfig), C.POINTER(_p)]),

@@ -237,6 +237,13 @@ __device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsig
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
   return r;
 }
+// a * b + c per lane with one rounding
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
 
 template <int KS, int TB>
 __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTaps& taps, int W, int H,
@@ -261,12 +268,12 @@ __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTa
       s_in[r * LD + q] = blur_src(in, mode, sc, gx, gy, W);
     }
     __syncthreads();
-    // Both passes run two outputs per packed f32x2 multiply and add, at half
-    // the FP instruction count.  Every output still accumulates its taps in
-    // order from 0.f with each product and sum rounded to nearest, as the
-    // reference does; the packed instructions differ from scalar FP32 only
-    // where an operand or a result is subnormal (measured on B200: such
-    // values are flushed), which moves defringe outputs by at most ~5e-6.
+    // Both passes run two outputs per packed f32x2 fused multiply-add, one
+    // instruction per tap and output pair.  Every output accumulates its
+    // taps in the reference's order from 0.f; each tap's product and sum
+    // are rounded once (fused) instead of twice, and the packed form
+    // flushes subnormal operands and results (measured on B200).  Both move
+    // a blurred value by a few float ulps, inside the defringe tolerance.
     // horizontal: item = (halo rows 2jp, 2jp + 1; group of 8 output columns)
     for (int item = threadIdx.x; item < (E / 2) * (TB / 8); item += blockDim.x) {
       const int j = (item / (TB / 8)) * 2, k0 = (item % (TB / 8)) * 8;
@@ -280,7 +287,7 @@ __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTa
       for (int t = 0; t <= 2 * KS; t++) {
         const unsigned long long wt = f2_pack(w[t], w[t]);
 #pragma unroll
-        for (int o = 0; o < 8; o++) acc[o] = f2_add(acc[o], f2_mul(wt, x[o + t]));
+        for (int o = 0; o < 8; o++) acc[o] = f2_fma(wt, x[o + t], acc[o]);
       }
 #pragma unroll
       for (int o = 0; o < 8; o++) f2_unpack(acc[o], s_h[j * TB + k0 + o], s_h[(j + 1) * TB + k0 + o]);
@@ -300,7 +307,7 @@ __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTa
       for (int t = 0; t <= 2 * KS; t++) {
         const unsigned long long wt = f2_pack(w[t], w[t]);
 #pragma unroll
-        for (int o = 0; o < 4; o++) acc[o] = f2_add(acc[o], f2_mul(wt, x[o + t]));
+        for (int o = 0; o < 4; o++) acc[o] = f2_fma(wt, x[o + t], acc[o]);
       }
       const int gx = x0 + k;
 #pragma unroll

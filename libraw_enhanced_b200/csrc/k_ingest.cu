@@ -11,6 +11,7 @@
 //                    float mosaic the demosaic kernels read
 //   adjust_maximum   core/libraw_wrapper.cpp:1010-1087
 // then the develop chain (pipeline.cu) with the adopted maximum.
+#include <cmath>
 #include <cstring>
 
 #include "common.cuh"
@@ -56,6 +57,93 @@ __global__ void k_raw2image(const uint16_t* __restrict__ raw, int raw_width, int
       }
     }
     image4[q] = make_ushort4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+// Fuji SuperCCD honeycomb raw2image (core/libraw_wrapper.cpp:2342-2392).
+// The reference scatters raw (row, col) onto the 45-degree frame; here one
+// thread owns one image4 pixel and inverts the map for each frame site
+// (r, c) that lands on it (one site, or the 2x2 cell when shrinking):
+//   fuji_layout: r + c = fuji_width - 1 + row,  col = c - (row + 1) / 2
+//   otherwise:   c - r = col - fuji_width + 1,   row = c - (col + 1) / 2
+// Where several samples land on one pixel, the one latest in the
+// reference's row-major (row, col) scan wins, per channel.
+__global__ void k_raw2image_fuji(const uint16_t* __restrict__ raw, int raw_width, int raw_height, size_t pitch_px,
+                                 int top, int left, int width, int height, int shrink, uint32_t filters,
+                                 int fuji_width, int fuji_layout, ushort4* __restrict__ image4, int iwidth,
+                                 int iheight) {
+  const size_t n = (size_t)iwidth * iheight;
+  const int copy_rows = max(0, raw_height - top * 2);
+  const int copy_cols = fuji_width << (fuji_layout ? 0 : 1);
+  const int span = 1 << shrink;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const int R = (int)(q / iwidth), Cc = (int)(q % iwidth);
+    unsigned short v[4] = {0, 0, 0, 0};
+    long long key[4] = {-1, -1, -1, -1};
+    for (int sy = 0; sy < span; sy++) {
+      const int r = (R << shrink) + sy;
+      if (r >= height) break;
+      for (int sx = 0; sx < span; sx++) {
+        const int c = (Cc << shrink) + sx;
+        if (c >= width) break;
+        int row, col;
+        if (fuji_layout) {
+          row = r + c - fuji_width + 1;
+          if (row < 0) continue;
+          col = c - ((row + 1) >> 1);
+        } else {
+          col = c - r + fuji_width - 1;
+          if (col < 0) continue;
+          row = c - ((col + 1) >> 1);
+        }
+        if (row < 0 || row >= copy_rows || col < 0 || col >= copy_cols) continue;
+        const int src_row = row + top, src_col = col + left;
+        if (src_row >= raw_height || src_col >= raw_width) continue;
+        const long long k = (long long)row * copy_cols + col;
+        const unsigned short val = raw[(size_t)src_row * pitch_px + src_col];
+        const unsigned ch = fcol_native((unsigned)r, (unsigned)c, filters);
+        if (k > key[ch]) {
+          key[ch] = k;
+          v[ch] = val;
+        }
+        if (ch == 3 && k > key[1]) {
+          key[1] = k;
+          v[1] = val;
+        }
+      }
+    }
+    image4[q] = make_ushort4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+// The Fuji rotate (core/libraw_wrapper.cpp:1709-1750): one thread per output
+// pixel; the sample position in double then float, the bilinear weights in
+// float, as the reference computes them.
+__global__ void k_fuji_rotate(const float* __restrict__ rgb, size_t w, size_t h, int fuji_width, float* __restrict__ out,
+                              size_t wide, size_t high) {
+  const double step = sqrt(0.5);
+  const size_t n = wide * high;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t row = q / wide, col = q % wide;
+    const float r = (float)(fuji_width + ((double)row - (double)col) * step);
+    const float c = (float)(((double)row + (double)col) * step);
+    const size_t ur = (size_t)r, uc = (size_t)c;
+    float* dst = out + q * 3;
+    if (ur >= h - 1 || uc >= w - 1) {
+      dst[0] = dst[1] = dst[2] = 0.f;
+      continue;
+    }
+    const float fr = r - (float)ur, fc = c - (float)uc;
+    const float* p00 = rgb + (ur * w + uc) * 3;
+    const float* p01 = rgb + (ur * w + uc + 1) * 3;
+    const float* p10 = rgb + ((ur + 1) * w + uc) * 3;
+    const float* p11 = rgb + ((ur + 1) * w + uc + 1) * 3;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+      const float top = p00[ch] * (1.0f - fc) + p01[ch] * fc;
+      const float bottom = p10[ch] * (1.0f - fc) + p11[ch] * fc;
+      dst[ch] = top * (1.0f - fr) + bottom * fr;
+    }
   }
 }
 
@@ -144,11 +232,46 @@ size_t raw_image_elems(const lre_raw_frame& f) {
   return f.raw_height * (f.filters == LRE_FILTERS_XTRANS ? f.raw_width : f.raw_pitch / 2);
 }
 
+bool fuji_honeycomb(const lre_raw_frame& f) { return f.fuji_width > 0 && f.filters >= 1000; }
+
+// fuji_width' and the rotated size (core/libraw_wrapper.cpp:1710-1718);
+// false when the reference leaves the image as it is.
+bool fuji_rotate_size(int fuji_width_io, int shrink, size_t h, int* fw, size_t* wide, size_t* high) {
+  *fw = (fuji_width_io - 1 + shrink) >> shrink;
+  if (*fw <= 0) return false;
+  const double step = std::sqrt(0.5);
+  const int wide_i = static_cast<int>(*fw / step);
+  const int high_i = static_cast<int>((static_cast<int>(h) - *fw) / step);
+  if (wide_i <= 1 || high_i <= 1) return false;
+  *wide = (size_t)wide_i;
+  *high = (size_t)high_i;
+  return true;
+}
+
+lre_status launch_fuji_rotate(Context* c, const float* in, size_t w, size_t h, int fuji_width_io, int shrink,
+                              float* out) {
+  int fw;
+  size_t wide, high;
+  if (!fuji_rotate_size(fuji_width_io, shrink, h, &fw, &wide, &high))
+    return fail(c, LRE_ERR_INVALID_ARGUMENT, "fuji_rotate: the reference leaves this image unrotated");
+  k_fuji_rotate<<<grid_for(wide * high, 256, c->sm_count * 8), 256, 0, c->stream>>>(in, w, h, fw, out, wide, high);
+  count_launch(c);
+  return check_launch(c, "fuji_rotate");
+}
+
 lre_status launch_raw2image(Context* c, const uint16_t* raw, const lre_raw_frame& f, uint16_t* image4) {
   const uint32_t filters = f.filters;
   const char* xtrans = f.xtrans;
   const int shrink = f.shrink ? 1 : 0;
   const size_t iw = (f.width + shrink) >> shrink, ih = (f.height + shrink) >> shrink;
+  if (fuji_honeycomb(f)) {
+    k_raw2image_fuji<<<grid_for(iw * ih, 256, c->sm_count * 8), 256, 0, c->stream>>>(
+        raw, (int)f.raw_width, (int)f.raw_height, f.raw_pitch / 2, (int)f.top_margin, (int)f.left_margin,
+        (int)f.width, (int)f.height, shrink, filters, f.fuji_width, f.fuji_layout ? 1 : 0,
+        reinterpret_cast<ushort4*>(image4), (int)iw, (int)ih);
+    count_launch(c);
+    return check_launch(c, "raw2image (Fuji honeycomb)");
+  }
   k_raw2image<<<grid_for(iw * ih, 256, c->sm_count * 8), 256, 0, c->stream>>>(
       raw, (int)f.raw_width, (int)f.raw_height, f.raw_pitch / 2, (int)f.top_margin, (int)f.left_margin,
       (int)f.width, (int)f.height, shrink, filters, make_pat(xtrans), reinterpret_cast<ushort4*>(image4), (int)iw,
@@ -207,6 +330,8 @@ lre_status check_frame(Context* c, const lre_raw_frame* f) {
   if (f->cblack[4] * f->cblack[5] > 36)
     return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "raw frame: positional black pattern larger than 6x6");
   if (f->width > (1u << 20) || f->height > (1u << 20)) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "raw frame: too large");
+  if (f->fuji_width < 0 || f->fuji_width > 65535)
+    return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "raw frame: fuji_width outside LibRaw's 16-bit range");
   return LRE_OK;
 }
 
@@ -311,6 +436,48 @@ lre_status lre_green_matching(lre_ctx* ctx, uint16_t* raw4, size_t width, size_t
   LRE_TRY(lre::launch_green_matching(c, reinterpret_cast<uint16_t*>(c->d_in), reinterpret_cast<uint16_t*>(c->d_out),
                                      width, height, filters, maximum));
   LRE_CUDA_TRY(c, cudaMemcpyAsync(raw4, c->d_in, bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return LRE_OK;
+}
+
+lre_status lre_fuji_rotate_size(int fuji_width, int shrink, size_t width, size_t height, size_t* out_w,
+                                size_t* out_h) {
+  (void)width;
+  if (!out_w || !out_h) return LRE_ERR_INVALID_ARGUMENT;
+  int fw;
+  if (!lre::fuji_rotate_size(fuji_width, shrink ? 1 : 0, height, &fw, out_w, out_h)) *out_w = *out_h = 0;
+  return LRE_OK;
+}
+
+lre_status lre_dev_fuji_rotate(lre_ctx* ctx, const float* in, size_t width, size_t height, int fuji_width, int shrink,
+                               float* out) {
+  Context* c = CX(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  if (!in || !out || width < 2 || height < 2) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "fuji_rotate: bad image");
+  cudaSetDevice(c->device);
+  LRE_TRY(lre::check_injection(c));
+  return lre::launch_fuji_rotate(c, in, width, height, fuji_width, shrink ? 1 : 0, out);
+}
+
+lre_status lre_fuji_rotate(lre_ctx* ctx, const float* in, size_t width, size_t height, int fuji_width, int shrink,
+                           float* out) {
+  Context* c = CX(ctx);
+  if (!c) return LRE_ERR_INVALID_ARGUMENT;
+  if (!in || !out || width < 2 || height < 2) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "fuji_rotate: bad image");
+  int fw;
+  size_t wide, high;
+  if (!lre::fuji_rotate_size(fuji_width, shrink ? 1 : 0, height, &fw, &wide, &high))
+    return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "fuji_rotate: the reference leaves this image unrotated");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  LRE_TRY(lre::check_injection(c));
+  const size_t in_bytes = width * height * 12, out_bytes = wide * high * 12;
+  LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, in_bytes));
+  LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, out_bytes));
+  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, in, in_bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::launch_fuji_rotate(c, reinterpret_cast<const float*>(c->d_in), width, height, fuji_width,
+                                  shrink ? 1 : 0, reinterpret_cast<float*>(c->d_out)));
+  LRE_CUDA_TRY(c, cudaMemcpyAsync(out, c->d_out, out_bytes, cudaMemcpyDeviceToHost, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }

@@ -92,6 +92,9 @@ _PORT_SIGS = {
     "port_scale_mul": (None, [_p, C.c_int, _f, _p]),
     "port_auto_wb": (None, [_p, _sz, _sz, C.c_uint32, _p, _p]),
     "port_border_interpolate": (None, [_p, _sz, _sz, C.c_uint32, _sz]),
+    "port_raw2image_fuji": (None, [_p, _sz, _sz, _sz, _sz, _sz, _sz, _sz, C.c_int, C.c_uint32, C.c_int, C.c_int,
+                                    _p]),
+    "port_fuji_rotate": (None, [_p, _sz, _sz, C.c_int, C.c_int, _p, C.POINTER(_sz), C.POINTER(_sz)]),
     "port_scale_colors": (C.c_int, [_p, _sz, _sz, C.c_uint32, _p, _p, _p, _p, _p, _p, C.c_int, C.c_int,
                                     C.POINTER(C.c_uint), C.c_uint, _p, _p]),
 }
@@ -373,6 +376,35 @@ def raw2image(raw, raw_pitch, top_margin, left_margin, width, height, filters, x
     out = np.zeros((ih, iw, 4), np.uint16)
     port().port_raw2image(_ptr(raw), rw, rh, int(raw_pitch), int(top_margin), int(left_margin), int(width),
                           int(height), int(shrink), int(filters), _ptr(_xt(xtrans_pattern)), _ptr(out))
+    return out
+
+
+def raw2image_fuji(raw, raw_pitch, top_margin, left_margin, width, height, filters, fuji_width, fuji_layout,
+                   shrink=0, raw_width=None):
+    """The Fuji SuperCCD honeycomb raw2image (core/libraw_wrapper.cpp:2342-2392).
+    raw: (raw_height, raw_pitch // 2) uint16; raw_width defaults to the row length."""
+    raw = np.ascontiguousarray(raw, dtype=np.uint16)
+    rh, rw = raw.shape
+    if raw_width is not None:
+        rw = int(raw_width)
+    iw, ih = (width + shrink) >> shrink, (height + shrink) >> shrink
+    out = np.zeros((ih, iw, 4), np.uint16)
+    port().port_raw2image_fuji(_ptr(raw), rw, rh, int(raw_pitch), int(top_margin), int(left_margin), int(width),
+                               int(height), int(shrink), int(filters), int(fuji_width), int(fuji_layout), _ptr(out))
+    return out
+
+
+def fuji_rotate(rgb, fuji_width, shrink=0):
+    """The 45-degree Fuji rotate after demosaic (core/libraw_wrapper.cpp:1709-1750);
+    returns the input unchanged when the reference would not rotate."""
+    a = _img(rgb)
+    h, w, _ = a.shape
+    ow, oh = _sz(0), _sz(0)
+    port().port_fuji_rotate(_ptr(a), w, h, int(fuji_width), int(shrink), None, C.byref(ow), C.byref(oh))
+    if ow.value == 0:
+        return a.copy()
+    out = np.empty((oh.value, ow.value, 3), np.float32)
+    port().port_fuji_rotate(_ptr(a), w, h, int(fuji_width), int(shrink), _ptr(out), C.byref(ow), C.byref(oh))
     return out
 
 

@@ -422,6 +422,91 @@ void port_raw2image(const uint16_t* raw, size_t raw_width, size_t raw_height, si
 }
 
 /*
+ * core/libraw_wrapper.cpp:2342-2392 (copy_bayer_image, Fuji SuperCCD
+ * honeycomb branch): raw rows [0, raw_height - 2 top_margin) and columns
+ * [0, fuji_width << !fuji_layout) land on the 45-degree frame at
+ *   fuji_layout:  r = fuji_width - 1 - col + row / 2, c = col + (row + 1) / 2
+ *   otherwise:    r = fuji_width - 1 + row - col / 2, c = row + (col + 1) / 2
+ * (halves rounded down), in the sample's fcol_bayer_native(r, c) channel (a
+ * colour-3 sample also in channel 1), halved by `shrink`; later samples of
+ * the row-major scan overwrite earlier ones.
+ */
+void port_raw2image_fuji(const uint16_t* raw, size_t raw_width, size_t raw_height, size_t raw_pitch,
+                         size_t top_margin, size_t left_margin, size_t width, size_t height, int shrink,
+                         uint32_t filters, int fuji_width, int fuji_layout, uint16_t* image4) {
+  int iwidth = (int)((width + shrink) >> shrink), iheight = (int)((height + shrink) >> shrink);
+  memset(image4, 0, (size_t)iwidth * iheight * 4 * sizeof(uint16_t));
+  int copy_rows = (int)raw_height - (int)top_margin * 2;
+  if (copy_rows < 0) copy_rows = 0;
+  const int copy_cols = fuji_width << (fuji_layout ? 0 : 1);
+  for (int row = 0; row < copy_rows; row++)
+    for (int col = 0; col < copy_cols; col++) {
+      int r, c;
+      if (fuji_layout) {
+        r = fuji_width - 1 - col + (row >> 1);
+        c = col + ((row + 1) >> 1);
+      } else {
+        r = fuji_width - 1 + row - (col >> 1);
+        c = row + ((col + 1) >> 1);
+      }
+      const int src_row = row + (int)top_margin, src_col = col + (int)left_margin;
+      if (src_row < 0 || src_row >= (int)raw_height || src_col < 0 || src_col >= (int)raw_width) continue;
+      if (r < 0 || c < 0 || r >= (int)height || c >= (int)width) continue;
+      const int dst_row = r >> shrink, dst_col = c >> shrink;
+      if (dst_row >= iheight || dst_col >= iwidth) continue;
+      const uint16_t val = raw[(size_t)src_row * (raw_pitch / 2) + src_col];
+      const unsigned ch = port_fcol_bayer_native((unsigned)r, (unsigned)c, filters);
+      const size_t dst = (size_t)dst_row * iwidth + dst_col;
+      image4[dst * 4 + ch] = val;
+      if (ch == 3) image4[dst * 4 + 1] = val;
+    }
+}
+
+/*
+ * core/libraw_wrapper.cpp:1709-1750 (process_raw_to_rgb, Fuji rotate):
+ * fuji_width' = (fuji_width - 1 + shrink) >> shrink, step = sqrt(0.5),
+ * output wide = (int)(fuji_width' / step) by high = (int)((h - fuji_width') / step)
+ * (returned through *out_w / *out_h; 0 when either is <= 1, no rotation);
+ * each output pixel bilinearly samples the demosaiced image at
+ *   r = (float)(fuji_width' + (row - col) step), c = (float)((row + col) step)
+ * and stays 0 where (int)r >= h - 1 or (int)c >= w - 1.  `out` holds
+ * wide * high * 3 floats (call once with out == NULL for the size).
+ */
+void port_fuji_rotate(const float* rgb, size_t w, size_t h, int fuji_width_io, int shrink, float* out,
+                      size_t* out_w, size_t* out_h) {
+  *out_w = *out_h = 0;
+  const int fuji_width = (fuji_width_io - 1 + shrink) >> shrink;
+  if (fuji_width <= 0) return;
+  const double step = sqrt(0.5);
+  const int wide_i = (int)(fuji_width / step);
+  const int high_i = (int)(((int)h - fuji_width) / step);
+  if (wide_i <= 1 || high_i <= 1) return;
+  *out_w = (size_t)wide_i;
+  *out_h = (size_t)high_i;
+  if (!out) return;
+  const size_t wide = (size_t)wide_i, high = (size_t)high_i;
+  memset(out, 0, wide * high * 3 * sizeof(float));
+  for (size_t row = 0; row < high; ++row)
+    for (size_t col = 0; col < wide; ++col) {
+      const float r = (float)(fuji_width + ((double)row - (double)col) * step);
+      const float c = (float)(((double)row + (double)col) * step);
+      const size_t ur = (size_t)r, uc = (size_t)c;
+      if (ur >= h - 1 || uc >= w - 1) continue;
+      const float fr = r - (float)ur, fc = c - (float)uc;
+      const float* p00 = rgb + (ur * w + uc) * 3;
+      const float* p01 = rgb + (ur * w + uc + 1) * 3;
+      const float* p10 = rgb + ((ur + 1) * w + uc) * 3;
+      const float* p11 = rgb + ((ur + 1) * w + uc + 1) * 3;
+      float* dst = out + (row * wide + col) * 3;
+      for (int ch = 0; ch < 3; ++ch) {
+        const float top = p00[ch] * (1.0f - fc) + p01[ch] * fc;
+        const float bottom = p10[ch] * (1.0f - fc) + p11[ch] * fc;
+        dst[ch] = top * (1.0f - fr) + bottom * fr;
+      }
+    }
+}
+
+/*
  * core/libraw_wrapper.cpp:496-585 (apply_green_matching): at the G2
  * positions of an RGGB layout (rows 3, 5, ..., columns 2, 4, ...), in flat,
  * unsaturated areas, scale channel 3 by the ratio of the surrounding G1 and

@@ -159,3 +159,38 @@ def test_develop_raw_derives_wb_like_scale_colors(lre, acc, mode):
     p.maximum_value = adopted
     ref = acc.develop(np.ascontiguousarray(dense), p)
     assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("fuji_layout,shrink", [(1, 0), (0, 0), (1, 1), (0, 1)])
+def test_raw2image_fuji_honeycomb(lre, acc, fuji_layout, shrink):
+    """Fuji SuperCCD honeycomb raw2image (core/libraw_wrapper.cpp:2342-2392):
+    raw rows and columns mapped onto the 45-degree frame, bit-exact against
+    the oracle's forward scan (the device inverts the map per pixel)."""
+    rng = np.random.default_rng(31 + 2 * fuji_layout + shrink)
+    fuji_width = 181
+    copy_cols = fuji_width << (0 if fuji_layout else 1)
+    top, left = 4, 3
+    rh, rw = 260 + 2 * top, copy_cols + left + 5
+    pitch_px = rw + 6
+    raw = rng.integers(0, 16384, size=(rh, pitch_px), dtype=np.uint16)
+    width, height = 420, 400
+    for filters in (RGGB, RGGB_G2):
+        f = lre.raw_frame(rw, rh, width, height, filters, raw_pitch=pitch_px * 2, top_margin=top, left_margin=left,
+                          shrink=shrink, fuji_width=fuji_width, fuji_layout=fuji_layout)
+        got = acc.raw2image(raw, f)
+        ref = oracle.raw2image_fuji(raw, pitch_px * 2, top, left, width, height, filters, fuji_width, fuji_layout,
+                                    shrink, raw_width=rw)
+        assert np.array_equal(got, ref)
+        assert (ref != 0).any(axis=2).mean() > 0.2
+
+
+def test_fuji_rotate_bit_exact(lre, acc):
+    """The 45-degree Fuji rotate after demosaic (core/libraw_wrapper.cpp:
+    1709-1750): same output size and values as the reference's loop."""
+    rgb = np.random.default_rng(33).random((403, 371, 3), dtype=np.float32) * np.float32(1.2)
+    for fuji_width, shrink in ((180, 0), (181, 1)):
+        ref = oracle.fuji_rotate(rgb, fuji_width, shrink)
+        assert lre.fuji_rotate_size(fuji_width, shrink, 371, 403) == (ref.shape[1], ref.shape[0])
+        got = acc.fuji_rotate(rgb, fuji_width, shrink)
+        assert np.array_equal(got, ref)
+    assert lre.fuji_rotate_size(0, 0, 371, 403) is None
