@@ -37,9 +37,9 @@ lre_status host_rgb_stage(Context* c, const float* in, float* out, size_t w, siz
   const size_t bytes = w * h * 3 * sizeof(float);
   LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, bytes));
   float* d = reinterpret_cast<float*>(c->d_in);
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(d, in, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, d, in, bytes, c->stream));
   LRE_TRY(fn(d));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, out, d, bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }
@@ -146,14 +146,14 @@ lre_status lre_enhance_micro_contrast(lre_ctx* ctx, const float* in, float* out,
   const size_t bytes = w * h * 3 * sizeof(float);
   LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, bytes));
   float* d = reinterpret_cast<float*>(c->d_in);
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(d, in, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, d, in, bytes, c->stream));
   float* dmask = nullptr;
   if (mask) {
     dmask = reinterpret_cast<float*>(c->ws.take(w * h * sizeof(float)));
-    LRE_CUDA_TRY(c, cudaMemcpyAsync(dmask, mask, w * h * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    LRE_TRY(lre::copy_h2d(c, dmask, mask, w * h * sizeof(float), c->stream));
   }
   LRE_TRY(lre::launch_micro_contrast(c, d, d, w, h, thr, strength, target, dmask));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, out, d, bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }
@@ -217,9 +217,9 @@ lre_status lre_demosaic_bayer_linear(lre_ctx* ctx, const float* raw_rgb, float* 
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, bytes));
   float* din = reinterpret_cast<float*>(c->d_in);
   float* dout = reinterpret_cast<float*>(c->d_out);
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(din, raw_rgb, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, din, raw_rgb, bytes, c->stream));
   LRE_TRY(lre::launch_bayer_linear(c, din, 3, dout, w, h, filters, maximum_value));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(rgb, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, rgb, dout, bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }
@@ -245,9 +245,9 @@ lre_status lre_demosaic_bayer_dcb(lre_ctx* ctx, const float* raw_rgb, float* rgb
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, bytes));
   float* din = reinterpret_cast<float*>(c->d_in);
   float* dout = reinterpret_cast<float*>(c->d_out);
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(din, raw_rgb, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, din, raw_rgb, bytes, c->stream));
   LRE_TRY(lre::launch_dcb(c, din, 3, dout, w, h, filters, maximum_value, iterations, dcb_enhance != 0, nullptr));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(rgb, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, rgb, dout, bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }
@@ -277,10 +277,10 @@ lre_status lre_recover_highlights(lre_ctx* ctx, const float* in, float* out, siz
   float* dout = reinterpret_cast<float*>(c->d_out);
   float* dmask = mask_out ? reinterpret_cast<float*>(c->d_aux) : nullptr;
   float* dmax = c->d_scalars + 40;
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(din, in, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, din, in, bytes, c->stream));
   LRE_TRY(lre::launch_recover_highlights(c, din, dout, w, h, thr, dmask, wb_rgb, dmax, nullptr));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
-  if (mask_out) LRE_CUDA_TRY(c, cudaMemcpyAsync(mask_out, dmask, mbytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, out, dout, bytes, c->stream));
+  if (mask_out) LRE_TRY(lre::copy_d2h(c, mask_out, dmask, mbytes, c->stream));
   if (max_val_out) LRE_CUDA_TRY(c, cudaMemcpyAsync(max_val_out, dmax, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
@@ -307,9 +307,9 @@ lre_status lre_demosaic_bayer_aahd(lre_ctx* ctx, const float* raw_rgb, float* rg
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, bytes));
   float* din = reinterpret_cast<float*>(c->d_in);
   float* dout = reinterpret_cast<float*>(c->d_out);
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(din, raw_rgb, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, din, raw_rgb, bytes, c->stream));
   LRE_TRY(lre::launch_aahd(c, din, 3, dout, w, h, filters, maximum_value, nullptr));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(rgb, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, rgb, dout, bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }
@@ -329,9 +329,9 @@ lre_status lre_demosaic_bayer_amaze(lre_ctx* ctx, const float* raw_rgb, float* r
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, bytes));
   float* din = reinterpret_cast<float*>(c->d_in);
   float* dout = reinterpret_cast<float*>(c->d_out);
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(din, raw_rgb, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, din, raw_rgb, bytes, c->stream));
   LRE_TRY(lre::launch_amaze(c, din, 3, dout, w, h, filters, cam_mul, maximum_value));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(rgb, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, rgb, dout, bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }
@@ -349,9 +349,9 @@ static lre_status xtrans_host(lre_ctx* ctx, const float* raw_rgb, float* rgb, si
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, bytes));
   float* din = reinterpret_cast<float*>(c->d_in);
   float* dout = reinterpret_cast<float*>(c->d_out);
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(din, raw_rgb, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, din, raw_rgb, bytes, c->stream));
   LRE_TRY(lre::launch_xtrans(c, din, 3, dout, w, h, xtrans, maximum_value, passes));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(rgb, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, rgb, dout, bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }
@@ -392,12 +392,12 @@ lre_status lre_apply_white_balance(lre_ctx* ctx, const uint16_t* raw4, float* rg
   const size_t in_bytes = w * h * 4 * sizeof(uint16_t), out_bytes = w * h * 3 * sizeof(float);
   LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, in_bytes));
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, out_bytes));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, raw4, in_bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, c->d_in, raw4, in_bytes, c->stream));
   // untouched channels keep the caller's values, as in the reference
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_out, rgb, out_bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, c->d_out, rgb, out_bytes, c->stream));
   LRE_TRY(lre::launch_white_balance(c, reinterpret_cast<const uint16_t*>(c->d_in), reinterpret_cast<float*>(c->d_out),
                                     w, h, wb, filters, xtrans));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(rgb, c->d_out, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, rgb, c->d_out, out_bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }
@@ -413,9 +413,9 @@ lre_status lre_black_level(lre_ctx* ctx, uint16_t* raw4, size_t w, size_t h, con
   LRE_TRY(begin(c, (cblack_len + 64) * sizeof(unsigned) + 256));
   const size_t bytes = w * h * 4 * sizeof(uint16_t);
   LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, bytes));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, raw4, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, c->d_in, raw4, bytes, c->stream));
   LRE_TRY(lre::launch_black_level(c, reinterpret_cast<uint16_t*>(c->d_in), w, h, cblack, cblack_len, black, maximum));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(raw4, c->d_in, bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, raw4, c->d_in, bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }
@@ -435,7 +435,7 @@ lre_status lre_adjust_maximum(lre_ctx* ctx, const float* raw_rgb, size_t w, size
     LRE_TRY(begin(c, 0));
     const size_t bytes = w * h * 3 * sizeof(float);
     LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, bytes));
-    LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, raw_rgb, bytes, cudaMemcpyHostToDevice, c->stream));
+    LRE_TRY(lre::copy_h2d(c, c->d_in, raw_rgb, bytes, c->stream));
     LRE_TRY(lre::launch_cfa_max(c, reinterpret_cast<const float*>(c->d_in), 3, w, h, filters, c->d_scalars));
     LRE_CUDA_TRY(c, cudaMemcpyAsync(&real_max, c->d_scalars, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -463,12 +463,12 @@ static lre_status quantize_host(lre_ctx* ctx, const float* in, void* out, size_t
   const size_t ob = n * (bits == 16 ? 2 : 1);
   LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, n * sizeof(float)));
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, ob));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, in, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, c->d_in, in, n * sizeof(float), c->stream));
   if (bits == 16)
     LRE_TRY(lre::launch_quantize_u16(c, reinterpret_cast<float*>(c->d_in), reinterpret_cast<uint16_t*>(c->d_out), n));
   else
     LRE_TRY(lre::launch_quantize_u8(c, reinterpret_cast<float*>(c->d_in), reinterpret_cast<uint8_t*>(c->d_out), n));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(out, c->d_out, ob, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, out, c->d_out, ob, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }

@@ -146,6 +146,8 @@ void lre_destroy(lre_ctx* ctx) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+  lre::destroy_stager(c);
   if (c->d_in) cudaFree(c->d_in);
   if (c->d_out) cudaFree(c->d_out);
   if (c->d_aux) cudaFree(c->d_aux);

@@ -1003,8 +1003,8 @@ lre_status launch_amaze_from_host(Context* c, const float* h_mosaic, float* d_mo
     // a tile row k reads mosaic rows [128k - 16, 128k + 144) (clamped)
     const size_t need = std::min(h, (size_t)std::max(0, -16 + (row_hi - 1) * (TS - 32) + TS));
     if (need > copied) {
-      LRE_CUDA_TRY(c, cudaMemcpyAsync(d_mosaic + copied * w, h_mosaic + copied * w, (need - copied) * w * sizeof(float),
-                                      cudaMemcpyHostToDevice, copy_stream));
+      LRE_TRY(copy_h2d(c, d_mosaic + copied * w, h_mosaic + copied * w, (need - copied) * w * sizeof(float),
+                       copy_stream));
       copied = need;
     }
     LRE_CUDA_TRY(c, cudaEventRecord(events[b], copy_stream));
@@ -1012,8 +1012,8 @@ lre_status launch_amaze_from_host(Context* c, const float* h_mosaic, float* d_mo
     LRE_TRY(launch_amaze_rows(c, A, row_lo, row_hi));
   }
   if (copied < h) {  // rows no tile reads still belong to the resident mosaic
-    LRE_CUDA_TRY(c, cudaMemcpyAsync(d_mosaic + copied * w, h_mosaic + copied * w, (h - copied) * w * sizeof(float),
-                                    cudaMemcpyHostToDevice, copy_stream));
+    LRE_TRY(copy_h2d(c, d_mosaic + copied * w, h_mosaic + copied * w, (h - copied) * w * sizeof(float),
+                     copy_stream));
     LRE_CUDA_TRY(c, cudaEventRecord(events[bands - 1], copy_stream));
     LRE_CUDA_TRY(c, cudaStreamWaitEvent(c->stream, events[bands - 1], 0));
   }

@@ -414,9 +414,9 @@ lre_status lre_raw2image(lre_ctx* ctx, const uint16_t* raw_image, const lre_raw_
   const size_t n_out = ((f->width + shrink) >> shrink) * ((f->height + shrink) >> shrink) * 4;
   LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, n_in * 2));
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, n_out * 2));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, raw_image, n_in * 2, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, c->d_in, raw_image, n_in * 2, c->stream));
   LRE_TRY(lre::launch_raw2image(c, reinterpret_cast<const uint16_t*>(c->d_in), *f, reinterpret_cast<uint16_t*>(c->d_out)));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(image4, c->d_out, n_out * 2, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, image4, c->d_out, n_out * 2, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }
@@ -432,10 +432,10 @@ lre_status lre_green_matching(lre_ctx* ctx, uint16_t* raw4, size_t width, size_t
   const size_t bytes = width * height * 8;
   LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, bytes));
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, bytes));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, raw4, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, c->d_in, raw4, bytes, c->stream));
   LRE_TRY(lre::launch_green_matching(c, reinterpret_cast<uint16_t*>(c->d_in), reinterpret_cast<uint16_t*>(c->d_out),
                                      width, height, filters, maximum));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(raw4, c->d_in, bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, raw4, c->d_in, bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }
@@ -474,10 +474,10 @@ lre_status lre_fuji_rotate(lre_ctx* ctx, const float* in, size_t width, size_t h
   const size_t in_bytes = width * height * 12, out_bytes = wide * high * 12;
   LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, in_bytes));
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, out_bytes));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, in, in_bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, c->d_in, in, in_bytes, c->stream));
   LRE_TRY(lre::launch_fuji_rotate(c, reinterpret_cast<const float*>(c->d_in), width, height, fuji_width,
                                   shrink ? 1 : 0, reinterpret_cast<float*>(c->d_out)));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(out, c->d_out, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, out, c->d_out, out_bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }
@@ -508,9 +508,9 @@ lre_status lre_develop_raw(lre_ctx* ctx, const uint16_t* raw_image, const lre_ra
   const size_t out_bytes = iw * ih * 3 * (params->output_bits == 16 ? 2 : 4);
   LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, n_in * 2));
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, out_bytes));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, raw_image, n_in * 2, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, c->d_in, raw_image, n_in * 2, c->stream));
   LRE_TRY(develop_raw_device(c, reinterpret_cast<const uint16_t*>(c->d_in), *f, c->d_out, *params, maximum_used));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(out, c->d_out, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, out, c->d_out, out_bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }

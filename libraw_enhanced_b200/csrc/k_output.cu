@@ -145,10 +145,10 @@ lre_status lre_output_epilogue(lre_ctx* ctx, const float* in, void* out, size_t 
   const size_t n = width * height, in_bytes = n * 12, out_bytes = n * 3 * (size_t)(bits / 8);
   LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, in_bytes));
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, out_bytes));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, in, in_bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, c->d_in, in, in_bytes, c->stream));
   LRE_TRY(lre::launch_output_epilogue(c, reinterpret_cast<const float*>(c->d_in), c->d_out, n, transform, gamma_power,
                                       gamma_slope, output_color_space, bits));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(out, c->d_out, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+  LRE_TRY(lre::copy_d2h(c, out, c->d_out, out_bytes, c->stream));
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return LRE_OK;
 }

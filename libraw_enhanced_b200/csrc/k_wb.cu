@@ -233,7 +233,7 @@ lre_status lre_channel_sums(lre_ctx* ctx, const uint16_t* raw4, size_t width, si
   LRE_TRY(lre::check_injection(c));
   const size_t bytes = width * height * 8;
   LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, bytes));
-  LRE_CUDA_TRY(c, cudaMemcpyAsync(c->d_in, raw4, bytes, cudaMemcpyHostToDevice, c->stream));
+  LRE_TRY(lre::copy_h2d(c, c->d_in, raw4, bytes, c->stream));
   return lre::dev_sums(c, reinterpret_cast<const uint16_t*>(c->d_in), width, height, filters, xtrans, sums, counts);
 }
 

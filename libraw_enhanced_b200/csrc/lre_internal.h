@@ -15,6 +15,8 @@
 
 namespace lre {
 
+class HostStager;  // pinned bounce ring for pageable host buffers (host_stage.cu)
+
 // One 256-byte-aligned bump arena on the device.  `reset()` releases every
 // allocation at once; the arena only grows (reallocation synchronises the
 // stream first, so pointers handed out earlier in the same call stay valid
@@ -87,7 +89,17 @@ struct Context {
   // the next sweep's band `sweep_hold_band` never reports its progress.
   long long sweep_wait_cycles = 0;
   int sweep_hold_band = -1;
+  HostStager* stager = nullptr;  // created on the first large pageable copy
 };
+
+// Host <-> device copies of the host-buffer entry points (host_stage.cu):
+// pageable buffers above a few MB go through the context's pinned chunk ring
+// with a parallel host memcpy; page-locked buffers and small copies are
+// direct.  copy_h2d returns once the source may be reused; copy_d2h returns
+// when the data is in `dst` (it synchronises `s`).
+lre_status copy_h2d(Context* c, void* dst, const void* src, size_t bytes, cudaStream_t s);
+lre_status copy_d2h(Context* c, void* dst, const void* src, size_t bytes, cudaStream_t s);
+void destroy_stager(Context* c);
 
 // Status helpers.
 lre_status fail(Context* c, lre_status st, const std::string& msg);

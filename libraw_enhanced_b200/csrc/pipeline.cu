@@ -110,8 +110,7 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
   // it after its final synchronisation.
   int* d_err = reinterpret_cast<int*>(c->d_scalars + 63);
   if (h_mosaic && route(p) != Demosaic::Amaze)
-    LRE_CUDA_TRY(c, cudaMemcpyAsync(const_cast<float*>(d_mosaic), h_mosaic, w * h * sizeof(float),
-                                    cudaMemcpyHostToDevice, c->stream));
+    LRE_TRY(lre::copy_h2d(c, const_cast<float*>(d_mosaic), h_mosaic, w * h * sizeof(float), c->stream));
   // cur_max_g: a device scalar holding max(0, max G) of `cur`, when the stage
   // that wrote `cur` reduced it on the way (nullptr otherwise).  Defringe and
   // the axial filter each need that maximum of their input; with the
@@ -360,18 +359,17 @@ lre_status lre_develop(lre_ctx* ctx, const float* mosaic, void* out, size_t w, s
     LRE_TRY(run_chain(c, reinterpret_cast<const float*>(c->d_in), rgb_a, rgb_b, w, h, p, &res, mosaic, &tail));
     for (int b = 0; b < nb; b++) {
       LRE_CUDA_TRY(c, cudaStreamWaitEvent(c->copy_stream, c->tail_ev[b], 0));
-      LRE_CUDA_TRY(c, cudaMemcpyAsync(static_cast<char*>(out) + bands[b].r0 * w * px_bytes, bands[b].src,
-                                      (bands[b].r1 - bands[b].r0) * w * px_bytes, cudaMemcpyDeviceToHost,
-                                      c->copy_stream));
+      LRE_TRY(lre::copy_d2h(c, static_cast<char*>(out) + bands[b].r0 * w * px_bytes, bands[b].src,
+                            (bands[b].r1 - bands[b].r0) * w * px_bytes, c->copy_stream));
     }
     LRE_CUDA_TRY(c, cudaStreamSynchronize(c->copy_stream));
   } else {
     LRE_TRY(run_chain(c, reinterpret_cast<const float*>(c->d_in), rgb_a, rgb_b, w, h, p, &res, mosaic));
     if (p.output_bits == 16) {
       LRE_TRY(lre::launch_quantize_u16(c, res, reinterpret_cast<uint16_t*>(c->d_out), w * h * 3));
-      LRE_CUDA_TRY(c, cudaMemcpyAsync(out, c->d_out, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+      LRE_TRY(lre::copy_d2h(c, out, c->d_out, out_bytes, c->stream));
     } else {
-      LRE_CUDA_TRY(c, cudaMemcpyAsync(out, res, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+      LRE_TRY(lre::copy_d2h(c, out, res, out_bytes, c->stream));
     }
   }
   LRE_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
