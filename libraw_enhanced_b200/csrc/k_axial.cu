@@ -7,12 +7,11 @@
 //   * R, G, B are normalised by norm = max(1e-6, max G) (float multiply by
 //     1/norm, exactly as the reference);
 //   * box means use an edge-truncated (2r+1)^2 window; the reference builds
-//     double summed-area tables, here every window sum is a float sliding
-//     sum (the streaming passes; the guide statistics of samples centred at
-//     0.5) or a double sum (the fused tile kernel), equal to the SAT
-//     difference up to rounding;
-//   * a = cov(G,X) / (var(G) + eps), b = mean(X) - a mean(G), stored as
-//     float; q = mean(a) * G + mean(b);
+//     double summed-area tables, here every window sum is accumulated in
+//     double directly (sliding sums), which equals the SAT difference up to
+//     double rounding;
+//   * a = cov(G,X) / (var(G) + eps), b = mean(X) - a mean(G) in double, stored
+//     as float; q = mean(a) * G + mean(b) in double, stored as float;
 //   * edge weight w = smoothstep(0.01, 0.06, boxmean_r(|central grad G|));
 //   * out = (X (1 - s w) + q s w) * norm, G passes through.
 //
@@ -23,7 +22,6 @@
 // older single fused tile kernel (k_axial_fused: both box levels out of
 // shared memory, the level-one statistics recomputed over each tile's halo)
 // remains for the allocation-free entry point at the end of this file.
-#include <algorithm>
 #include <mutex>
 
 #include <functional>
@@ -392,167 +390,148 @@ cudaError_t axial_dispatch(int T, int NT, size_t w, size_t h, cudaStream_t s, co
 // ---------------------------------------------------------------------------
 // Streaming two-pass form (the default path).  The image is cut into strips
 // of WS output columns and HS output rows; one warp walks a strip down its
-// rows, and a CTA holds NW such independent warps (each with its own shared
-// window sums; the warps never synchronise with one another).  The vertical
-// window sum of every column of the strip (plus r halo columns each side)
-// lives in shared memory and slides: each row step adds the row entering the
-// window and subtracts the row leaving it.  Each lane then forms the
-// horizontal window sums of PL = WS / 32 adjacent output columns, sliding
-// across them.  Every pixel's statistics are computed once.
+// rows.  The vertical window sum of every column of the strip (plus r halo
+// columns each side) lives in shared memory and slides: each row step adds
+// the row entering the window and subtracts the row leaving it.  Each lane
+// then forms the horizontal window sums of 4 adjacent output columns, sliding
+// across them.  Every pixel's statistics are computed once, all sums are in
+// double, and HBM carries the a/b planes between the two box levels.
 //   pass A: G, G^2, R, G R, B, G B -> a_R, b_R, a_B, b_B, |grad G| (float planes)
 //   pass B: box means of those five -> blended output
-//
-// Sums are float.  The reference forms its box means from double summed-area
-// tables; float sliding sums of the same window differ by rounding only.
-// A sliding sum's rounding depends on where it started, so the vertical sums
-// restart at fixed block rows (every B rows, B = the smallest power of two
-// above 2r, at least 16): there the window sum is the fresh sum of its 2r + 1
-// rows in order, accumulated from the rows entering the window during the
-// block's last 2r steps.  Strips and row bands start on block rows, so every
-// strip height and band split gives the same bits.  And
-// pass A sums the normalised samples centred at 0.5 (x - 0.5), which keeps
-// the partial sums small wherever the image is near that level: the
-// variance and covariance are shift-invariant, and the means get the 0.5
-// back before b = mean(X) - a mean(G) is formed.  Measured against the
-// reference CPU accelerator the output moves by at most ~1e-5 (tests bound
-// it at 1e-4), with the window sums at half the shared-memory footprint and
-// instruction count of double sums.
+// Window sums use the same truncated windows, area reciprocals and float /
+// double conversions as the fused kernel; only the summation order differs.
+// A strip is WS = 32 * PL columns: each lane forms the horizontal sums of PL
+// adjacent output columns (PL = 4 or 2).
 
-// Column j of a strip's shared-memory window sums, one pad slot per 4
-// floats: lanes reading 4 columns apart then hit 32 distinct banks.
-__device__ __forceinline__ int fidx(int j) { return j + (j >> 2); }
+// Column j of a strip's shared-memory window sums, with one pad slot per 16
+// doubles: lanes reading 4 apart then hit 16 distinct 8-byte bank pairs.
+__device__ __forceinline__ int vidx(int j) { return j + (j >> 4); }
 template <int WS>
-__host__ __device__ constexpr int fvs_len() { return (WS + 32) + (WS + 32) / 4 + 1; }
+__host__ __device__ constexpr int vs_len() { return (WS + 32) + (WS + 32) / 16 + 1; }
 
-enum : int { kSlide = 0, kSlideStart = 1, kSlideAcc = 2, kRestart = 3 };
+// Quantities of pass A at (x, y) of the normalised image (zeros outside).
+struct AbQ {
+  __device__ static void load(const float* __restrict__ src, int W, int H, int x, int y, float inv_norm, double* q) {
+    float g = 0.f, rr = 0.f, b = 0.f;
+    if (x >= 0 && x < W && y >= 0 && y < H) {
+      const float* p = src + ((size_t)y * W + x) * 3;
+      rr = p[0] * inv_norm;
+      g = p[1] * inv_norm;
+      b = p[2] * inv_norm;
+    }
+    q[0] = (double)g;
+    q[1] = (double)(g * g);
+    q[2] = (double)rr;
+    q[3] = (double)(g * rr);
+    q[4] = (double)b;
+    q[5] = (double)(g * b);
+  }
+};
 
-// One row step of a strip's vertical window sums: the row entering and the
-// row leaving the window, fetched as raw samples one step ahead of its use
-// (issued after the step's last __syncwarp, so the loads stay in flight
-// while the warp writes the current row's outputs).
-template <int NR, int WS>
-struct FStep {
+template <int NQ, int WS, typename Loader>
+__device__ __forceinline__ void strip_update(double (*Vs)[vs_len<WS>()], int VC, int xv0, int y_add, int y_sub, Loader ld) {
+  for (int j = threadIdx.x; j < VC; j += 32) {
+    double qa[NQ], qs[NQ];
+    const int x = xv0 + j;
+    ld(x, y_add, qa);
+    ld(x, y_sub, qs);
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+      double v = Vs[q][vidx(j)];
+      v += qa[q];
+      v -= qs[q];
+      Vs[q][vidx(j)] = v;
+    }
+  }
+}
+
+// One row step of a strip's vertical window sums (the row entering and the
+// row leaving the window), fetched as raw samples one step ahead of its use.
+// The fetch is issued after the step's last __syncwarp, so the loads stay in
+// flight while the warp writes the current row's outputs.  The per-sample
+// doubles and the order of the additions are those of strip_update.
+template <int NQ, int NR, int WS>
+struct StripStep {
   static constexpr int SL = WS / 32 + 1;  // window columns per lane: WS + 2r <= WS + 32
   float add[SL][NR], sub[SL][NR];
-  bool add_ok[SL], sub_ok[SL];
   template <typename Fetch>
-  __device__ __forceinline__ void fetch(int lane, int VC, int xv0, int y_add, int y_sub, Fetch f) {
+  __device__ __forceinline__ void fetch(int VC, int xv0, int y_add, int y_sub, Fetch f) {
 #pragma unroll
     for (int s = 0; s < SL; s++) {
-      const int j = lane + 32 * s;
-      add_ok[s] = sub_ok[s] = false;
+      const int j = threadIdx.x + 32 * s;
       if (j < VC) {
-        add_ok[s] = f(xv0 + j, y_add, add[s]);
-        sub_ok[s] = f(xv0 + j, y_sub, sub[s]);
+        f(xv0 + j, y_add, add[s]);
+        f(xv0 + j, y_sub, sub[s]);
       }
     }
   }
-  // mode kSlide: V += entering - leaving; kSlideStart / kSlideAcc: the
-  // same, and the fresh sum S of the next block row starts at / adds the
-  // entering row; kRestart: V = S + entering (the fresh window sum).
-  template <int NQ, typename Conv>
-  __device__ __forceinline__ void apply(float (*Vs)[fvs_len<WS>()], float (*Ss)[fvs_len<WS>()], int lane, int VC,
-                                        int mode, Conv cv) const {
+  template <typename Conv>
+  __device__ __forceinline__ void apply(double (*Vs)[vs_len<WS>()], int VC, Conv cv) const {
 #pragma unroll
     for (int s = 0; s < SL; s++) {
-      const int j = lane + 32 * s;
+      const int j = threadIdx.x + 32 * s;
       if (j < VC) {
-        float qa[NQ], qs[NQ];
-        cv(add[s], add_ok[s], qa);
-        cv(sub[s], sub_ok[s], qs);
+        double qa[NQ], qs[NQ];
+        cv(add[s], qa);
+        cv(sub[s], qs);
 #pragma unroll
         for (int q = 0; q < NQ; q++) {
-          float v;
-          if (mode == kRestart) {
-            v = Ss[q][fidx(j)] + qa[q];
-          } else {
-            v = Vs[q][fidx(j)];
-            v += qa[q];
-            v -= qs[q];
-            if (mode == kSlideStart) Ss[q][fidx(j)] = qa[q];
-            else if (mode == kSlideAcc) Ss[q][fidx(j)] += qa[q];
-          }
-          Vs[q][fidx(j)] = v;
+          double v = Vs[q][vidx(j)];
+          v += qa[q];
+          v -= qs[q];
+          Vs[q][vidx(j)] = v;
         }
       }
     }
   }
 };
 
-// Block rows of the vertical sums for radius r (see above).
-__host__ __device__ inline int ax_block_rows(int r) {
-  int b = 16;
-  while (b <= 2 * r) b *= 2;
-  return b;
-}
-// Update mode of the row step that brings the window to row y (y > the
-// strip's first row, which starts from the fresh sum of its prologue).
-__device__ __forceinline__ int ax_step_mode(int y, int r, int B) {
-  const int m = y & (B - 1);
-  if (m == 0) return kRestart;
-  if (m == B - 2 * r) return kSlideStart;
-  if (m > B - 2 * r) return kSlideAcc;
-  return kSlide;
-}
-
-// Horizontal window sums of the lane's PL output columns: hs[q][k].
+// Horizontal window sums of the lane's 4 output columns: hs[q][k].
 template <int NQ, int WS>
-__device__ __forceinline__ void fstrip_hsum(float (*Vs)[fvs_len<WS>()], int lane, int r, float hs[NQ][WS / 32]) {
+__device__ __forceinline__ void strip_hsum(double (*Vs)[vs_len<WS>()], int r, double hs[NQ][WS / 32]) {
   constexpr int PL = WS / 32;
-  const int c0 = lane * PL;
+  const int c0 = threadIdx.x * PL;
 #pragma unroll
   for (int q = 0; q < NQ; q++) {
-    float s = 0.f;
-    for (int t = 0; t <= 2 * r; t++) s += Vs[q][fidx(c0 + t)];
+    double s = 0.0;
+    for (int t = 0; t <= 2 * r; t++) s += Vs[q][vidx(c0 + t)];
     hs[q][0] = s;
 #pragma unroll
     for (int k = 1; k < PL; k++) {
-      s += Vs[q][fidx(c0 + k + 2 * r)];
-      s -= Vs[q][fidx(c0 + k - 1)];
+      s += Vs[q][vidx(c0 + k + 2 * r)];
+      s -= Vs[q][vidx(c0 + k - 1)];
       hs[q][k] = s;
     }
   }
 }
 
-// Strip (x0, y0) of a launch over row chunks [yb0, yb1): warp `w` of CTA
-// (bx, by) takes chunk yb0 + by * NW + w.
-struct StripPos {
-  int x0, y0;
-  bool ok;
-};
-template <int WS, int NW>
-__device__ __forceinline__ StripPos strip_pos(int HS, int yb0, int yb1) {
-  StripPos p;
-  const int chunk = yb0 + (int)blockIdx.y * NW + (int)(threadIdx.x >> 5);
-  p.x0 = blockIdx.x * WS;
-  p.y0 = chunk * HS;
-  p.ok = chunk < yb1;
-  return p;
-}
-
-constexpr int kAxWarps = 4;  // independent strips per CTA
-
 template <int WS>
-__global__ void __launch_bounds__(32 * kAxWarps, WS == 128 ? 4 : 5)
-    k_ax_ab(const float* __restrict__ src, int W, int H, int r, float eps, int HS, const float* __restrict__ d_maxg,
-            float* __restrict__ aR, float* __restrict__ bR, float* __restrict__ aB, float* __restrict__ bB,
-            float* __restrict__ er, int yb0, int yb1) {
+__global__ void __launch_bounds__(32, WS == 128 ? 16 : 20) k_ax_ab(const float* __restrict__ src, int W, int H, int r, float eps, int HS,
+                                             const float* __restrict__ d_maxg, float* __restrict__ aR,
+                                             float* __restrict__ bR, float* __restrict__ aB, float* __restrict__ bB,
+                                             float* __restrict__ er, int yb0) {
   constexpr int NQ = 6;
   constexpr int PL = WS / 32;
-  __shared__ float Vs_all[kAxWarps][NQ][fvs_len<WS>()];
-  __shared__ float Ss_all[kAxWarps][NQ][fvs_len<WS>()];
-  const StripPos sp = strip_pos<WS, kAxWarps>(HS, yb0, yb1);
-  if (!sp.ok) return;
-  const int lane = threadIdx.x & 31;
-  float (*Vs)[fvs_len<WS>()] = Vs_all[threadIdx.x >> 5];
-  float (*Ss)[fvs_len<WS>()] = Ss_all[threadIdx.x >> 5];
-  const int B = ax_block_rows(r);
+  __shared__ double Vs[NQ][vs_len<WS>()];
   const int VC = WS + 2 * r;
   const float inv_norm = 1.f / fmaxf(*d_maxg, 1e-6f);
-  const int x0 = sp.x0, y0 = sp.y0;
+  const int x0 = blockIdx.x * WS, y0 = (blockIdx.y + yb0) * HS;  // yb0: first row chunk of this launch
   const int xv0 = x0 - r;
   const int y_end = min(y0 + HS, H);
-  // raw (r, g, b) of the sample; false (and no contribution) outside the image
+  auto ld = [&](int x, int y, double* q) { AbQ::load(src, W, H, x, y, inv_norm, q); };
+  for (int j = threadIdx.x; j < VC; j += 32)
+#pragma unroll
+    for (int q = 0; q < NQ; q++) Vs[q][vidx(j)] = 0.0;
+  // window of the first output row: rows [y0 - r, y0 + r] (out-of-image rows load zeros)
+  for (int iy = y0 - r; iy <= y0 + r; iy++) strip_update<NQ, WS>(Vs, VC, xv0, iy, -1, ld);
+  double inv_cx[PL];
+#pragma unroll
+  for (int k = 0; k < PL; k++) {
+    const int x = x0 + threadIdx.x * PL + k;
+    inv_cx[k] = x < W ? 1.0 / (double)win_count(x, r, W) : 0.0;
+  }
+  // raw (r, g, b) of the sample, zeros outside the image; cv forms the six
+  // doubles exactly as AbQ::load does
   auto fetch = [&](int x, int y, float* v) {
     v[0] = v[1] = v[2] = 0.f;
     if (x >= 0 && x < W && y >= 0 && y < H) {
@@ -560,52 +539,33 @@ __global__ void __launch_bounds__(32 * kAxWarps, WS == 128 ? 4 : 5)
       v[0] = p[0];
       v[1] = p[1];
       v[2] = p[2];
-      return true;
     }
-    return false;
   };
-  // the six window quantities of the normalised sample centred at 0.5
-  auto cv = [&](const float* v, bool ok, float* q) {
-    const float rr = ok ? v[0] * inv_norm - 0.5f : 0.f;
-    const float g = ok ? v[1] * inv_norm - 0.5f : 0.f;
-    const float b = ok ? v[2] * inv_norm - 0.5f : 0.f;
-    q[0] = g;
-    q[1] = g * g;
-    q[2] = rr;
-    q[3] = g * rr;
-    q[4] = b;
-    q[5] = g * b;
+  auto cv = [&](const float* v, double* q) {
+    const float rr = v[0] * inv_norm, g = v[1] * inv_norm, b = v[2] * inv_norm;
+    q[0] = (double)g;
+    q[1] = (double)(g * g);
+    q[2] = (double)rr;
+    q[3] = (double)(g * rr);
+    q[4] = (double)b;
+    q[5] = (double)(g * b);
   };
-  for (int j = lane; j < VC; j += 32)
-#pragma unroll
-    for (int q = 0; q < NQ; q++) Vs[q][fidx(j)] = 0.f;
-  // window of the first output row: rows [y0 - r, y0 + r]
-  FStep<3, WS> step;
-  for (int iy = y0 - r; iy <= y0 + r; iy++) {
-    step.fetch(lane, VC, xv0, iy, -1, fetch);
-    step.template apply<NQ>(Vs, Ss, lane, VC, kSlide, cv);
-  }
-  float inv_cx[PL];
-#pragma unroll
-  for (int k = 0; k < PL; k++) {
-    const int x = x0 + lane * PL + k;
-    inv_cx[k] = x < W ? 1.f / (float)win_count(x, r, W) : 0.f;
-  }
+  StripStep<NQ, 3, WS> step;
   for (int y = y0; y < y_end; y++) {
-    if (y > y0) step.template apply<NQ>(Vs, Ss, lane, VC, ax_step_mode(y, r, B), cv);
+    if (y > y0) step.apply(Vs, VC, cv);
     __syncwarp();
-    float hs[NQ][PL];
-    fstrip_hsum<NQ, WS>(Vs, lane, r, hs);
+    double hs[NQ][PL];
+    strip_hsum<NQ, WS>(Vs, r, hs);
     __syncwarp();  // the next update rewrites Vs
-    if (y + 1 < y_end) step.fetch(lane, VC, xv0, y + 1 + r, y - r, fetch);
-    const float inv_cy = 1.f / (float)win_count(y, r, H);
+    if (y + 1 < y_end) step.fetch(VC, xv0, y + 1 + r, y - r, fetch);
+    const double inv_cy = 1.0 / (double)win_count(y, r, H);
 #pragma unroll
     for (int k = 0; k < PL; k++) {
-      const int x = x0 + lane * PL + k;
+      const int x = x0 + threadIdx.x * PL + k;
       if (x >= W) continue;
-      const float ia = inv_cx[k] * inv_cy;
-      const float mi = hs[0][k] * ia;  // mean(G) - 0.5
-      const float vi = hs[1][k] * ia - mi * mi;
+      const double ia = inv_cx[k] * inv_cy;
+      const double mi = hs[0][k] * ia;
+      const double vi = hs[1][k] * ia - mi * mi;
       const size_t o = (size_t)y * W + x;
       // |central gradient of G| (interior pixels), boxed by pass B
       float e = 0.f;
@@ -617,39 +577,58 @@ __global__ void __launch_bounds__(32 * kAxWarps, WS == 128 ? 4 : 5)
       er[o] = e;
 #pragma unroll
       for (int ch = 0; ch < 2; ch++) {
-        const float mp = hs[2 + 2 * ch][k] * ia, mIp = hs[3 + 2 * ch][k] * ia;
-        const float cov = mIp - mi * mp;
-        const float a = cov / (vi + eps);
-        const float b = (mp + 0.5f) - a * (mi + 0.5f);
-        (ch == 0 ? aR : aB)[o] = a;
-        (ch == 0 ? bR : bB)[o] = b;
+        const double mp = hs[2 + 2 * ch][k] * ia, mIp = hs[3 + 2 * ch][k] * ia;
+        const double cov = mIp - mi * mp;
+        const double a = cov / (vi + (double)eps);
+        const double b = mp - a * mi;
+        (ch == 0 ? aR : aB)[o] = (float)a;
+        (ch == 0 ? bR : bB)[o] = (float)b;
       }
     }
   }
 }
 
 template <int WS>
-__global__ void __launch_bounds__(32 * kAxWarps, WS == 128 ? 4 : 5)
-    k_ax_q(const float* __restrict__ src, float* __restrict__ dst, int W, int H, int r, float strength, int HS,
-           const float* __restrict__ d_maxg, const float* __restrict__ aR, const float* __restrict__ bR,
-           const float* __restrict__ aB, const float* __restrict__ bB, const float* __restrict__ er, int yb0,
-           int yb1) {
+__global__ void __launch_bounds__(32, WS == 128 ? 16 : 20) k_ax_q(const float* __restrict__ src, float* __restrict__ dst, int W, int H,
+                                            int r, float strength, int HS, const float* __restrict__ d_maxg,
+                                            const float* __restrict__ aR, const float* __restrict__ bR,
+                                            const float* __restrict__ aB, const float* __restrict__ bB,
+                                            const float* __restrict__ er, int yb0) {
   constexpr int NQ = 5;
   constexpr int PL = WS / 32;
-  __shared__ float Vs_all[kAxWarps][NQ][fvs_len<WS>()];
-  __shared__ float Ss_all[kAxWarps][NQ][fvs_len<WS>()];
-  const StripPos sp = strip_pos<WS, kAxWarps>(HS, yb0, yb1);
-  if (!sp.ok) return;
-  const int lane = threadIdx.x & 31;
-  float (*Vs)[fvs_len<WS>()] = Vs_all[threadIdx.x >> 5];
-  float (*Ss)[fvs_len<WS>()] = Ss_all[threadIdx.x >> 5];
-  const int B = ax_block_rows(r);
+  __shared__ double Vs[NQ][vs_len<WS>()];
   const int VC = WS + 2 * r;
   const float norm_ref = fmaxf(*d_maxg, 1e-6f);
   const float inv_norm = 1.f / norm_ref;
-  const int x0 = sp.x0, y0 = sp.y0;
+  const int x0 = blockIdx.x * WS, y0 = (blockIdx.y + yb0) * HS;  // yb0: first row chunk of this launch
   const int xv0 = x0 - r;
   const int y_end = min(y0 + HS, H);
+  auto ld = [&](int x, int y, double* q) {
+    float va = 0.f, vb = 0.f, vc = 0.f, vd = 0.f, e = 0.f;
+    if (x >= 0 && x < W && y >= 0 && y < H) {
+      const size_t i = (size_t)y * W + x;
+      va = aR[i];
+      vb = bR[i];
+      vc = aB[i];
+      vd = bB[i];
+      e = er[i];
+    }
+    q[0] = (double)va;
+    q[1] = (double)vb;
+    q[2] = (double)vc;
+    q[3] = (double)vd;
+    q[4] = (double)e;
+  };
+  for (int j = threadIdx.x; j < VC; j += 32)
+#pragma unroll
+    for (int q = 0; q < NQ; q++) Vs[q][vidx(j)] = 0.0;
+  for (int iy = y0 - r; iy <= y0 + r; iy++) strip_update<NQ, WS>(Vs, VC, xv0, iy, -1, ld);
+  double inv_cx[PL];
+#pragma unroll
+  for (int k = 0; k < PL; k++) {
+    const int x = x0 + threadIdx.x * PL + k;
+    inv_cx[k] = x < W ? 1.0 / (double)win_count(x, r, W) : 0.0;
+  }
   auto fetch = [&](int x, int y, float* v) {
     v[0] = v[1] = v[2] = v[3] = v[4] = 0.f;
     if (x >= 0 && x < W && y >= 0 && y < H) {
@@ -659,59 +638,40 @@ __global__ void __launch_bounds__(32 * kAxWarps, WS == 128 ? 4 : 5)
       v[2] = aB[i];
       v[3] = bB[i];
       v[4] = er[i];
-      return true;
     }
-    return false;
   };
-  auto cv = [](const float* v, bool, float* q) {
+  auto cv = [](const float* v, double* q) {
 #pragma unroll
-    for (int t = 0; t < 5; t++) q[t] = v[t];
+    for (int t = 0; t < 5; t++) q[t] = (double)v[t];
   };
-  for (int j = lane; j < VC; j += 32)
-#pragma unroll
-    for (int q = 0; q < NQ; q++) Vs[q][fidx(j)] = 0.f;
-  FStep<5, WS> step;
-  for (int iy = y0 - r; iy <= y0 + r; iy++) {
-    step.fetch(lane, VC, xv0, iy, -1, fetch);
-    step.template apply<NQ>(Vs, Ss, lane, VC, kSlide, cv);
-  }
-  float inv_cx[PL];
-#pragma unroll
-  for (int k = 0; k < PL; k++) {
-    const int x = x0 + lane * PL + k;
-    inv_cx[k] = x < W ? 1.f / (float)win_count(x, r, W) : 0.f;
-  }
+  StripStep<NQ, 5, WS> step;
   for (int y = y0; y < y_end; y++) {
-    if (y > y0) step.template apply<NQ>(Vs, Ss, lane, VC, ax_step_mode(y, r, B), cv);
+    if (y > y0) step.apply(Vs, VC, cv);
     __syncwarp();
-    float hs[NQ][PL];
-    fstrip_hsum<NQ, WS>(Vs, lane, r, hs);
+    double hs[NQ][PL];
+    strip_hsum<NQ, WS>(Vs, r, hs);
     __syncwarp();
-    if (y + 1 < y_end) step.fetch(lane, VC, xv0, y + 1 + r, y - r, fetch);
-    const float inv_cy = 1.f / (float)win_count(y, r, H);
+    if (y + 1 < y_end) step.fetch(VC, xv0, y + 1 + r, y - r, fetch);
+    const double inv_cy = 1.0 / (double)win_count(y, r, H);
 #pragma unroll
     for (int k = 0; k < PL; k++) {
-      const int x = x0 + lane * PL + k;
+      const int x = x0 + threadIdx.x * PL + k;
       if (x >= W) continue;
-      const float ia = inv_cx[k] * inv_cy;
+      const double ia = inv_cx[k] * inv_cy;
       const size_t o = ((size_t)y * W + x) * 3;
       const float R = src[o + 0] * inv_norm;
       const float G = src[o + 1];
       const float I = G * inv_norm;
       const float B = src[o + 2] * inv_norm;
-      const float qR = (hs[0][k] * ia) * I + hs[1][k] * ia;
-      const float qB = (hs[2][k] * ia) * I + hs[3][k] * ia;
-      const float tt = clampf((hs[4][k] * ia - 0.01f) / 0.05f, 0.f, 1.f);
+      const float qR = (float)((hs[0][k] * ia) * (double)I + hs[1][k] * ia);
+      const float qB = (float)((hs[2][k] * ia) * (double)I + hs[3][k] * ia);
+      const float tt = clampf(((float)(hs[4][k] * ia) - 0.01f) / 0.05f, 0.f, 1.f);
       const float w = strength * (tt * tt * (3.f - 2.f * tt));
       dst[o + 0] = (R * (1.f - w) + qR * w) * norm_ref;
       dst[o + 1] = G;
       dst[o + 2] = (B * (1.f - w) + qB * w) * norm_ref;
     }
   }
-}
-
-inline dim3 strip_grid(size_t w, int WS, int k0, int k1) {
-  return dim3((unsigned)((w + WS - 1) / WS), (unsigned)((k1 - k0 + kAxWarps - 1) / kAxWarps));
 }
 
 template <int WS>
@@ -723,11 +683,9 @@ cudaError_t axial_stream(size_t w, size_t h, int HS, cudaStream_t s, const float
   float* aB = planes + 2 * n;
   float* bB = planes + 3 * n;
   float* er = planes + 4 * n;
-  const int nch = (int)((h + HS - 1) / HS);
-  const dim3 grid = strip_grid(w, WS, 0, nch);
-  k_ax_ab<WS><<<grid, 32 * kAxWarps, 0, s>>>(src, (int)w, (int)h, r, eps, HS, d_max, aR, bR, aB, bB, er, 0, nch);
-  k_ax_q<WS><<<grid, 32 * kAxWarps, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max, aR, bR, aB, bB, er, 0,
-                                           nch);
+  dim3 grid((unsigned)((w + WS - 1) / WS), (unsigned)((h + HS - 1) / HS));
+  k_ax_ab<WS><<<grid, 32, 0, s>>>(src, (int)w, (int)h, r, eps, HS, d_max, aR, bR, aB, bB, er, 0);
+  k_ax_q<WS><<<grid, 32, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max, aR, bR, aB, bB, er, 0);
   return cudaPeekAtLastError();
 }
 
@@ -737,9 +695,9 @@ cudaError_t axial_pass_a(size_t w, size_t h, int HS, int k0, int k1, cudaStream_
                          float eps, const float* d_max, float* planes) {
   if (k1 <= k0) return cudaSuccess;
   const size_t n = w * h;
-  k_ax_ab<WS><<<strip_grid(w, WS, k0, k1), 32 * kAxWarps, 0, s>>>(src, (int)w, (int)h, r, eps, HS, d_max, planes,
-                                                                  planes + n, planes + 2 * n, planes + 3 * n,
-                                                                  planes + 4 * n, k0, k1);
+  dim3 grid((unsigned)((w + WS - 1) / WS), (unsigned)(k1 - k0));
+  k_ax_ab<WS><<<grid, 32, 0, s>>>(src, (int)w, (int)h, r, eps, HS, d_max, planes, planes + n, planes + 2 * n,
+                                  planes + 3 * n, planes + 4 * n, k0);
   return cudaPeekAtLastError();
 }
 template <int WS>
@@ -747,11 +705,12 @@ cudaError_t axial_pass_b(size_t w, size_t h, int HS, int k0, int k1, cudaStream_
                          int r, float strength, const float* d_max, float* planes) {
   if (k1 <= k0) return cudaSuccess;
   const size_t n = w * h;
-  k_ax_q<WS><<<strip_grid(w, WS, k0, k1), 32 * kAxWarps, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max,
-                                                                 planes, planes + n, planes + 2 * n, planes + 3 * n,
-                                                                 planes + 4 * n, k0, k1);
+  dim3 grid((unsigned)((w + WS - 1) / WS), (unsigned)(k1 - k0));
+  k_ax_q<WS><<<grid, 32, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max, planes, planes + n,
+                                 planes + 2 * n, planes + 3 * n, planes + 4 * n, k0);
   return cudaPeekAtLastError();
 }
+
 }  // namespace
 
 size_t ws_bytes_axial(size_t w, size_t h, int radius) {
@@ -779,7 +738,6 @@ lre_status launch_axial_ca_banded(Context* c, const float* in, float* out, size_
   bands = std::max(1, bands);
   int HS = c->tune.axial_rows == 128 ? 128 : 64;
   while (HS > 16 && strips_x * ((h + HS - 1) / HS) < want * (size_t)bands) HS /= 2;
-  HS = std::max(HS, ax_block_rows(radius));  // strips start on block rows
   // pass B of a chunk reads pass A's planes up to `radius` (<= HS) rows below
   // it, so pass A runs one band ahead of pass B
   const int nch = (int)((h + HS - 1) / HS);
@@ -832,7 +790,6 @@ lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, si
   const size_t want = (size_t)c->sm_count * 24;
   int HS = c->tune.axial_rows == 128 ? 128 : 64;
   while (HS > 16 && strips_x * ((h + HS - 1) / HS) < want) HS /= 2;
-  HS = std::max(HS, ax_block_rows(radius));  // strips start on block rows
   LRE_CUDA_TRY(c, WS == 64 ? axial_stream<64>(w, h, HS, c->stream, src, out, radius, eps, strength, d_max_g, planes)
                            : axial_stream<128>(w, h, HS, c->stream, src, out, radius, eps, strength, d_max_g, planes));
   count_launch(c, 2);
