@@ -462,9 +462,9 @@ __device__ __forceinline__ float line_along(const float* s_ls, int c) {
   return along;
 }
 
-// A direction's contribution to a pixel's line support, given its `along`.
-template <int TX, int TY>
-__device__ __forceinline__ void line_update(const float* s_fs, int c, float along, float& best) {
+template <int TX, int TY, int STEPS>
+__device__ __forceinline__ void line_dir(const float* s_ls, const float* s_fs, int c, float& best) {
+  const float along = line_along<TX, TY, STEPS>(s_ls, c);
   // along == 0 contributes 0 * thin (thin in [0, 1], or NaN which
   // std::max ignores) to a running max that is already >= 0
   if (along == 0.f) return;
@@ -474,33 +474,7 @@ __device__ __forceinline__ void line_update(const float* s_fs, int c, float alon
   best = smax(best, along * thin);
 }
 
-template <int TX, int TY, int STEPS>
-__device__ __forceinline__ void line_dir(const float* s_ls, const float* s_fs, int c, float& best) {
-  line_update<TX, TY>(s_fs, c, line_along<TX, TY, STEPS>(s_ls, c), best);
-}
-
-// Two pixels c and c + d next to each other along the direction d share all
-// but four of their line samples: with M the running max of the shared
-// samples (steps -(STEPS-1)..-1 and 2..STEPS from c),
-//   along(c)     = max(M, s[c - STEPS d], s[c + d]),
-//   along(c + d) = max(M, s[c], s[c + (STEPS + 1) d]).
-// fmaxf is exact and ignores NaN in any order, so both equal line_along's.
-template <int TX, int TY, int STEPS>
-__device__ __forceinline__ void line_dir_pair(const float* s_ls, const float* s_fs, int c, float& best0,
-                                              float& best1) {
-  constexpr int D = TY * LE + TX;
-  float m = 0.f;
-#pragma unroll
-  for (int step = 1; step <= STEPS - 1; step++) m = fmaxf(m, s_ls[c - D * step]);
-#pragma unroll
-  for (int step = 2; step <= STEPS; step++) m = fmaxf(m, s_ls[c + D * step]);
-  const float a0 = fmaxf(fmaxf(m, s_ls[c - D * STEPS]), s_ls[c + D]);
-  const float a1 = fmaxf(fmaxf(m, s_ls[c]), s_ls[c + D * (STEPS + 1)]);
-  line_update<TX, TY>(s_fs, c, a0, best0);
-  line_update<TX, TY>(s_fs, c + D, a1, best1);
-}
-
-__global__ void __launch_bounds__(256, 3) k_df_line(const float* __restrict__ src, int W, int H, DfPlanes P, DfConst k) {
+__global__ void __launch_bounds__(256) k_df_line(const float* __restrict__ src, int W, int H, DfPlanes P, DfConst k) {
   __shared__ float s_ls[LE * LE];
   __shared__ float s_fs[LE * LE];
   __shared__ int s_any;
@@ -525,77 +499,48 @@ __global__ void __launch_bounds__(256, 3) k_df_line(const float* __restrict__ sr
   const bool tile_active = s_any != 0;
   const float sensitivity = sclamp(sqrtf(smax(k.strength, 1.0f)), 1.0f, 2.5f);
   const float inv_s = 1.0f / sensitivity;
-  // One 2x2 pixel block per thread (256 threads, 16 x 16 blocks): pixels
-  // next to each other along a line direction share most line samples
-  // (line_dir_pair).  The solo-seed operands of the four pixels are loaded
-  // first, so their latency overlaps the line search (shared memory only).
-  static_assert((LT / 2) * (LT / 2) == 256, "k_df_line runs 256 threads, one per 2x2 block");
-  const int lx0 = 2 * ((int)threadIdx.x % (LT / 2)), ly0 = 2 * ((int)threadIdx.x / (LT / 2));
-  const int c0 = (ly0 + LH) * LE + (lx0 + LH);
-  float s0[4], s1[4], s2[4], blur_guide[4], blrg[4], blbg[4], bfs[4], be[4], ber[4];
-  bool on[4];
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int x = x0 + lx0 + (q & 1), y = y0 + ly0 + (q >> 1);
-    on[q] = x < W && y < H;
-    s0[q] = s1[q] = s2[q] = blur_guide[q] = blrg[q] = blbg[q] = bfs[q] = be[q] = ber[q] = 0.f;
-    if (on[q]) {
-      const size_t gi = (size_t)y * W + x;
-      const float* sp = src + gi * 3;
-      s0[q] = sp[0];
-      s1[q] = sp[1];
-      s2[q] = sp[2];
-      blur_guide[q] = P.bg[gi];
-      blrg[q] = P.blrg[gi];
-      blbg[q] = P.blbg[gi];
-      bfs[q] = P.bfs[gi];
-      be[q] = P.be[gi];
-      ber[q] = P.ber[gi];
+  for (int i = threadIdx.x; i < LT * LT; i += blockDim.x) {
+    int ly = i / LT, lx = i % LT;
+    int y = y0 + ly, x = x0 + lx;
+    if (x >= W || y >= H) continue;
+    const int c = (ly + LH) * LE + (lx + LH);
+    const size_t gi = (size_t)y * W + x;
+    // the solo-seed operands are loaded first, so their latency overlaps
+    // the line search (which reads shared memory only); loaded after the
+    // lfs store below, they would wait for it
+    const float* s = src + gi * 3;
+    const float s0 = s[0], s1 = s[1], s2 = s[2];
+    const float blur_guide = P.bg[gi];
+    const float blrg = P.blrg[gi], blbg = P.blbg[gi];
+    const float bfs = P.bfs[gi], be = P.be[gi], ber = P.ber[gi];
+    float best = 0.f;
+    if (tile_active) {
+      // directions and step counts of core/cpu_accelerator.cpp:4290-4318
+      line_dir<1, 0, 14>(s_ls, s_fs, c, best);
+      line_dir<0, 1, 14>(s_ls, s_fs, c, best);
+      line_dir<1, 1, 14>(s_ls, s_fs, c, best);
+      line_dir<1, -1, 14>(s_ls, s_fs, c, best);
+      line_dir<2, 1, 6>(s_ls, s_fs, c, best);
+      line_dir<1, 2, 6>(s_ls, s_fs, c, best);
+      line_dir<2, -1, 6>(s_ls, s_fs, c, best);
+      line_dir<1, -2, 6>(s_ls, s_fs, c, best);
     }
-  }
-  // pixel q sits at c0 + (q >> 1) * LE + (q & 1)
-  float best[4] = {0.f, 0.f, 0.f, 0.f};
-  if (tile_active) {
-    // directions and step counts of core/cpu_accelerator.cpp:4290-4318
-    line_dir_pair<1, 0, 14>(s_ls, s_fs, c0, best[0], best[1]);
-    line_dir_pair<1, 0, 14>(s_ls, s_fs, c0 + LE, best[2], best[3]);
-    line_dir_pair<0, 1, 14>(s_ls, s_fs, c0, best[0], best[2]);
-    line_dir_pair<0, 1, 14>(s_ls, s_fs, c0 + 1, best[1], best[3]);
-    line_dir_pair<1, 1, 14>(s_ls, s_fs, c0, best[0], best[3]);
-    line_dir<1, 1, 14>(s_ls, s_fs, c0 + 1, best[1]);
-    line_dir<1, 1, 14>(s_ls, s_fs, c0 + LE, best[2]);
-    line_dir_pair<1, -1, 14>(s_ls, s_fs, c0 + LE, best[2], best[1]);
-    line_dir<1, -1, 14>(s_ls, s_fs, c0, best[0]);
-    line_dir<1, -1, 14>(s_ls, s_fs, c0 + LE + 1, best[3]);
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const int c = c0 + (q >> 1) * LE + (q & 1);
-      line_dir<2, 1, 6>(s_ls, s_fs, c, best[q]);
-      line_dir<1, 2, 6>(s_ls, s_fs, c, best[q]);
-      line_dir<2, -1, 6>(s_ls, s_fs, c, best[q]);
-      line_dir<1, -2, 6>(s_ls, s_fs, c, best[q]);
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    if (!on[q]) continue;
-    const size_t gi = (size_t)(y0 + ly0 + (q >> 1)) * W + (x0 + lx0 + (q & 1));
-    P.lfs[gi] = best[q];
+    P.lfs[gi] = best;
 
     // solo seeds (core/cpu_accelerator.cpp:4325-4374)
-    const float g = smax(s1[q], 0.f);
-    const float target_r = g * exp_cr(blrg[q]);
-    const float target_b = g * exp_cr(blbg[q]);
-    const float solo_r = smax(0.f, s0[q] - target_r) / smax(blur_guide[q], 0.05f);
-    const float solo_b = smax(0.f, s2[q] - target_b) / smax(blur_guide[q], 0.05f);
-    const float linked_fringe = ssmooth(0.004f, 0.045f, smax(bfs[q], best[q] * 0.90f));
-    const float c_edge_solo = ssmooth(k.edge_thr * 0.35f * inv_s, k.edge_thr * 1.50f * inv_s, be[q]) *
-                              ssmooth(0.55f * inv_s, 1.35f * inv_s, ber[q]);
-    const float c_bright_solo = ssmooth(0.24f * inv_s, 0.52f * inv_s, blur_guide[q]);
+    const float g = smax(s1, 0.f);
+    const float target_r = g * exp_cr(blrg);
+    const float target_b = g * exp_cr(blbg);
+    const float solo_r = smax(0.f, s0 - target_r) / smax(blur_guide, 0.05f);
+    const float solo_b = smax(0.f, s2 - target_b) / smax(blur_guide, 0.05f);
+    const float linked_fringe = ssmooth(0.004f, 0.045f, smax(bfs, best * 0.90f));
+    const float c_edge_solo = ssmooth(k.edge_thr * 0.35f * inv_s, k.edge_thr * 1.50f * inv_s, be) *
+                              ssmooth(0.55f * inv_s, 1.35f * inv_s, ber);
+    const float c_bright_solo = ssmooth(0.24f * inv_s, 0.52f * inv_s, blur_guide);
     const float solo_enable = ssmooth(1.25f, 3.0f, k.strength);
-    const float r0 = smax(s0[q], 0.f);
-    const float g0 = smax(s1[q], 0.f);
-    const float b0 = smax(s2[q], 0.f);
+    const float r0 = smax(s0, 0.f);
+    const float g0 = smax(s1, 0.f);
+    const float b0 = smax(s2, 0.f);
     const float red_strength_solo = smax(0.f, r0 - smax(g0, b0)) / smax(r0, 1e-4f);
     const float solo_red_guard = 1.f - 0.90f * ssmooth(0.12f, 0.32f, red_strength_solo);
     P.srs[gi] = solo_enable * c_edge_solo * c_bright_solo * linked_fringe * solo_red_guard *
