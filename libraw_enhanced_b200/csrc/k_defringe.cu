@@ -237,12 +237,87 @@ __device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsig
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
   return r;
 }
-// a * b + c per lane with one rounding
-__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
-                                                     unsigned long long c) {
-  unsigned long long r;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-  return r;
+// acc + w * x per lane, the product and the sum each rounded to nearest.
+// Packed (EXACT = false): one mul.rn.f32x2 and one add.rn.f32x2, which flush
+// subnormal operands and results to zero (measured on B200); scalar
+// (EXACT = true): IEEE operations with gradual underflow, as the reference.
+template <bool EXACT>
+__device__ __forceinline__ unsigned long long f2_madd(unsigned long long acc, unsigned long long w,
+                                                      unsigned long long x) {
+  if (EXACT) {
+    float a0, a1, w0, w1, x0, x1;
+    f2_unpack(acc, a0, a1);
+    f2_unpack(w, w0, w1);
+    f2_unpack(x, x0, x1);
+    return f2_pack(__fadd_rn(a0, __fmul_rn(w0, x0)), __fadd_rn(a1, __fmul_rn(w1, x1)));
+  }
+  return f2_add(acc, f2_mul(w, x));
+}
+
+// Below this magnitude a nonzero blur input could, through the two passes'
+// products and partial sums, reach a subnormal, where the packed
+// instructions differ from the reference's arithmetic.
+constexpr float kBlurTiny = 0x1p-50f;
+// With every input 0 or of magnitude >= 2^-50 and every tap >= 2^-15, each
+// horizontal product is >= 2^-65 and each horizontal partial sum is 0 or a
+// multiple of 2^-88; each vertical product is >= 2^-103 and each vertical
+// partial sum 0 or a multiple of 2^-126: all normal, so the packed and the
+// scalar forms round identically.
+constexpr float kBlurMinTap = 0x1p-15f;
+
+// The two separable passes of one plane on the tile in shared memory.
+template <int KS, int TB, bool EXACT>
+__device__ __forceinline__ void blur_passes(const float* s_in, float* s_h, const float (&w)[2 * KS + 1], float* out,
+                                            int x0, int y0, int W, int H) {
+  constexpr int E = TB + 2 * KS;
+  constexpr int LD = E + 1;
+  // horizontal: item = (halo rows 2jp, 2jp + 1; group of 8 output columns)
+  for (int item = threadIdx.x; item < (E / 2) * (TB / 8); item += blockDim.x) {
+    const int j = (item / (TB / 8)) * 2, k0 = (item % (TB / 8)) * 8;
+    unsigned long long x[8 + 2 * KS];
+#pragma unroll
+    for (int i = 0; i < 8 + 2 * KS; i++) x[i] = f2_pack(s_in[j * LD + k0 + i], s_in[(j + 1) * LD + k0 + i]);
+    unsigned long long acc[8];
+#pragma unroll
+    for (int o = 0; o < 8; o++) acc[o] = 0ull;  // {+0.f, +0.f}
+#pragma unroll
+    for (int t = 0; t <= 2 * KS; t++) {
+      const unsigned long long wt = f2_pack(w[t], w[t]);
+#pragma unroll
+      for (int o = 0; o < 8; o++) acc[o] = f2_madd<EXACT>(acc[o], wt, x[o + t]);
+    }
+#pragma unroll
+    for (int o = 0; o < 8; o++) f2_unpack(acc[o], s_h[j * TB + k0 + o], s_h[(j + 1) * TB + k0 + o]);
+  }
+  __syncthreads();
+  // vertical: item = (output columns 2kp, 2kp + 1; group of 4 output rows)
+  for (int item = threadIdx.x; item < (TB / 2) * (TB / 4); item += blockDim.x) {
+    const int k = (item % (TB / 2)) * 2, j0 = (item / (TB / 2)) * 4;
+    unsigned long long x[4 + 2 * KS];
+#pragma unroll
+    for (int i = 0; i < 4 + 2 * KS; i++) x[i] = *reinterpret_cast<const unsigned long long*>(&s_h[(j0 + i) * TB + k]);
+    unsigned long long acc[4];
+#pragma unroll
+    for (int o = 0; o < 4; o++) acc[o] = 0ull;
+#pragma unroll
+    for (int t = 0; t <= 2 * KS; t++) {
+      const unsigned long long wt = f2_pack(w[t], w[t]);
+#pragma unroll
+      for (int o = 0; o < 4; o++) acc[o] = f2_madd<EXACT>(acc[o], wt, x[o + t]);
+    }
+    const int gx = x0 + k;
+#pragma unroll
+    for (int o = 0; o < 4; o++) {
+      float a, b;
+      f2_unpack(acc[o], a, b);
+      const int gy = y0 + j0 + o;
+      if (gy < H) {
+        if (gx < W) out[(size_t)gy * W + gx] = a;
+        if (gx + 1 < W) out[(size_t)gy * W + gx + 1] = b;
+      }
+    }
+  }
+  __syncthreads();
 }
 
 template <int KS, int TB>
@@ -255,8 +330,12 @@ __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTa
   float* s_h = sm_fast + E * LD;   // [E][TB]
   const int x0 = blockIdx.x * TB, y0 = blockIdx.y * TB;
   float w[2 * KS + 1];
+  bool taps_ok = true;
 #pragma unroll
-  for (int t = 0; t <= 2 * KS; t++) w[t] = taps.w[t];
+  for (int t = 0; t <= 2 * KS; t++) {
+    w[t] = taps.w[t];
+    taps_ok &= w[t] >= kBlurMinTap;
+  }
   for (int p = 0; p < job.np; p++) {
     const float* in = pick5(job.in, p);
     const int mode = pick5(job.mode, p);
@@ -264,6 +343,7 @@ __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTa
     // clamped halo, one row per warp and step, lanes across the row; the
     // source mode and the edge normaliser (1 / max_edge, as blur_src forms
     // it) are fixed for the plane
+    int tiny = 0;
     {
       const int warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31, nwarps = (int)blockDim.x >> 5;
       const float edge_inv = 1.f / smax(sc->max_edge, 1e-6f);
@@ -276,65 +356,19 @@ __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTa
           if (mode == BS_GUIDE_LINEAR) v = smax(row[(size_t)gx * 3 + 1], 0.f);
           else if (mode == BS_PLANE_EDGE_NORM) v = row[gx] * edge_inv;
           else v = row[gx];
+          tiny |= v != 0.f && !(fabsf(v) >= kBlurTiny);
           s_in[r * LD + q] = v;
         }
       }
     }
-    __syncthreads();
-    // Both passes run two outputs per packed f32x2 fused multiply-add, one
-    // instruction per tap and output pair.  Every output accumulates its
-    // taps in the reference's order from 0.f; each tap's product and sum
-    // are rounded once (fused) instead of twice, and the packed form
-    // flushes subnormal operands and results (measured on B200).  Both move
-    // a blurred value by a few float ulps, inside the defringe tolerance.
-    // horizontal: item = (halo rows 2jp, 2jp + 1; group of 8 output columns)
-    for (int item = threadIdx.x; item < (E / 2) * (TB / 8); item += blockDim.x) {
-      const int j = (item / (TB / 8)) * 2, k0 = (item % (TB / 8)) * 8;
-      unsigned long long x[8 + 2 * KS];
-#pragma unroll
-      for (int i = 0; i < 8 + 2 * KS; i++) x[i] = f2_pack(s_in[j * LD + k0 + i], s_in[(j + 1) * LD + k0 + i]);
-      unsigned long long acc[8];
-#pragma unroll
-      for (int o = 0; o < 8; o++) acc[o] = 0ull;  // {+0.f, +0.f}
-#pragma unroll
-      for (int t = 0; t <= 2 * KS; t++) {
-        const unsigned long long wt = f2_pack(w[t], w[t]);
-#pragma unroll
-        for (int o = 0; o < 8; o++) acc[o] = f2_fma(wt, x[o + t], acc[o]);
-      }
-#pragma unroll
-      for (int o = 0; o < 8; o++) f2_unpack(acc[o], s_h[j * TB + k0 + o], s_h[(j + 1) * TB + k0 + o]);
-    }
-    __syncthreads();
-    // vertical: item = (output columns 2kp, 2kp + 1; group of 4 output rows)
-    for (int item = threadIdx.x; item < (TB / 2) * (TB / 4); item += blockDim.x) {
-      const int k = (item % (TB / 2)) * 2, j0 = (item / (TB / 2)) * 4;
-      unsigned long long x[4 + 2 * KS];
-#pragma unroll
-      for (int i = 0; i < 4 + 2 * KS; i++)
-        x[i] = *reinterpret_cast<const unsigned long long*>(&s_h[(j0 + i) * TB + k]);
-      unsigned long long acc[4];
-#pragma unroll
-      for (int o = 0; o < 4; o++) acc[o] = 0ull;
-#pragma unroll
-      for (int t = 0; t <= 2 * KS; t++) {
-        const unsigned long long wt = f2_pack(w[t], w[t]);
-#pragma unroll
-        for (int o = 0; o < 4; o++) acc[o] = f2_fma(wt, x[o + t], acc[o]);
-      }
-      const int gx = x0 + k;
-#pragma unroll
-      for (int o = 0; o < 4; o++) {
-        float a, b;
-        f2_unpack(acc[o], a, b);
-        const int gy = y0 + j0 + o;
-        if (gy < H) {
-          if (gx < W) out[(size_t)gy * W + gx] = a;
-          if (gx + 1 < W) out[(size_t)gy * W + gx + 1] = b;
-        }
-      }
-    }
-    __syncthreads();
+    // Both passes run two outputs per packed f32x2 multiply and add, at half
+    // the FP instruction count, and every output accumulates its taps in the
+    // reference's order from 0.f with each product and sum rounded to
+    // nearest.  The packed forms flush subnormals, so a tile whose inputs
+    // could lead there (kBlurTiny; NaN counts) runs the scalar IEEE form.
+    const bool exact = __syncthreads_or(tiny) != 0 || !taps_ok;
+    if (exact) blur_passes<KS, TB, true>(s_in, s_h, w, out, x0, y0, W, H);
+    else blur_passes<KS, TB, false>(s_in, s_h, w, out, x0, y0, W, H);
   }
 }
 
