@@ -193,40 +193,6 @@ __device__ __forceinline__ float s3_finish(float h, float c, float cm, float cp,
   return h;
 }
 
-// In-place Gauss-Seidel sweep of a half-indexed weight plane (hvwt in stage
-// 6, :1456-1464; pmwt in stage 9, :1537-1542) over rows [a, rr1 - a): site
-// (rr, cc), cc = a + (row's R/B column parity) + 2k < cc1 - a, takes the
-// mean of its four diagonal neighbours when that is closer to 0.5, reading
-// row rr - 1 already swept and row rr + 1 not yet.  Sites of one row read
-// only other rows, and a row's diagonal neighbours are its neighbours'
-// sites k - 1 .. k + 1.  So one warp runs a 32-row band as a wavefront:
-// lane l (row rr) takes site k = t - 2l at step t.  At that step lane l - 1
-// has finished sites up to k + 1 of the row above and lane l + 1 has not yet
-// started site k - 1 of the row below, and the three lanes touch disjoint
-// sites: the reference's row-by-row order, with no CTA barrier per row.
-__device__ __forceinline__ void gs_sweep_warp(const AmazeArgs& A, float* w, int a, int rr1, int cc1, int lane) {
-  constexpr int m1 = TS + 1, p1 = -TS + 1;
-  const int nrows = rr1 - 2 * a;
-  const int per_row = (cc1 - a - a + 1) / 2 + 1;
-  for (int b0 = 0; b0 < nrows; b0 += 32) {
-    const int rr = a + b0 + lane;
-    const bool row_on = b0 + lane < nrows;
-    const int o = (int)(fc_rt(A, rr, 2) & 1);
-    const int nsteps = per_row + 2 * 31;
-    for (int t = 0; t < nsteps; t++) {
-      const int k = t - 2 * lane;
-      const int cc = a + o + 2 * k;
-      if (row_on && k >= 0 && cc < cc1 - a) {
-        const int idx = rr * TS + cc;
-        const float alt = 0.25f * (w[(idx - m1) >> 1] + w[(idx + p1) >> 1] + w[(idx - p1) >> 1] + w[(idx + m1) >> 1]);
-        const float cur = w[idx >> 1];
-        w[idx >> 1] = fabsf(0.5f - cur) < fabsf(0.5f - alt) ? alt : cur;
-      }
-      __syncwarp();
-    }
-  }
-}
-
 // Directional variance of three consecutive chain values (:1380-1381).
 __device__ __forceinline__ float s3_var(float a, float b, float c) {
   return 3.f * (SQR(a) + SQR(b) + SQR(c)) - SQR(a + b + c);
@@ -576,8 +542,18 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
       const int a = 8;
       const int per_row = rb_count(a);
       const FDiv fdr(per_row);
-      if (tid < 32) gs_sweep_warp(A, hvwt, a, rr1, cc1, tid);
-      __syncthreads();
+      for (int rr = a; rr < rr1 - a; rr++) {
+        for (int k = tid; k < per_row; k += nth) {
+          const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * k;
+          if (cc >= cc1 - a) continue;
+          const int idx = rr * TS + cc;
+          const float hvwtalt =
+              0.25f * (hvwt[(idx - m1) >> 1] + hvwt[(idx + p1) >> 1] + hvwt[(idx - p1) >> 1] + hvwt[(idx + m1) >> 1]);
+          const float cur = hvwt[idx >> 1];
+          hvwt[idx >> 1] = fabsf(0.5f - cur) < fabsf(0.5f - hvwtalt) ? hvwtalt : cur;
+        }
+        __syncthreads();
+      }
       for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
         const int q_ = fdr.div(i), rr = a + q_;
         const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i - q_ * per_row);
@@ -714,8 +690,18 @@ __global__ void __launch_bounds__(AMZ_THREADS, 1) k_amaze(AmazeArgs A) {
       const int a = 10;
       const int per_row = rb_count(a);
       const FDiv fdr(per_row);
-      if (tid < 32) gs_sweep_warp(A, pmwt, a, rr1, cc1, tid);
-      __syncthreads();
+      for (int rr = a; rr < rr1 - a; rr++) {
+        for (int k = tid; k < per_row; k += nth) {
+          const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * k;
+          if (cc >= cc1 - a) continue;
+          const int idx = rr * TS + cc, idx1 = idx >> 1;
+          const float pmwtalt =
+              0.25f * (pmwt[(idx - m1) >> 1] + pmwt[(idx + p1) >> 1] + pmwt[(idx - p1) >> 1] + pmwt[(idx + m1) >> 1]);
+          const float pw = pmwt[idx1];
+          if (fabsf(0.5f - pw) < fabsf(0.5f - pmwtalt)) pmwt[idx1] = pmwtalt;
+        }
+        __syncthreads();
+      }
       for (int i = tid; i < (rr1 - 2 * a) * per_row; i += nth) {
         const int q_ = fdr.div(i), rr = a + q_;
         const int cc = a + (fc_rt(A, rr, 2) & 1) + 2 * (i - q_ * per_row);
