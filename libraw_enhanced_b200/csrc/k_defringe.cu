@@ -23,6 +23,10 @@
 #include "lre_internal.h"
 #include "stencil.cuh"
 
+#ifndef LRE_BLUR_FORM
+#define LRE_BLUR_FORM 0
+#endif
+
 namespace lre {
 
 GaussTaps make_defringe_taps(float radius) {
@@ -237,36 +241,37 @@ __device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsig
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
   return r;
 }
-// acc + w * x per lane, the product and the sum each rounded to nearest.
-// Packed (EXACT = false): one mul.rn.f32x2 and one add.rn.f32x2, which flush
-// subnormal operands and results to zero (measured on B200); scalar
-// (EXACT = true): IEEE operations with gradual underflow, as the reference.
-template <bool EXACT>
+// acc + w * x per lane, the product and the sum each rounded to nearest
+// (the reference's order, no contraction): two IEEE scalar operations per
+// lane.  A packed mul.rn.f32x2 followed by add.rn.f32x2 gave the results of
+// a fused multiply-add on B200 (checked against these scalar operations),
+// and that single rounding flipped a classification on the 51 MP workload,
+// so the blurs keep the two roundings explicitly.
 __device__ __forceinline__ unsigned long long f2_madd(unsigned long long acc, unsigned long long w,
                                                       unsigned long long x) {
-  if (EXACT) {
-    float a0, a1, w0, w1, x0, x1;
-    f2_unpack(acc, a0, a1);
-    f2_unpack(w, w0, w1);
-    f2_unpack(x, x0, x1);
-    return f2_pack(__fadd_rn(a0, __fmul_rn(w0, x0)), __fadd_rn(a1, __fmul_rn(w1, x1)));
-  }
-  return f2_add(acc, f2_mul(w, x));
+#if LRE_BLUR_FORM == 1
+  // packed product, then fma(1, p, acc): a single rounding of p + acc
+  const unsigned long long one = f2_pack(1.f, 1.f);
+  const unsigned long long p = f2_mul(w, x);
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(one), "l"(p), "l"(acc));
+  return r;
+#elif LRE_BLUR_FORM == 2
+  unsigned long long r;
+  asm("{\n\t.reg .b64 t;\n\tmul.rn.f32x2 t, %1, %2;\n\tadd.rn.f32x2 %0, %3, t;\n\t}"
+      : "=l"(r) : "l"(w), "l"(x), "l"(acc));
+  return r;
+#else
+  float a0, a1, w0, w1, x0, x1;
+  f2_unpack(acc, a0, a1);
+  f2_unpack(w, w0, w1);
+  f2_unpack(x, x0, x1);
+  return f2_pack(__fadd_rn(a0, __fmul_rn(w0, x0)), __fadd_rn(a1, __fmul_rn(w1, x1)));
+#endif
 }
 
-// Below this magnitude a nonzero blur input could, through the two passes'
-// products and partial sums, reach a subnormal, where the packed
-// instructions differ from the reference's arithmetic.
-constexpr float kBlurTiny = 0x1p-50f;
-// With every input 0 or of magnitude >= 2^-50 and every tap >= 2^-15, each
-// horizontal product is >= 2^-65 and each horizontal partial sum is 0 or a
-// multiple of 2^-88; each vertical product is >= 2^-103 and each vertical
-// partial sum 0 or a multiple of 2^-126: all normal, so the packed and the
-// scalar forms round identically.
-constexpr float kBlurMinTap = 0x1p-15f;
-
 // The two separable passes of one plane on the tile in shared memory.
-template <int KS, int TB, bool EXACT>
+template <int KS, int TB>
 __device__ __forceinline__ void blur_passes(const float* s_in, float* s_h, const float (&w)[2 * KS + 1], float* out,
                                             int x0, int y0, int W, int H) {
   constexpr int E = TB + 2 * KS;
@@ -284,7 +289,7 @@ __device__ __forceinline__ void blur_passes(const float* s_in, float* s_h, const
     for (int t = 0; t <= 2 * KS; t++) {
       const unsigned long long wt = f2_pack(w[t], w[t]);
 #pragma unroll
-      for (int o = 0; o < 8; o++) acc[o] = f2_madd<EXACT>(acc[o], wt, x[o + t]);
+      for (int o = 0; o < 8; o++) acc[o] = f2_madd(acc[o], wt, x[o + t]);
     }
 #pragma unroll
     for (int o = 0; o < 8; o++) f2_unpack(acc[o], s_h[j * TB + k0 + o], s_h[(j + 1) * TB + k0 + o]);
@@ -303,7 +308,7 @@ __device__ __forceinline__ void blur_passes(const float* s_in, float* s_h, const
     for (int t = 0; t <= 2 * KS; t++) {
       const unsigned long long wt = f2_pack(w[t], w[t]);
 #pragma unroll
-      for (int o = 0; o < 4; o++) acc[o] = f2_madd<EXACT>(acc[o], wt, x[o + t]);
+      for (int o = 0; o < 4; o++) acc[o] = f2_madd(acc[o], wt, x[o + t]);
     }
     const int gx = x0 + k;
 #pragma unroll
@@ -330,12 +335,8 @@ __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTa
   float* s_h = sm_fast + E * LD;   // [E][TB]
   const int x0 = blockIdx.x * TB, y0 = blockIdx.y * TB;
   float w[2 * KS + 1];
-  bool taps_ok = true;
 #pragma unroll
-  for (int t = 0; t <= 2 * KS; t++) {
-    w[t] = taps.w[t];
-    taps_ok &= w[t] >= kBlurMinTap;
-  }
+  for (int t = 0; t <= 2 * KS; t++) w[t] = taps.w[t];
   for (int p = 0; p < job.np; p++) {
     const float* in = pick5(job.in, p);
     const int mode = pick5(job.mode, p);
@@ -343,7 +344,6 @@ __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTa
     // clamped halo, one row per warp and step, lanes across the row; the
     // source mode and the edge normaliser (1 / max_edge, as blur_src forms
     // it) are fixed for the plane
-    int tiny = 0;
     {
       const int warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31, nwarps = (int)blockDim.x >> 5;
       const float edge_inv = 1.f / smax(sc->max_edge, 1e-6f);
@@ -356,19 +356,15 @@ __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTa
           if (mode == BS_GUIDE_LINEAR) v = smax(row[(size_t)gx * 3 + 1], 0.f);
           else if (mode == BS_PLANE_EDGE_NORM) v = row[gx] * edge_inv;
           else v = row[gx];
-          tiny |= v != 0.f && !(fabsf(v) >= kBlurTiny);
           s_in[r * LD + q] = v;
         }
       }
     }
-    // Both passes run two outputs per packed f32x2 multiply and add, at half
-    // the FP instruction count, and every output accumulates its taps in the
-    // reference's order from 0.f with each product and sum rounded to
-    // nearest.  The packed forms flush subnormals, so a tile whose inputs
-    // could lead there (kBlurTiny; NaN counts) runs the scalar IEEE form.
-    const bool exact = __syncthreads_or(tiny) != 0 || !taps_ok;
-    if (exact) blur_passes<KS, TB, true>(s_in, s_h, w, out, x0, y0, W, H);
-    else blur_passes<KS, TB, false>(s_in, s_h, w, out, x0, y0, W, H);
+    __syncthreads();
+    // Both passes run two outputs per item and accumulate every output's
+    // taps in the reference's order from 0.f, each product and each sum
+    // rounded to nearest (f2_madd).
+    blur_passes<KS, TB>(s_in, s_h, w, out, x0, y0, W, H);
   }
 }
 
