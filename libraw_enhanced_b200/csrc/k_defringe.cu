@@ -23,10 +23,6 @@
 #include "lre_internal.h"
 #include "stencil.cuh"
 
-#ifndef LRE_BLUR_FORM
-#define LRE_BLUR_FORM 0
-#endif
-
 namespace lre {
 
 GaussTaps make_defringe_taps(float radius) {
@@ -221,8 +217,8 @@ __global__ void __launch_bounds__(256) k_df_blur(BlurJob job, GaussTaps taps, in
 // with 1.7x instead of 2.6x halo reads), each thread produces 8 horizontal
 // or 4 vertical outputs from operands held in registers.  Tap order and
 // clamping are those of k_df_blur.
-// Packed FP32 pairs (sm_100 f32x2): lane-wise round-to-nearest, the same
-// result as two scalar instructions for normal operands and results.
+// Two floats in one 64-bit register: a blur item carries the outputs of two
+// rows (horizontal pass) or two adjacent columns (vertical pass) together.
 __device__ __forceinline__ unsigned long long f2_pack(float a, float b) {
   unsigned long long r;
   asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
@@ -231,43 +227,21 @@ __device__ __forceinline__ unsigned long long f2_pack(float a, float b) {
 __device__ __forceinline__ void f2_unpack(unsigned long long v, float& a, float& b) {
   asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
 }
-__device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsigned long long b) {
-  unsigned long long r;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b) {
-  unsigned long long r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
 // acc + w * x per lane, the product and the sum each rounded to nearest
-// (the reference's order, no contraction): two IEEE scalar operations per
-// lane.  A packed mul.rn.f32x2 followed by add.rn.f32x2 gave the results of
-// a fused multiply-add on B200 (checked against these scalar operations),
-// and that single rounding flipped a classification on the 51 MP workload,
-// so the blurs keep the two roundings explicitly.
+// (the reference's order, no contraction), as two IEEE scalar operations per
+// lane.  The packed f32x2 forms cannot stand in: a probe of mul.rn.f32x2
+// followed by add.rn.f32x2 on B200 (as separate instructions, as one asm
+// block, or with the add written as fma.rn.f32x2(1, p, acc)) returned the
+// fused result, w * x + acc rounded once, on 12.6% of random pairs, and on
+// the 51 MP workload that single rounding flipped one pixel's
+// classification by 1.6e-3.
 __device__ __forceinline__ unsigned long long f2_madd(unsigned long long acc, unsigned long long w,
                                                       unsigned long long x) {
-#if LRE_BLUR_FORM == 1
-  // packed product, then fma(1, p, acc): a single rounding of p + acc
-  const unsigned long long one = f2_pack(1.f, 1.f);
-  const unsigned long long p = f2_mul(w, x);
-  unsigned long long r;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(one), "l"(p), "l"(acc));
-  return r;
-#elif LRE_BLUR_FORM == 2
-  unsigned long long r;
-  asm("{\n\t.reg .b64 t;\n\tmul.rn.f32x2 t, %1, %2;\n\tadd.rn.f32x2 %0, %3, t;\n\t}"
-      : "=l"(r) : "l"(w), "l"(x), "l"(acc));
-  return r;
-#else
   float a0, a1, w0, w1, x0, x1;
   f2_unpack(acc, a0, a1);
   f2_unpack(w, w0, w1);
   f2_unpack(x, x0, x1);
   return f2_pack(__fadd_rn(a0, __fmul_rn(w0, x0)), __fadd_rn(a1, __fmul_rn(w1, x1)));
-#endif
 }
 
 // The two separable passes of one plane on the tile in shared memory.
@@ -341,24 +315,11 @@ __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTa
     const float* in = pick5(job.in, p);
     const int mode = pick5(job.mode, p);
     float* out = pick5(job.out, p);
-    // clamped halo, one row per warp and step, lanes across the row; the
-    // source mode and the edge normaliser (1 / max_edge, as blur_src forms
-    // it) are fixed for the plane
-    {
-      const int warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31, nwarps = (int)blockDim.x >> 5;
-      const float edge_inv = 1.f / smax(sc->max_edge, 1e-6f);
-      for (int r = warp; r < E; r += nwarps) {
-        const int gy = min(max(y0 - KS + r, 0), H - 1);
-        const float* row = in + (size_t)gy * W * (mode == BS_GUIDE_LINEAR ? 3 : 1);
-        for (int q = lane; q < E; q += 32) {
-          const int gx = min(max(x0 - KS + q, 0), W - 1);
-          float v;
-          if (mode == BS_GUIDE_LINEAR) v = smax(row[(size_t)gx * 3 + 1], 0.f);
-          else if (mode == BS_PLANE_EDGE_NORM) v = row[gx] * edge_inv;
-          else v = row[gx];
-          s_in[r * LD + q] = v;
-        }
-      }
+    for (int i = threadIdx.x; i < E * E; i += blockDim.x) {
+      const int r = i / E, q = i % E;
+      const int gy = min(max(y0 - KS + r, 0), H - 1);
+      const int gx = min(max(x0 - KS + q, 0), W - 1);
+      s_in[r * LD + q] = blur_src(in, mode, sc, gx, gy, W);
     }
     __syncthreads();
     // Both passes run two outputs per item and accumulate every output's
