@@ -315,13 +315,26 @@ __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTa
     const float* in = pick5(job.in, p);
     const int mode = pick5(job.mode, p);
     float* out = pick5(job.out, p);
+    int nonzero = 0;
     for (int i = threadIdx.x; i < E * E; i += blockDim.x) {
       const int r = i / E, q = i % E;
       const int gy = min(max(y0 - KS + r, 0), H - 1);
       const int gx = min(max(x0 - KS + q, 0), W - 1);
-      s_in[r * LD + q] = blur_src(in, mode, sc, gx, gy, W);
+      const float v = blur_src(in, mode, sc, gx, gy, W);
+      nonzero |= v != 0.f;
+      s_in[r * LD + q] = v;
     }
-    __syncthreads();
+    // A halo of zeros (either sign) blurs to +0 everywhere: every product is
+    // a signed zero and every sum from +0 stays +0.  The sparse seed planes
+    // have many such tiles.
+    if (!__syncthreads_or(nonzero)) {
+      for (int i = threadIdx.x; i < TB * TB; i += blockDim.x) {
+        const int gx = x0 + i % TB, gy = y0 + i / TB;
+        if (gx < W && gy < H) out[(size_t)gy * W + gx] = 0.f;
+      }
+      __syncthreads();  // as after the passes: the support epilogue reads these
+      continue;
+    }
     // Both passes run two outputs per item and accumulate every output's
     // taps in the reference's order from 0.f, each product and each sum
     // rounded to nearest (f2_madd).
