@@ -29,6 +29,12 @@ __device__ __forceinline__ float sstep(float e0, float e1, float x) {
 
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
 
+// ACES filmic curve, core/cpu_accelerator.cpp:3048-3056.
+__device__ __forceinline__ float aces(float x) {
+  const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+  return (x * (a * x + b)) / (x * (c * x + d) + e);
+}
+
 // Median of three with the reference's swap network (shader_common.h:52-58).
 __device__ __forceinline__ float median3(float a, float b, float c) {
   if (a > b) { float t = a; a = b; b = t; }

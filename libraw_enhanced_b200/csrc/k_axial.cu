@@ -593,7 +593,8 @@ __global__ void __launch_bounds__(32, WS == 128 ? 16 : 20) k_ax_q(const float* _
                                             int r, float strength, int HS, const float* __restrict__ d_maxg,
                                             const float* __restrict__ aR, const float* __restrict__ bR,
                                             const float* __restrict__ aB, const float* __restrict__ bB,
-                                            const float* __restrict__ er, int yb0) {
+                                            const float* __restrict__ er, int yb0, bool tone,
+                                            float tone_scale) {
   constexpr int NQ = 5;
   constexpr int PL = WS / 32;
   __shared__ double Vs[NQ][vs_len<WS>()];
@@ -667,16 +668,22 @@ __global__ void __launch_bounds__(32, WS == 128 ? 16 : 20) k_ax_q(const float* _
       const float qB = (float)((hs[2][k] * ia) * (double)I + hs[3][k] * ia);
       const float tt = clampf(((float)(hs[4][k] * ia) - 0.01f) / 0.05f, 0.f, 1.f);
       const float w = strength * (tt * tt * (3.f - 2.f * tt));
-      dst[o + 0] = (R * (1.f - w) + qR * w) * norm_ref;
-      dst[o + 1] = G;
-      dst[o + 2] = (B * (1.f - w) + qB * w) * norm_ref;
+      float o0 = (R * (1.f - w) + qR * w) * norm_ref, o1 = G, o2 = (B * (1.f - w) + qB * w) * norm_ref;
+      if (tone) {  // the ACES stage that follows, applied to the stored floats
+        o0 = aces(o0) * tone_scale;
+        o1 = aces(o1) * tone_scale;
+        o2 = aces(o2) * tone_scale;
+      }
+      dst[o + 0] = o0;
+      dst[o + 1] = o1;
+      dst[o + 2] = o2;
     }
   }
 }
 
 template <int WS>
 cudaError_t axial_stream(size_t w, size_t h, int HS, cudaStream_t s, const float* src, float* out, int r, float eps,
-                         float strength, const float* d_max, float* planes) {
+                         float strength, const float* d_max, float* planes, bool tone, float tone_scale) {
   const size_t n = w * h;
   float* aR = planes;
   float* bR = planes + n;
@@ -685,7 +692,8 @@ cudaError_t axial_stream(size_t w, size_t h, int HS, cudaStream_t s, const float
   float* er = planes + 4 * n;
   dim3 grid((unsigned)((w + WS - 1) / WS), (unsigned)((h + HS - 1) / HS));
   k_ax_ab<WS><<<grid, 32, 0, s>>>(src, (int)w, (int)h, r, eps, HS, d_max, aR, bR, aB, bB, er, 0);
-  k_ax_q<WS><<<grid, 32, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max, aR, bR, aB, bB, er, 0);
+  k_ax_q<WS><<<grid, 32, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max, aR, bR, aB, bB, er, 0, tone,
+                                 tone_scale);
   return cudaPeekAtLastError();
 }
 
@@ -702,12 +710,12 @@ cudaError_t axial_pass_a(size_t w, size_t h, int HS, int k0, int k1, cudaStream_
 }
 template <int WS>
 cudaError_t axial_pass_b(size_t w, size_t h, int HS, int k0, int k1, cudaStream_t s, const float* src, float* out,
-                         int r, float strength, const float* d_max, float* planes) {
+                         int r, float strength, const float* d_max, float* planes, bool tone, float tone_scale) {
   if (k1 <= k0) return cudaSuccess;
   const size_t n = w * h;
   dim3 grid((unsigned)((w + WS - 1) / WS), (unsigned)(k1 - k0));
   k_ax_q<WS><<<grid, 32, 0, s>>>(src, out, (int)w, (int)h, r, strength, HS, d_max, planes, planes + n,
-                                 planes + 2 * n, planes + 3 * n, planes + 4 * n, k0);
+                                 planes + 2 * n, planes + 3 * n, planes + 4 * n, k0, tone, tone_scale);
   return cudaPeekAtLastError();
 }
 
@@ -723,7 +731,7 @@ size_t ws_bytes_axial(size_t w, size_t h, int radius) {
 
 lre_status launch_axial_ca_banded(Context* c, const float* in, float* out, size_t w, size_t h, int radius, float eps,
                                   float strength, const float* d_max_g, int bands,
-                                  const std::function<lre_status(size_t, size_t)>& rows_done) {
+                                  const std::function<lre_status(size_t, size_t)>& rows_done, float tone_scale) {
   if (radius < 1) radius = 1;
   if (radius > 16) return fail(c, LRE_ERR_INVALID_ARGUMENT, "ca_axial_cleanup: radius > 16 is not supported");
   if (in == out) return fail(c, LRE_ERR_INVALID_ARGUMENT, "ca_axial_cleanup: banded form runs out of place");
@@ -754,10 +762,11 @@ lre_status launch_axial_ca_banded(Context* c, const float* in, float* out, size_
       LRE_CUDA_TRY(c, pass_a(b + 1));
       count_launch(c);
     }
+    const bool tone = tone_scale >= 0.f;
     LRE_CUDA_TRY(c, WS == 64 ? axial_pass_b<64>(w, h, HS, edge(b), edge(b + 1), c->stream, in, out, radius, strength,
-                                                  d_max_g, planes)
+                                                  d_max_g, planes, tone, tone_scale)
                              : axial_pass_b<128>(w, h, HS, edge(b), edge(b + 1), c->stream, in, out, radius, strength,
-                                                   d_max_g, planes));
+                                                   d_max_g, planes, tone, tone_scale));
     count_launch(c);
     LRE_TRY(check_launch(c, "ca_axial_cleanup"));
     const size_t r0 = std::min(h, (size_t)edge(b) * HS), r1 = std::min(h, (size_t)edge(b + 1) * HS);
@@ -767,7 +776,7 @@ lre_status launch_axial_ca_banded(Context* c, const float* in, float* out, size_
 }
 
 lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, size_t h, int radius, float eps,
-                           float strength, const float* d_max_g) {
+                           float strength, const float* d_max_g, float tone_scale) {
   if (radius < 1) radius = 1;
   if (radius > 16) return fail(c, LRE_ERR_INVALID_ARGUMENT, "ca_axial_cleanup: radius > 16 is not supported");
   strength = fminf(fmaxf(strength, 0.f), 1.f);
@@ -790,8 +799,11 @@ lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, si
   const size_t want = (size_t)c->sm_count * 24;
   int HS = c->tune.axial_rows == 128 ? 128 : 64;
   while (HS > 16 && strips_x * ((h + HS - 1) / HS) < want) HS /= 2;
-  LRE_CUDA_TRY(c, WS == 64 ? axial_stream<64>(w, h, HS, c->stream, src, out, radius, eps, strength, d_max_g, planes)
-                           : axial_stream<128>(w, h, HS, c->stream, src, out, radius, eps, strength, d_max_g, planes));
+  const bool tone = tone_scale >= 0.f;
+  LRE_CUDA_TRY(c, WS == 64 ? axial_stream<64>(w, h, HS, c->stream, src, out, radius, eps, strength, d_max_g, planes,
+                                              tone, tone_scale)
+                           : axial_stream<128>(w, h, HS, c->stream, src, out, radius, eps, strength, d_max_g, planes,
+                                               tone, tone_scale));
   count_launch(c, 2);
   return check_launch(c, "ca_axial_cleanup");
 }

@@ -7,12 +7,6 @@
 
 namespace lre {
 
-// ACES filmic curve, core/cpu_accelerator.cpp:3048-3056.
-__device__ __forceinline__ float aces(float x) {
-  const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
-  return (x * (a * x + b)) / (x * (c * x + d) + e);
-}
-
 __global__ void k_tone_mapping_v4(const float4* __restrict__ in, float4* __restrict__ out, size_t n4,
                                   float s) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {

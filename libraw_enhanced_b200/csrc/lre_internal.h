@@ -145,13 +145,17 @@ lre_status launch_pack_cfa(Context* c, const float* raw_rgb, float* dense, size_
                            uint32_t filters, const char* xtrans);
 lre_status launch_channel_max(Context* c, const float* rgb, size_t n_px, int channel, float* d_out,
                               bool clamp0);
+// tone_scale >= 0: the ACES tone map (after_scale tone_scale) that follows
+// the filter is applied to its output in the same pass (bit for bit the
+// separate stage); < 0: plain filter output.
 lre_status launch_axial_ca(Context* c, const float* in, float* out, size_t w, size_t h, int radius,
-                           float eps, float strength, const float* d_max_g);
+                           float eps, float strength, const float* d_max_g, float tone_scale = -1.f);
 // The guided filter in row bands (out of place): after pass B of each band,
 // rows_done(row_lo, row_hi) enqueues what may follow on those rows.
 lre_status launch_axial_ca_banded(Context* c, const float* in, float* out, size_t w, size_t h, int radius, float eps,
                                   float strength, const float* d_max_g, int bands,
-                                  const std::function<lre_status(size_t, size_t)>& rows_done);
+                                  const std::function<lre_status(size_t, size_t)>& rows_done,
+                                  float tone_scale = -1.f);
 // in_max_g (nullable): max(0, max G) of `in`, already reduced on the device
 // by the stage that wrote it (the defringe then skips its own reduction).
 // out_max_g (nullable): receives max(0, max G) of `out`, reduced in the

@@ -178,6 +178,10 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
     return LRE_OK;
   };
   const bool in_bands = tail && banded_tail(p);
+  // In the 51 MP order an ACES tone map right after the axial filter runs
+  // inside the filter's last pass (same bits, one pass over the image less).
+  const bool tone_in_axial = p.stage_order == 1 && p.axial_ca_correction && p.tone_mapping == 1;
+  const float tone_scale = tone_in_axial ? p.tone_after_scale : -1.f;
   auto axial = [&]() -> lre_status {
     if (!p.axial_ca_correction) return LRE_OK;
     float* dmax = cur_max_g;
@@ -189,15 +193,10 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
       float* dst = other;
       LRE_TRY(lre::launch_axial_ca_banded(
           c, cur, dst, w, h, p.axial_ca_radius, p.axial_ca_epsilon, p.axial_ca_strength, dmax, 8,
-          [&](size_t r0, size_t r1) -> lre_status {
-            if (p.tone_mapping == 1)
-              LRE_TRY(lre::launch_tone_mapping(c, dst + r0 * w * 3, dst + r0 * w * 3, (r1 - r0) * w,
-                                               p.tone_after_scale));
-            return (*tail)(dst, r0, r1);
-          }));
+          [&](size_t r0, size_t r1) -> lre_status { return (*tail)(dst, r0, r1); }, tone_scale));
     } else {
       LRE_TRY(lre::launch_axial_ca(c, cur, other, w, h, p.axial_ca_radius, p.axial_ca_epsilon, p.axial_ca_strength,
-                                   dmax));
+                                   dmax, tone_scale));
     }
     std::swap(cur, other);
     cur_max_g = nullptr;
@@ -218,7 +217,7 @@ lre_status run_chain(Context* c, const float* d_mosaic, float* rgb_a, float* rgb
   if (p.stage_order == 1) {
     LRE_TRY(defringe());
     LRE_TRY(axial());
-    if (!in_bands) LRE_TRY(tone());
+    if (!tone_in_axial) LRE_TRY(tone());
   } else {
     LRE_TRY(tone());
     LRE_TRY(lateral());
