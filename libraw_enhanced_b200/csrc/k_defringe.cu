@@ -315,24 +315,11 @@ __device__ __forceinline__ void blur_fast_body(const BlurJob& job, const GaussTa
     const float* in = pick5(job.in, p);
     const int mode = pick5(job.mode, p);
     float* out = pick5(job.out, p);
-    // clamped halo, one row per warp and step, lanes across the row; the
-    // source mode and the edge normaliser (1 / max_edge, as blur_src forms
-    // it) are fixed for the plane
-    {
-      const int warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31, nwarps = (int)blockDim.x >> 5;
-      const float edge_inv = 1.f / smax(sc->max_edge, 1e-6f);
-      for (int r = warp; r < E; r += nwarps) {
-        const int gy = min(max(y0 - KS + r, 0), H - 1);
-        const float* row = in + (size_t)gy * W * (mode == BS_GUIDE_LINEAR ? 3 : 1);
-        for (int q = lane; q < E; q += 32) {
-          const int gx = min(max(x0 - KS + q, 0), W - 1);
-          float v;
-          if (mode == BS_GUIDE_LINEAR) v = smax(row[(size_t)gx * 3 + 1], 0.f);
-          else if (mode == BS_PLANE_EDGE_NORM) v = row[gx] * edge_inv;
-          else v = row[gx];
-          s_in[r * LD + q] = v;
-        }
-      }
+    for (int i = threadIdx.x; i < E * E; i += blockDim.x) {
+      const int r = i / E, q = i % E;
+      const int gy = min(max(y0 - KS + r, 0), H - 1);
+      const int gx = min(max(x0 - KS + q, 0), W - 1);
+      s_in[r * LD + q] = blur_src(in, mode, sc, gx, gy, W);
     }
     __syncthreads();
     // Both passes run two outputs per item and accumulate every output's

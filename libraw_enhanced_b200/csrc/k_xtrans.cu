@@ -800,6 +800,395 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
   }
 }
 
+// --------------------------------------------------------- 3-pass, one plane on chip
+// The interpolation steps (b) to (f) never mix direction planes: each
+// direction's reads and writes stay in its own plane, and passes 1 and 2
+// continue planes 4..7 from copies of planes 0..3 (:2131-2136).  So one CTA
+// carries one plane at a time in shared memory through all of its passes:
+// plane k through pass 0, whose derivatives (g) and RGB then go to the CTA's
+// global scratch, and on in place as plane k + 4 through passes 1 and 2.  The
+// green min/max table stays in shared memory for the whole tile.  The
+// homogeneity steps read the eight derivative planes back from the scratch
+// and keep their byte maps in shared memory, and the final average reads the
+// RGB planes back.  Every step visits each site of its class once and reads
+// no value that the same step writes (xt_sites_ok replays the reference's
+// scans), so each step runs one site per thread; sites stay in fresh-buffer
+// semantics (zeros where a tile computes nothing).
+constexpr int XS_THREADS = 1024;
+constexpr int kXsMaxCtas = 148;
+constexpr int XDN = XTS - 10;  // derivative plane edge
+constexpr size_t kPlaneFloats = (size_t)XTS * XTS * 3;
+constexpr size_t kPlaneBytes = kPlaneFloats * 4;            // 155,952
+constexpr size_t kXsSmemBytes = kPlaneBytes + kGmmBytes;    // 207,936
+constexpr size_t kXsSpillBytes = ((kRgbBytes + kDrvBytes + 255) / 256) * 256;
+static_assert(2 * kHomoBytes <= kXsSmemBytes, "the homogeneity maps reuse the plane's shared memory");
+static_assert(kPlaneBytes % 16 == 0 && kHomoBytes % 16 == 0, "float4 fills");
+
+// (g) YPbPr derivatives of one finished direction plane D (:2346-2405),
+// yuv recomputed at the three taps, and the plane's RGB, into the CTA's
+// scratch.  Reads the plane only.
+__device__ __forceinline__ void xs_plane_out(const float* pl, float* srgb, float* sdrv, int D, int nr, int nc) {
+  constexpr int ts = XTS;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int rows = nr - 10, cols = nc - 10;
+  if (rows > 0 && cols > 0) {
+    const int dv = D & 3;
+    // direction steps 1, ts, ts + 1, ts - 1 of directions 0..3 (and 4..7)
+    int f = dv == 0 ? 1 : (dv == 1 ? ts : (dv == 2 ? ts + 1 : ts - 1));
+    f = f == 1 ? 1 : f - 8;
+    // yuv buffer offset f (width ts - 8) -> tile offset
+    const int fr = (f == 1) ? 0 : 1, fc = (f == 1) ? 1 : (f - (XTS - 8));
+    const int step = (fr * ts + fc) * 3;
+    float* out = sdrv + (size_t)D * XDN * XDN;
+    const XDiv fd(cols);
+    for (int i = tid; i < rows * cols; i += nth) {
+      const int q = fd.div(i), row = 5 + q, col = 5 + i - q * cols;
+      const float* p = pl + (row * ts + col) * 3;
+      auto yuv = [](const float* s, float& y, float& u, float& v) {
+        y = 0.2627f * s[0] + 0.6780f * s[1] + 0.0593f * s[2];
+        u = (s[2] - y) * 0.56433f;
+        v = (s[0] - y) * 0.67815f;
+      };
+      float y0, u0, v0, yp, up, vp, ym, um, vm;
+      yuv(p, y0, u0, v0);
+      yuv(p + step, yp, up, vp);
+      yuv(p - step, ym, um, vm);
+      out[(row - 5) * XDN + (col - 5)] = SQRf(2 * y0 - yp - ym) + SQRf(2 * u0 - up - um) + SQRf(2 * v0 - vp - vm);
+    }
+  }
+  const float4* s4 = reinterpret_cast<const float4*>(pl);
+  float4* d4 = reinterpret_cast<float4*>(srgb + (size_t)D * kPlaneFloats);
+  for (int i = tid; i < (int)(kPlaneBytes / 16); i += nth) d4[i] = s4[i];
+}
+
+__global__ void __launch_bounds__(XS_THREADS, 1) k_xtrans_3pass_planes(XtArgs Ain) {
+  constexpr int ts = XTS;
+  extern __shared__ __align__(16) unsigned char xs_smem[];
+  float* pl = reinterpret_cast<float*>(xs_smem);                   // [XTS][XTS][3]
+  float2* gmm = reinterpret_cast<float2*>(xs_smem + kPlaneBytes);  // [XTS][XTS/2] (min, max)
+  const int tid = threadIdx.x, nth = blockDim.x;
+  __shared__ XtArgs sA;
+  {
+    constexpr int NW = (int)(sizeof(XtArgs) / 4);
+    const int* from = reinterpret_cast<const int*>(&Ain);
+    int* to = reinterpret_cast<int*>(&sA);
+#pragma unroll
+    for (int k = 0; k < NW; k++)
+      if (k % XS_THREADS == tid) to[k] = from[k];
+  }
+  __syncthreads();
+  const XtArgs& A = sA;
+  const XtParams& P = A.P;
+  float* srgb = reinterpret_cast<float*>(A.scratch + (size_t)blockIdx.x * kXsSpillBytes);  // [NDIR][XTS][XTS][3]
+  float* sdrv = srgb + NDIR * kPlaneFloats;                                                // [NDIR][XDN][XDN]
+  __shared__ int s_tile;
+  const int W = A.W, H = A.H;
+
+  for (;;) {
+    if (tid == 0) s_tile = atomicAdd(A.tile_counter, 1);
+    __syncthreads();
+    const int tile = s_tile;
+    __syncthreads();
+    if (tile >= A.n_top * A.n_left) break;
+    const int top = 3 + (tile / A.n_left) * (ts - 16);
+    const int left = 3 + (tile % A.n_left) * (ts - 16);
+    const int mrow_g = min(top + ts, H - 3);  // global row bound of the computations
+    const int mcol_g = min(left + ts, W - 3);
+    const int nr = mrow_g - top, nc = mcol_g - left;
+    const XDiv fd_nc(nc);
+
+    // (a) green min / max (:1968-2053).  The scan stores a site's hexagon
+    // min/max at its half-column slot; on rows with adjacent non-green pairs
+    // it stores the first site's values at both sites' slots and computes
+    // none for the second.
+    for (int i = tid; i < nr * nc; i += nth) {
+      const int lr = fd_nc.div(i), lc = i - lr * nc;
+      const int row = top + lr, col = left + lc;
+      if (xisgreen(P, row, col)) continue;
+      if (lc > 0 && !xisgreen(P, row, col - 1)) continue;  // second of a pair
+      const short* hex = P.allhex0[row % 3][col % 3];
+      float minval = FLT_MAX, maxval = 0.f;
+      for (int c = 0; c < 6; c++) {
+        const float val = xraw_hex(A, row, col, hex[c]);
+        minval = minval < val ? minval : val;
+        maxval = maxval > val ? maxval : val;
+      }
+      const float2 v = make_float2(minval, maxval);
+      float2* g = gmm + (size_t)lr * (ts / 2);
+      g[lc >> 1] = v;
+      if (lc + 1 < nc && !xisgreen(P, row, col + 1)) g[(lc + 1) >> 1] = v;
+    }
+
+    for (int k = 0; k < 4; k++) {
+      // fresh plane k: zeros, the native samples (:2055-2061; planes 1..3 are
+      // copies of plane 0 without its last float, :2067-2069) and (b) the
+      // green of direction k at every non-green site (:2071-2127)
+      {
+        float4* z = reinterpret_cast<float4*>(pl);
+        for (int i = tid; i < (int)(kPlaneBytes / 16); i += nth) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      __syncthreads();
+      for (int i = tid; i < nr * nc; i += nth) {
+        const int lr = fd_nc.div(i), lc = i - lr * nc;
+        const int row = top + lr, col = left + lc;
+        float* rix = pl + (lr * ts + lc) * 3;
+        const int fcv = xfc(P, row, col);
+        if (k == 0 || (lr * ts + lc) * 3 + fcv != (int)kPlaneFloats - 1) rix[fcv] = xraw(A, row, col);
+        if (fcv == 1) continue;
+        const short* hex = P.allhex0[row % 3][col % 3];
+        const int cdir = k ^ (P.right_shift[row % 3] == 1 ? 0 : 1);
+        float color;
+        if (cdir == 0) {
+          color = 0.6796875f * (xraw_hex(A, row, col, hex[1]) + xraw_hex(A, row, col, hex[0])) -
+                  0.1796875f * (xraw_hex(A, row, col, 2 * hex[1]) + xraw_hex(A, row, col, 2 * hex[0]));
+        } else if (cdir == 1) {
+          color = 0.87109375f * xraw_hex(A, row, col, hex[3]) + xraw_hex(A, row, col, hex[2]) * 0.12890625f +
+                  0.359375f * (xraw_hex(A, row, col, 0) - xraw_hex(A, row, col, -hex[2]));
+        } else {
+          const int h4 = hex[cdir + 2];
+          color = 0.640625f * xraw_hex(A, row, col, h4) + 0.359375f * xraw_hex(A, row, col, -2 * h4) +
+                  0.12890625f * (2.f * xraw_hex(A, row, col, 0) - xraw_hex(A, row, col, 3 * h4) -
+                                 xraw_hex(A, row, col, -3 * h4));
+        }
+        const float2 mmv = gmm[(size_t)lr * (ts / 2) + (lc >> 1)];
+        rix[1] = LIMf(color, mmv.x, mmv.y);
+      }
+      __syncthreads();
+
+      for (int pass = 0; pass < 3; pass++) {
+        if (pass == 1) {
+          // plane k is final: (g) its derivatives and its RGB go to the
+          // scratch, and the plane continues in place as plane k + 4
+          xs_plane_out(pl, srgb, sdrv, k, nr, nc);
+          __syncthreads();
+        }
+        // (c) recalculate green from closer pixels (:2138-2183): direction
+        // d = 3..5 updates plane (d - 2) ^ flip, reading green sites only
+        if (pass) {
+          const int rows = nr - 4, ncols = nc - 4;
+          if (rows > 0 && ncols > 0) {
+            const XDiv fd(ncols);
+            for (int i = tid; i < rows * ncols; i += nth) {
+              const int q = fd.div(i), lr = 2 + q, lc = 2 + i - q * ncols;
+              const int row = top + lr, col = left + lc;
+              if (xisgreen(P, row, col)) continue;
+              const int dd = k ^ (P.right_shift[row % 3] == 1 ? 0 : 1);
+              if (dd == 0) continue;
+              const int f = xfc(P, row, col);
+              const int hx = P.allhex1[row % 3][col % 3][dd + 2];
+              float* rix = pl + (lr * ts + lc) * 3;
+              const int o1 = hx * 3, o2 = -2 * hx * 3;
+              const float val = 0.33333333f * (rix[o2 + 1] + 2 * (rix[o1 + 1] - rix[o1 + f]) - rix[o2 + f]) + rix[f];
+              const float2 mmv = gmm[(size_t)lr * (ts / 2) + (lc >> 1)];
+              rix[1] = LIMf(val, mmv.x, mmv.y);
+            }
+          }
+          __syncthreads();
+        }
+        // (d) R/B at solitary green pixels (:2185-2222): plane k carries
+        // direction k (k < 2), directions 2 and 3 (k = 2) or 4 and 5 (k = 3),
+        // the second of a pair falling back to the first where its
+        // difference is larger
+        {
+          const int sgstartcol = (left - P.sgcol + 4) / 3 * 3 + P.sgcol;
+          const int row0 = (top - P.sgrow + 4) / 3 * 3 + P.sgrow;
+          const int nrow = row0 < mrow_g - 2 ? (mrow_g - 2 - row0 + 2) / 3 : 0;
+          const int ncol = sgstartcol < mcol_g - 2 ? (mcol_g - 2 - sgstartcol + 2) / 3 : 0;
+          const int d_lo = k < 2 ? k : 2 * k - 2, nd = k < 2 ? 1 : 2;
+          for (int item = tid; item < nrow * ncol; item += nth) {
+            const int row = row0 + 3 * (item / ncol), kk = item % ncol;
+            const int col = sgstartcol + 3 * kk;
+            float* rix = pl + ((row - top) * ts + (col - left)) * 3;
+            const int h0 = xfc(P, row, sgstartcol + 1) ^ ((kk & 1) << 1);
+            float cr0 = 0.f, cb0 = 0.f, df0 = 0.f, r = 0.f, b = 0.f, df1 = 0.f;
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+              if (j >= nd) break;
+              const int d = d_lo + j;
+              const int i = (d & 1) ? ts : 1;
+              int h = h0 ^ ((d & 1) << 1);
+              float df = 0.f, cr = 0.f, cb = 0.f;
+#pragma unroll
+              for (int c = 0; c < 2; c++, h ^= 2) {
+                const int op = i * (1 << c) * 3, om = -i * (1 << c) * 3;
+                const float g = rix[1] + rix[1] - rix[op + 1] - rix[om + 1];
+                const float v = g + rix[op + h] + rix[om + h];
+                if (h == 0) cr = v;
+                else cb = v;
+                if (d > 1) df += SQRf(rix[op + 1] - rix[om + 1] - rix[op + h] + rix[om + h]) + SQRf(g);
+              }
+              if (j == 0) {
+                cr0 = cr;
+                cb0 = cb;
+                df0 = df;
+              }
+              r = cr;
+              b = cb;
+              df1 = df;
+            }
+            if (nd == 2 && df0 < df1) {
+              r = cr0;
+              b = cb0;
+            }
+            rix[0] = 0.5f * r;
+            rix[2] = 0.5f * b;
+          }
+        }
+        __syncthreads();
+        // (e) red for blue pixels and vice versa (:2224-2264): every non-green
+        // site writes its other colour f = 2 - own
+        {
+          const int rows = nr - 6, ncols = nc - 6;
+          if (rows > 0 && ncols > 0) {
+            const XDiv fd(ncols);
+            for (int i = tid; i < rows * ncols; i += nth) {
+              const int q = fd.div(i), lr = 3 + q, lc = 3 + i - q * ncols;
+              const int row = top + lr, col = left + lc;
+              if (xisgreen(P, row, col)) continue;
+              const int c = ((row - P.sgrow) % 3) ? ts : 1;
+              const int h = 3 * (c ^ ts ^ 1);
+              const int f = 2 - xfc(P, row, col);
+              float* rix = pl + (lr * ts + lc) * 3;
+              const float g0 = rix[1];
+              const bool use_c = k > 1 || ((k ^ c) & 1) ||
+                                 ((fabsf(g0 - rix[c * 3 + 1]) + fabsf(g0 - rix[-c * 3 + 1])) <
+                                  2.f * (fabsf(g0 - rix[h * 3 + 1]) + fabsf(g0 - rix[-h * 3 + 1])));
+              const int s = use_c ? c : h;
+              rix[f] = g0 + 0.5f * (rix[s * 3 + f] + rix[-s * 3 + f] - rix[s * 3 + 1] - rix[-s * 3 + 1]);
+            }
+          }
+        }
+        __syncthreads();
+        // (f) R and B for 2x2 green blocks (:2266-2310): greens off the
+        // solitary-green row and column classes, hexagon allhex1
+        {
+          int topstart = top + 2;
+          for (; topstart < mrow_g - 2; topstart++)
+            if ((topstart - P.sgrow) % 3) break;
+          int leftstart = left + 2;
+          for (; leftstart < mcol_g - 2; leftstart++)
+            if ((leftstart - P.sgcol) % 3) break;
+          const int ncols = mcol_g - 2 - leftstart, nrows = mrow_g - 2 - topstart;
+          if (nrows > 0 && ncols > 0) {
+            const XDiv fd(ncols);
+            for (int i = tid; i < nrows * ncols; i += nth) {
+              const int q = fd.div(i), row = topstart + q, col = leftstart + i - q * ncols;
+              if (!((row - P.sgrow) % 3) || !((col - P.sgcol) % 3)) continue;
+              float* rix = pl + ((row - top) * ts + (col - left)) * 3;
+              const short* hex = P.allhex1[row % 3][col % 3];
+              const int o0 = hex[2 * k] * 3, o1 = hex[2 * k + 1] * 3;
+              const float v1 = rix[1], a1 = rix[o0 + 1], b1 = rix[o1 + 1];
+              const float a0 = rix[o0], b0 = rix[o1], a2 = rix[o0 + 2], b2 = rix[o1 + 2];
+              if (hex[2 * k] + hex[2 * k + 1]) {
+                const float g = 3 * v1 - 2 * a1 - b1;
+                rix[0] = (g + 2 * a0 + b0) * 0.33333333f;
+                rix[2] = (g + 2 * a2 + b2) * 0.33333333f;
+              } else {
+                const float g = 2 * v1 - a1 - b1;
+                rix[0] = (g + a0 + b0) * 0.5f;
+                rix[2] = (g + a2 + b2) * 0.5f;
+              }
+            }
+          }
+        }
+        __syncthreads();
+      }
+      xs_plane_out(pl, srgb, sdrv, k + 4, nr, nc);
+      __syncthreads();
+    }
+
+    // (h) homogeneity maps (:2407-2496) from the derivative planes
+    unsigned char* homo = xs_smem;             // [NDIR][XTS][XTS]
+    unsigned char* hs5 = xs_smem + kHomoBytes;  // [NDIR][XTS][XTS]
+    {
+      float4* z = reinterpret_cast<float4*>(homo);
+      for (int i = tid; i < (int)(kHomoBytes / 16); i += nth) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    {
+      const int rows = nr - 12, cols = nc - 12;
+      if (rows > 0 && cols > 0) {
+        const XDiv fd(cols);
+        for (int i = tid; i < rows * cols; i += nth) {
+          const int q = fd.div(i), row = 6 + q, col = 6 + i - q * cols;
+          const float* dp = sdrv + (row - 5) * XDN + (col - 5);
+          float tr = dp[0] < dp[XDN * XDN] ? dp[0] : dp[XDN * XDN];
+          for (int d = 2; d < NDIR; d++) tr = (dp[d * XDN * XDN] < tr ? dp[d * XDN * XDN] : tr);
+          tr *= 8;
+          unsigned char temp[NDIR];
+#pragma unroll
+          for (int d = 0; d < NDIR; d++) {
+            temp[d] = 0;
+            for (int v = -1; v <= 1; v++)
+              for (int h = -1; h <= 1; h++) temp[d] += (dp[d * XDN * XDN + v * XDN + h] <= tr ? 1 : 0);
+          }
+#pragma unroll
+          for (int d = 0; d < NDIR; d++) homo[(d * ts + row) * ts + col] = temp[d];
+        }
+      }
+    }
+    __syncthreads();
+    int mrow = nr, mcol = nc;
+    if (H - top < ts + 4) mrow = H - top + 2;
+    if (W - left < ts + 4) mcol = W - left + 2;
+    // (j) 5x5 homogeneity sums (:2504-2612), separably: row 5-sums first
+    const int r0 = min(top, 8), c0 = min(left, 8);
+    {
+      const int rows = mrow - 8 - r0 + 4, cols = mcol - 8 - c0;
+      if (rows > 0 && cols > 0) {
+        const XDiv fdr(rows * cols), fdc(cols);
+        for (int i = tid; i < NDIR * rows * cols; i += nth) {
+          const int d = fdr.div(i), rem = i - d * (rows * cols);
+          const int q = fdc.div(rem), row = r0 - 2 + q, col = c0 + rem - q * cols;
+          const unsigned char* hp = homo + (d * ts + row) * ts + col;
+          hs5[(d * ts + row) * ts + col] = (unsigned char)(hp[-2] + hp[-1] + hp[0] + hp[1] + hp[2]);
+        }
+      }
+    }
+    __syncthreads();
+    // (j) column sums and their max, then (l) the average of the most
+    // homogeneous directions (:2614-2650), one output pixel per thread
+    {
+      const int rows = mrow - 8 - r0, cols = mcol - 8 - c0;
+      if (rows > 0 && cols > 0) {
+        const XDiv fd(cols);
+        for (int i = tid; i < rows * cols; i += nth) {
+          const int q = fd.div(i), row = r0 + q, col = c0 + i - q * cols;
+          unsigned char hm[NDIR];
+          unsigned char maxval = 0;
+#pragma unroll
+          for (int d = 0; d < NDIR; d++) {
+            int s = 0;
+            for (int v = -2; v <= 2; v++) s += hs5[(d * ts + row + v) * ts + col];
+            hm[d] = (unsigned char)s;
+            if (d == 0 || maxval < hm[d]) maxval = hm[d];
+          }
+          maxval -= maxval >> 3;
+#pragma unroll
+          for (int d = 4; d < NDIR; d++) {
+            if (hm[d - 4] < hm[d]) hm[d - 4] = 0;
+            else if (hm[d - 4] > hm[d]) hm[d] = 0;
+          }
+          float avg[4] = {0.f, 0.f, 0.f, 0.f};
+          const float* px = srgb + (size_t)(row * ts + col) * 3;
+#pragma unroll
+          for (int d = 0; d < NDIR; d++)
+            if (hm[d] >= maxval) {
+              const float* p = px + d * kPlaneFloats;
+              for (int c = 0; c < 3; c++) avg[c] += p[c];
+              avg[3] += 1.f;
+            }
+          float* o = A.rgb_out + ((size_t)(row + top) * W + (col + left)) * 3;
+          o[0] = fmaxf(0.f, avg[0] / avg[3]);
+          o[1] = fmaxf(0.f, avg[1] / avg[3]);
+          o[2] = fmaxf(0.f, avg[2] / avg[3]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // allhex / solitary green / RightShift tables (:1887-1940), host side.
 XtParams make_xt_params(const char* xtrans, int width) {
   XtParams P;
@@ -840,10 +1229,10 @@ XtParams make_xt_params(const char* xtrans, int width) {
   return P;
 }
 
-// Whether the reference's row scans of phases (b), (e) and (f) reduce to
-// "every site of the class" for this pattern (true for the X-Trans layouts
-// and their shifts), so the site-parallel kernel variant applies.  Checked
-// by replaying the scans over every tile-origin residue.
+// Whether the reference's row scans of phases (a), (b), (c), (e) and (f)
+// reduce to "every site of the class" for this pattern (true for the X-Trans
+// layouts and their shifts), so the site-parallel kernels apply.  Checked by
+// replaying the scans over every tile-origin residue.
 bool xt_sites_ok(const XtParams& P) {
   auto isg = [&](int r, int c) { return P.xt[((r % 3) + 3) % 3][((c % 3) + 3) % 3] & 1; };
   auto fc = [&](int r, int c) { return (int)P.xt[(r + 6) % 6][(c + 6) % 6]; };
@@ -876,6 +1265,66 @@ bool xt_sites_ok(const XtParams& P) {
             if (isg(row, col) || f != 2 - fc(row, col)) return false;
         }
       }
+      // (a): the slot a non-green site reads holds the min/max of the site
+      // itself, or of its left neighbour when that is a non-green site of
+      // the tile (the second site of a pair); replayed in the scan's write
+      // order
+      for (int row = top; row < mrow; row++) {
+        int src[40];
+        for (int j = 0; j < 40; j++) src[j] = -1;
+        int ls = left;
+        while (ls < mcol && isg(row, ls)) ls++;
+        const int co = P.right_shift[row % 3] == 1 ? 3 : 1 + (fc(row, ls + 1) & 1);
+        if (co == 3) {
+          for (int col = ls; col < mcol; col += 3) src[(col - left) >> 1] = col;
+        } else {
+          int col = ls;
+          if (co == 2) {
+            src[(col - left) >> 1] = col;
+            col += 2;
+          }
+          for (; col < mcol - 1; col += 3) src[(col - left) >> 1] = src[(col + 1 - left) >> 1] = col;
+          if (col < mcol) src[(col - left) >> 1] = col;
+        }
+        for (int col = left; col < mcol; col++) {
+          if (isg(row, col)) continue;
+          const int expect_src = (col > left && !isg(row, col - 1)) ? col - 1 : col;
+          if (src[(col - left) >> 1] != expect_src) return false;
+        }
+      }
+      // (c): visits every non-green site from left + 2 with f = own colour
+      // and hexagon allhex1[row % 3][col % 3], and reads green sites only
+      // (which the step does not write)
+      for (int row = top + 2; row < mrow - 2; row++) {
+        int ls = left + 2;
+        while (ls < mcol - 2 && isg(row, ls)) ls++;
+        int co = P.right_shift[row % 3] == 1 ? 3 : 1 + (fc(row, ls + 1) & 1);
+        int f = fc(row, ls);
+        int expect = ls;
+        for (int col = ls; col < mcol - 2;) {
+          while (expect < mcol - 2 && isg(row, expect)) expect++;
+          if (col != expect || f != fc(row, col)) return false;
+          expect++;
+          for (int d = 3; d < 6; d++)
+            for (int m = -2; m <= 1; m += 3) {
+              const int x = m * P.allhex1[row % 3][col % 3][d];
+              int v = -7, h = 0;
+              for (int vv = -6; vv <= 6; vv++)
+                if (x - vv * XTS >= -6 && x - vv * XTS <= 6) v = vv, h = x - vv * XTS;
+              if (v < -6 || !isg(row + v, col + h)) return false;
+            }
+          if (co == 3) {
+            col += 3;
+            f ^= 2;
+          } else {
+            col += co;
+            co ^= 3;
+            f ^= (co & 2);
+          }
+        }
+        while (expect < mcol - 2 && isg(row, expect)) expect++;
+        if (expect < mcol - 2) return false;
+      }
       // (f): visited columns are those off the solitary-green column class
       int ts_ = top;
       while (ts_ < mrow && !((ts_ - P.sgrow + 6) % 3)) ts_++;
@@ -897,7 +1346,7 @@ bool xt_sites_ok(const XtParams& P) {
 size_t ws_bytes_xtrans(size_t w, size_t h, int passes) {
   (void)w;
   (void)h;
-  return passes == 1 ? 0 : (size_t)kXtMaxCtas * kXtSlabBytes + 4096;
+  return passes == 1 ? 0 : std::max((size_t)kXtMaxCtas * kXtSlabBytes, (size_t)kXsMaxCtas * kXsSpillBytes) + 4096;
 }
 
 lre_status launch_xtrans(Context* c, const float* raw, int cstride, float* rgb, size_t w, size_t h, const char* xtrans,
@@ -929,18 +1378,23 @@ lre_status launch_xtrans(Context* c, const float* raw, int cstride, float* rgb, 
   A.n_left = n_left;
   const int tiles = n_top * n_left;
   if (tiles > 0) {
-    // two 512-thread CTAs (two tiles) per SM: with fewer slabs in flight more
-    // of them stay in L2 than with eight 128-thread CTAs, and the site
-    // phases have more threads per tile (26 MP: 11.3 against 12.8 ms)
-    int nblk = std::min(std::min(tiles, c->sm_count * kXtCtasPerSm), kXtMaxCtas);
-    A.scratch = reinterpret_cast<unsigned char*>(c->ws.take((size_t)nblk * kXtSlabBytes));
+    // Patterns whose scans the replay confirms run the plane-resident kernel:
+    // one 1024-thread CTA per SM.  Others run the row-scan kernel, two
+    // 512-thread CTAs per SM, each with its whole tile in a global slab.
+    const bool sites = xt_sites_ok(A.P);
+    const int nblk = sites ? std::min(std::min(tiles, c->sm_count), kXsMaxCtas)
+                           : std::min(std::min(tiles, c->sm_count * kXtCtasPerSm), kXtMaxCtas);
+    A.scratch = reinterpret_cast<unsigned char*>(c->ws.take((size_t)nblk * (sites ? kXsSpillBytes : kXtSlabBytes)));
     A.tile_counter = reinterpret_cast<int*>(c->ws.take(256));
     if (!A.scratch || !A.tile_counter) return fail(c, LRE_ERR_OUT_OF_MEMORY, "demosaic_xtrans_3pass: workspace too small");
     LRE_CUDA_TRY(c, cudaMemsetAsync(A.tile_counter, 0, sizeof(int), c->stream));
-    if (xt_sites_ok(A.P))
-      k_xtrans_3pass<true><<<nblk, XT_THREADS, 0, c->stream>>>(A);
-    else
+    if (sites) {
+      LRE_CUDA_TRY(c, cudaFuncSetAttribute(k_xtrans_3pass_planes, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kXsSmemBytes));
+      k_xtrans_3pass_planes<<<nblk, XS_THREADS, kXsSmemBytes, c->stream>>>(A);
+    } else {
       k_xtrans_3pass<false><<<nblk, XT_THREADS, 0, c->stream>>>(A);
+    }
     count_launch(c);
   }
   k_xtrans_border<<<grid_for(16 * (w + h), 256, c->sm_count * 2), 256, 0, c->stream>>>(A, 8);
