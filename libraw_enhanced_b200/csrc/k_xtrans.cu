@@ -9,13 +9,15 @@
 // 3-pass device design: the reference's 114 x 114 tiles (step 98, origin 3)
 // are kept -- its homogeneity maps read outside the rows a tile computes at
 // the first/last tile rows and columns, so the tiling is part of the result.
-// One CTA runs one tile; the row scans whose column walk is data-pattern
-// driven (green min/max, green interpolation, green recalculation, R/B
-// fills) run one row per thread in the reference's column order; the
-// derivative, homogeneity and averaging steps run one pixel per thread.
-// Tile planes (8 directions x 114^2 RGB, derivatives, homogeneity maps) live
-// in a per-CTA global scratch slab; positions a tile reads without computing
-// read zeros (a freshly allocated reference buffer).
+// One CTA runs one tile at a time; positions a tile reads without computing
+// read zeros (a freshly allocated reference buffer).  Two kernels:
+// * k_xtrans_3pass_planes, for every pattern whose row scans a host replay
+//   reduces to "every site of the class" (the X-Trans layouts and their
+//   shifts): one direction plane at a time in shared memory, every step one
+//   site per thread;
+// * k_xtrans_3pass, for any other pattern: the reference's row scans, one
+//   row per thread in its column order, with the whole tile (8 directions x
+//   114^2 RGB, derivatives, homogeneity maps) in a per-CTA global slab.
 #include <cfloat>
 #include <cstring>
 
@@ -229,7 +231,6 @@ __global__ void k_xtrans_1pass(XtArgs A) {
 }
 
 // --------------------------------------------------------- 3-pass
-template <bool SITES>
 __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArgs Ain) {
   const int ts = XTS;
   const int tid = threadIdx.x, nth = blockDim.x;
@@ -347,19 +348,14 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
       }
     }
     __syncthreads();
-    // (b) green in 4 directions (:2071-2127).  The reference scans each row
-    // from its first non-green site; for the X-Trans layouts the scan visits
-    // every non-green site, with hexagon allhex0[row % 3][col % 3] and
-    // directions swapped pairwise on rows with one green per period, and
-    // sites only read the mosaic, so they are computed independently.
-    if (SITES) {
-      const int ncols = mcol_g - left;
-      const XDiv fdb(ncols);
-      for (int i = tid; i < (mrow_g - top) * ncols; i += nth) {
-        const int q_ = fdb.div(i), row = top + q_, col = left + i - q_ * ncols;
-        if (xisgreen(P, row, col)) continue;
-        const short* hex = P.allhex0[row % 3][col % 3];
-        float color[4];
+    // (b) green in 4 directions (:2071-2127), one row per thread
+    for (int row = top + tid; row < mrow_g; row += nth) {
+      int leftstart = left;
+      for (; leftstart < mcol_g; leftstart++)
+        if (!xisgreen(P, row, leftstart)) break;
+      int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1 + (xfc(P, row, leftstart + 1) & 1));
+      const float2* g = S.gmm + (size_t)(row - top) * (ts / 2);
+      auto colors = [&](int col, const short* hex, float* color) {
         color[0] = 0.6796875f * (xraw_hex(A, row, col, hex[1]) + xraw_hex(A, row, col, hex[0])) -
                    0.1796875f * (xraw_hex(A, row, col, 2 * hex[1]) + xraw_hex(A, row, col, 2 * hex[0]));
         color[1] = 0.87109375f * xraw_hex(A, row, col, hex[3]) + xraw_hex(A, row, col, hex[2]) * 0.12890625f +
@@ -368,50 +364,27 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
           color[2 + c] = 0.640625f * xraw_hex(A, row, col, hex[4 + c]) + 0.359375f * xraw_hex(A, row, col, -2 * hex[4 + c]) +
                          0.12890625f * (2.f * xraw_hex(A, row, col, 0) - xraw_hex(A, row, col, 3 * hex[4 + c]) -
                                         xraw_hex(A, row, col, -3 * hex[4 + c]));
-        const float2 mmv = S.gmm[(size_t)(row - top) * (ts / 2) + ((col - left) >> 1)];
-        const int swap = P.right_shift[row % 3] == 1 ? 0 : 1;
-        for (int c = 0; c < 4; c++) RGB(c ^ swap, row - top, col - left)[1] = LIMf(color[c], mmv.x, mmv.y);
-      }
-      __syncthreads();
-    } else {
-      // (b) green in 4 directions (:2071-2127), one row per thread
-      for (int row = top + tid; row < mrow_g; row += nth) {
-        int leftstart = left;
-        for (; leftstart < mcol_g; leftstart++)
-          if (!xisgreen(P, row, leftstart)) break;
-        int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1 + (xfc(P, row, leftstart + 1) & 1));
-        const float2* g = S.gmm + (size_t)(row - top) * (ts / 2);
-        auto colors = [&](int col, const short* hex, float* color) {
-          color[0] = 0.6796875f * (xraw_hex(A, row, col, hex[1]) + xraw_hex(A, row, col, hex[0])) -
-                     0.1796875f * (xraw_hex(A, row, col, 2 * hex[1]) + xraw_hex(A, row, col, 2 * hex[0]));
-          color[1] = 0.87109375f * xraw_hex(A, row, col, hex[3]) + xraw_hex(A, row, col, hex[2]) * 0.12890625f +
-                     0.359375f * (xraw_hex(A, row, col, 0) - xraw_hex(A, row, col, -hex[2]));
-          for (int c = 0; c < 2; c++)
-            color[2 + c] = 0.640625f * xraw_hex(A, row, col, hex[4 + c]) + 0.359375f * xraw_hex(A, row, col, -2 * hex[4 + c]) +
-                           0.12890625f * (2.f * xraw_hex(A, row, col, 0) - xraw_hex(A, row, col, 3 * hex[4 + c]) -
-                                          xraw_hex(A, row, col, -3 * hex[4 + c]));
-        };
-        if (coloffset == 3) {
-          const short* hex = P.allhex0[row % 3][leftstart % 3];
-          for (int col = leftstart; col < mcol_g; col += coloffset) {
-            float color[4];
-            colors(col, hex, color);
-            const float2 mmv = g[(col - left) >> 1];
-            for (int c = 0; c < 4; c++) RGB(c, row - top, col - left)[1] = LIMf(color[c], mmv.x, mmv.y);
-          }
-        } else {
-          const short* hexmod[2] = {P.allhex0[row % 3][leftstart % 3], P.allhex0[row % 3][(leftstart + coloffset) % 3]};
-          for (int col = leftstart, hexindex = 0; col < mcol_g; col += coloffset, coloffset ^= 3, hexindex ^= 1) {
-            const short* hex = hexmod[hexindex];
-            float color[4];
-            colors(col, hex, color);
-            const float2 mmv = g[(col - left) >> 1];
-            for (int c = 0; c < 4; c++) RGB(c ^ 1, row - top, col - left)[1] = LIMf(color[c], mmv.x, mmv.y);
-          }
+      };
+      if (coloffset == 3) {
+        const short* hex = P.allhex0[row % 3][leftstart % 3];
+        for (int col = leftstart; col < mcol_g; col += coloffset) {
+          float color[4];
+          colors(col, hex, color);
+          const float2 mmv = g[(col - left) >> 1];
+          for (int c = 0; c < 4; c++) RGB(c, row - top, col - left)[1] = LIMf(color[c], mmv.x, mmv.y);
+        }
+      } else {
+        const short* hexmod[2] = {P.allhex0[row % 3][leftstart % 3], P.allhex0[row % 3][(leftstart + coloffset) % 3]};
+        for (int col = leftstart, hexindex = 0; col < mcol_g; col += coloffset, coloffset ^= 3, hexindex ^= 1) {
+          const short* hex = hexmod[hexindex];
+          float color[4];
+          colors(col, hex, color);
+          const float2 mmv = g[(col - left) >> 1];
+          for (int c = 0; c < 4; c++) RGB(c ^ 1, row - top, col - left)[1] = LIMf(color[c], mmv.x, mmv.y);
         }
       }
-      __syncthreads();
     }
+    __syncthreads();
 
     for (int pass = 0; pass < 3; pass++) {
       if (pass == 1) {
@@ -505,157 +478,67 @@ __global__ void __launch_bounds__(XT_THREADS, kXtCtasPerSm) k_xtrans_3pass(XtArg
         }
       }
       __syncthreads();
-      // (e) red for blue pixels and vice versa (:2224-2264): every non-green
-      // site from the scan start, writing its other colour f = 2 - own; it
-      // reads greens and its neighbours' native colours only.
-      if (SITES) {
-        const int r0e = top + 3, c0e = left + 3;
-        const int ncols = mcol_g - 3 - c0e;
-        const XDiv fde(ncols > 0 ? ncols : 1);
-        for (int i = tid; i < (mrow_g - 3 - r0e) * (ncols > 0 ? ncols : 0); i += nth) {
-          const int q_ = fde.div(i), row = r0e + q_, col = c0e + i - q_ * ncols;
-          if (xisgreen(P, row, col)) continue;
-          const int c = ((row - P.sgrow) % 3) ? ts : 1;
-          const int h = 3 * (c ^ ts ^ 1);
-          const int f = 2 - xfc(P, row, col);
-          float* rix0 = RGB(0, row - top, col - left);
-          // every operand of the four directions is loaded before the first
-          // store (the stores go to this site's own colour f in each plane,
-          // which no load reads), so the loads are in flight together; the
-          // h operands are loaded even where the reference does not need
-          // them (they lie inside the tile plane)
-          float g0[4], gc0[4], gc1[4], gh0[4], gh1[4], fc0[4], fc1[4], fh0[4], fh1[4];
-#pragma unroll
-          for (int d = 0; d < 4; d++) {
-            const float* rix = rix0 + (size_t)d * ts * ts * 3;
-            g0[d] = rix[1];
-            gc0[d] = rix[c * 3 + 1];
-            gc1[d] = rix[-c * 3 + 1];
-            gh0[d] = rix[h * 3 + 1];
-            gh1[d] = rix[-h * 3 + 1];
-            fc0[d] = rix[c * 3 + f];
-            fc1[d] = rix[-c * 3 + f];
-            fh0[d] = rix[h * 3 + f];
-            fh1[d] = rix[-h * 3 + f];
+      // (e) red for blue pixels and vice versa (:2224-2264), one row per
+      // thread in the reference's column order
+      for (int row = top + 3 + tid; row < mrow_g - 3; row += nth) {
+        int leftstart = left + 3;
+        for (; leftstart < mcol_g - 1; leftstart++)
+          if (!xisgreen(P, row, leftstart)) break;
+        int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1);
+        const int c = ((row - P.sgrow) % 3) ? ts : 1;
+        const int h = 3 * (c ^ ts ^ 1);
+        auto body = [&](int col, int f) {
+          float* rix = RGB(0, row - top, col - left);
+          for (int d = 0; d < 4; d++, rix += (size_t)ts * ts * 3) {
+            const int i = d > 1 || ((d ^ c) & 1) ||
+                                  ((fabsf(rix[1] - rix[c * 3 + 1]) + fabsf(rix[1] - rix[-c * 3 + 1])) <
+                                   2.f * (fabsf(rix[1] - rix[h * 3 + 1]) + fabsf(rix[1] - rix[-h * 3 + 1])))
+                              ? c
+                              : h;
+            rix[f] = rix[1] + 0.5f * (rix[i * 3 + f] + rix[-i * 3 + f] - rix[i * 3 + 1] - rix[-i * 3 + 1]);
           }
-#pragma unroll
-          for (int d = 0; d < 4; d++) {
-            const bool use_c = d > 1 || ((d ^ c) & 1) ||
-                               ((fabsf(g0[d] - gc0[d]) + fabsf(g0[d] - gc1[d])) <
-                                2.f * (fabsf(g0[d] - gh0[d]) + fabsf(g0[d] - gh1[d])));
-            const float a0 = use_c ? fc0[d] : fh0[d], a1 = use_c ? fc1[d] : fh1[d];
-            const float b0 = use_c ? gc0[d] : gh0[d], b1 = use_c ? gc1[d] : gh1[d];
-            rix0[(size_t)d * ts * ts * 3 + f] = g0[d] + 0.5f * (a0 + a1 - b0 - b1);
-          }
+        };
+        if (coloffset == 3) {
+          int f = 2 - xfc(P, row, leftstart);
+          for (int col = leftstart; col < mcol_g - 3; col += coloffset, f ^= 2) body(col, f);
+        } else {
+          coloffset = xfc(P, row, leftstart + 1) == 1 ? 2 : 1;
+          int f = 2 - xfc(P, row, leftstart);
+          for (int col = leftstart; col < mcol_g - 3; col += coloffset, coloffset ^= 3, f = f ^ (coloffset & 2)) body(col, f);
         }
-        __syncthreads();
-      } else {
-        for (int row = top + 3 + tid; row < mrow_g - 3; row += nth) {
-          int leftstart = left + 3;
-          for (; leftstart < mcol_g - 1; leftstart++)
-            if (!xisgreen(P, row, leftstart)) break;
-          int coloffset = (P.right_shift[row % 3] == 1 ? 3 : 1);
-          const int c = ((row - P.sgrow) % 3) ? ts : 1;
-          const int h = 3 * (c ^ ts ^ 1);
-          auto body = [&](int col, int f) {
-            float* rix = RGB(0, row - top, col - left);
-            for (int d = 0; d < 4; d++, rix += (size_t)ts * ts * 3) {
-              const int i = d > 1 || ((d ^ c) & 1) ||
-                                    ((fabsf(rix[1] - rix[c * 3 + 1]) + fabsf(rix[1] - rix[-c * 3 + 1])) <
-                                     2.f * (fabsf(rix[1] - rix[h * 3 + 1]) + fabsf(rix[1] - rix[-h * 3 + 1])))
-                                ? c
-                                : h;
-              rix[f] = rix[1] + 0.5f * (rix[i * 3 + f] + rix[-i * 3 + f] - rix[i * 3 + 1] - rix[-i * 3 + 1]);
-            }
-          };
-          if (coloffset == 3) {
-            int f = 2 - xfc(P, row, leftstart);
-            for (int col = leftstart; col < mcol_g - 3; col += coloffset, f ^= 2) body(col, f);
-          } else {
-            coloffset = xfc(P, row, leftstart + 1) == 1 ? 2 : 1;
-            int f = 2 - xfc(P, row, leftstart);
-            for (int col = leftstart; col < mcol_g - 3; col += coloffset, coloffset ^= 3, f = f ^ (coloffset & 2)) body(col, f);
-          }
-        }
-        __syncthreads();
       }
-      // (f) R and B for 2x2 green blocks (:2266-2310): the scan visits the
-      // greens off the solitary-green row and column classes, hexagon
-      // allhex1[row % 3][col % 3]; each writes only its own R and B.
-      if (SITES) {
-        int topstart = top + 2;
-        for (; topstart < mrow_g - 2; topstart++)
-          if ((topstart - P.sgrow) % 3) break;
-        int leftstart = left + 2;
-        for (; leftstart < mcol_g - 2; leftstart++)
-          if ((leftstart - P.sgcol) % 3) break;
-        const int ncols = mcol_g - 2 - leftstart;
-        const int nrows = mrow_g - 2 - topstart;
-        const XDiv fdf(ncols > 0 ? ncols : 1);
-        for (int i = tid; i < (nrows > 0 ? nrows : 0) * (ncols > 0 ? ncols : 0); i += nth) {
-          const int q_ = fdf.div(i), row = topstart + q_, col = leftstart + i - q_ * ncols;
-          if (!((row - P.sgrow) % 3) || !((col - P.sgcol) % 3)) continue;
-          float* rix0 = RGB(0, row - top, col - left);
-          const short* hex = P.allhex1[row % 3][col % 3];
-          // all loads of the four direction planes first, then the stores
-          // (this site's own R and B, which no load reads)
-          float v1[4], a1[4], b1[4], a0[4], b0[4], a2[4], b2[4];
-#pragma unroll
-          for (int q = 0; q < 4; q++) {
-            const float* rix = rix0 + (size_t)q * ts * ts * 3;
-            const int o0 = hex[2 * q] * 3, o1 = hex[2 * q + 1] * 3;
-            v1[q] = rix[1];
-            a1[q] = rix[o0 + 1];
-            b1[q] = rix[o1 + 1];
-            a0[q] = rix[o0];
-            b0[q] = rix[o1];
-            a2[q] = rix[o0 + 2];
-            b2[q] = rix[o1 + 2];
-          }
-#pragma unroll
-          for (int q = 0; q < 4; q++) {
-            float* rix = rix0 + (size_t)q * ts * ts * 3;
-            if (hex[2 * q] + hex[2 * q + 1]) {
-              const float g = 3 * v1[q] - 2 * a1[q] - b1[q];
-              rix[0] = (g + 2 * a0[q] + b0[q]) * 0.33333333f;
-              rix[2] = (g + 2 * a2[q] + b2[q]) * 0.33333333f;
+      __syncthreads();
+      // (f) R and B for 2x2 green blocks (:2266-2310), one row per thread in
+      // the reference's column order
+      int topstart = top + 2;
+      for (; topstart < mrow_g - 2; topstart++)
+        if ((topstart - P.sgrow) % 3) break;
+      int leftstart = left + 2;
+      for (; leftstart < mcol_g - 2; leftstart++)
+        if ((leftstart - P.sgcol) % 3) break;
+      const int coloffsetstart = 2 - (xfc(P, topstart, leftstart + 1) & 1);
+      for (int row = topstart + tid; row < mrow_g - 2; row += nth) {
+        if (!((row - P.sgrow) % 3)) continue;
+        const short* hexmod[2] = {P.allhex1[row % 3][leftstart % 3], P.allhex1[row % 3][(leftstart + coloffsetstart) % 3]};
+        for (int col = leftstart, coloffset = coloffsetstart, hexindex = 0; col < mcol_g - 2;
+             col += coloffset, coloffset ^= 3, hexindex ^= 1) {
+          float* rix = RGB(0, row - top, col - left);
+          const short* hex = hexmod[hexindex];
+          for (int d = 0; d < NDIR; d += 2, rix += (size_t)ts * ts * 3) {
+            const int o0 = hex[d] * 3, o1 = hex[d + 1] * 3;
+            if (hex[d] + hex[d + 1]) {
+              const float g = 3 * rix[1] - 2 * rix[o0 + 1] - rix[o1 + 1];
+              for (int c = 0; c < 4; c += 2) rix[c] = (g + 2 * rix[o0 + c] + rix[o1 + c]) * 0.33333333f;
             } else {
-              const float g = 2 * v1[q] - a1[q] - b1[q];
-              rix[0] = (g + a0[q] + b0[q]) * 0.5f;
-              rix[2] = (g + a2[q] + b2[q]) * 0.5f;
-            }
-          }
-        }
-      } else {
-        int topstart = top + 2;
-        for (; topstart < mrow_g - 2; topstart++)
-          if ((topstart - P.sgrow) % 3) break;
-        int leftstart = left + 2;
-        for (; leftstart < mcol_g - 2; leftstart++)
-          if ((leftstart - P.sgcol) % 3) break;
-        const int coloffsetstart = 2 - (xfc(P, topstart, leftstart + 1) & 1);
-        for (int row = topstart + tid; row < mrow_g - 2; row += nth) {
-          if (!((row - P.sgrow) % 3)) continue;
-          const short* hexmod[2] = {P.allhex1[row % 3][leftstart % 3], P.allhex1[row % 3][(leftstart + coloffsetstart) % 3]};
-          for (int col = leftstart, coloffset = coloffsetstart, hexindex = 0; col < mcol_g - 2;
-               col += coloffset, coloffset ^= 3, hexindex ^= 1) {
-            float* rix = RGB(0, row - top, col - left);
-            const short* hex = hexmod[hexindex];
-            for (int d = 0; d < NDIR; d += 2, rix += (size_t)ts * ts * 3) {
-              const int o0 = hex[d] * 3, o1 = hex[d + 1] * 3;
-              if (hex[d] + hex[d + 1]) {
-                const float g = 3 * rix[1] - 2 * rix[o0 + 1] - rix[o1 + 1];
-                for (int c = 0; c < 4; c += 2) rix[c] = (g + 2 * rix[o0 + c] + rix[o1 + c]) * 0.33333333f;
-              } else {
-                const float g = 2 * rix[1] - rix[o0 + 1] - rix[o1 + 1];
-                for (int c = 0; c < 4; c += 2) rix[c] = (g + rix[o0 + c] + rix[o1 + c]) * 0.5f;
-              }
+              const float g = 2 * rix[1] - rix[o0 + 1] - rix[o1 + 1];
+              for (int c = 0; c < 4; c += 2) rix[c] = (g + rix[o0 + c] + rix[o1 + c]) * 0.5f;
             }
           }
         }
       }
       __syncthreads();
-    }    rgb = S.rgb;
+    }
+    rgb = S.rgb;
     int mrow = mrow_g - top;
     int mcol = mcol_g - left;
 
@@ -1393,7 +1276,7 @@ lre_status launch_xtrans(Context* c, const float* raw, int cstride, float* rgb, 
                                            (int)kXsSmemBytes));
       k_xtrans_3pass_planes<<<nblk, XS_THREADS, kXsSmemBytes, c->stream>>>(A);
     } else {
-      k_xtrans_3pass<false><<<nblk, XT_THREADS, 0, c->stream>>>(A);
+      k_xtrans_3pass<<<nblk, XT_THREADS, 0, c->stream>>>(A);
     }
     count_launch(c);
   }
