@@ -343,7 +343,7 @@ static lre_status xtrans_host(lre_ctx* ctx, const float* raw_rgb, float* rgb, si
   LRE_TRY(check_img(c, raw_rgb, rgb, w, h, "demosaic_xtrans"));
   if (!xtrans) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "demosaic_xtrans: null xtrans pattern");
   std::lock_guard<std::mutex> lk(c->mu);
-  LRE_TRY(begin(c, lre::ws_bytes_xtrans(w, h, passes)));
+  LRE_TRY(begin(c, lre::ws_bytes_xtrans(w, h, passes, xtrans)));
   const size_t bytes = w * h * 3 * sizeof(float);
   LRE_TRY(lre::ensure_buffer(c, &c->d_in, &c->d_in_cap, bytes));
   LRE_TRY(lre::ensure_buffer(c, &c->d_out, &c->d_out_cap, bytes));
@@ -374,7 +374,7 @@ lre_status lre_dev_demosaic_xtrans(lre_ctx* ctx, const float* raw, float* rgb, s
   if (!c) return LRE_ERR_INVALID_ARGUMENT;
   LRE_TRY(check_img(c, raw, rgb, w, h, "demosaic_xtrans"));
   if (!xtrans) return lre::fail(c, LRE_ERR_INVALID_ARGUMENT, "demosaic_xtrans: null xtrans pattern");
-  LRE_TRY(begin(c, lre::ws_bytes_xtrans(w, h, passes)));
+  LRE_TRY(begin(c, lre::ws_bytes_xtrans(w, h, passes, xtrans)));
   return lre::launch_xtrans(c, raw, 1, rgb, w, h, xtrans, maximum_value, passes);
 }
 

@@ -44,6 +44,7 @@ struct XtParams {
 
 struct XtArgs {
   const float* raw;
+  const float* norm;  // dense raw / maximum (plane-resident kernel)
   int cstride;
   float* rgb_out;
   int W, H;
@@ -106,6 +107,13 @@ __device__ __forceinline__ float xraw_hex(const XtArgs& A, int row, int col, int
     v = A.raw[pos * 3 + xfc(A.P, r, c)];
   }
   return v / A.maximum;
+}
+
+// The same samples from the dense normalised mosaic (k_xt_normalize): the
+// value at (row, col), and at a linear offset from it.
+__device__ __forceinline__ float xn(const XtArgs& A, int row, int col) { return A.norm[(size_t)row * A.W + col]; }
+__device__ __forceinline__ float xn_hex(const XtArgs& A, int row, int col, int hex) {
+  return A.norm[(long long)row * A.W + col + hex];
 }
 
 // n / d by a multiply-high, exact while n * d < 2^32 (every loop here); the
@@ -702,10 +710,22 @@ constexpr int kXsMaxCtas = 148;
 constexpr int XDN = XTS - 10;  // derivative plane edge
 constexpr size_t kPlaneFloats = (size_t)XTS * XTS * 3;
 constexpr size_t kPlaneBytes = kPlaneFloats * 4;            // 155,952
-constexpr size_t kXsSmemBytes = kPlaneBytes + kGmmBytes;    // 207,936
+// site lists: 4 of every 3x3 sites per class (the replay's bound), 38 x 38
+// such blocks in a tile
+constexpr int kXsListCap = (XTS / 3) * (XTS / 3) * 4;  // 5,776
+constexpr size_t kXsSmemBytes = kPlaneBytes + kGmmBytes + 2 * kXsListCap * 2 + 2 * XTS;  // 231,268
 constexpr size_t kXsSpillBytes = ((kRgbBytes + kDrvBytes + 255) / 256) * 256;
-static_assert(2 * kHomoBytes <= kXsSmemBytes, "the homogeneity maps reuse the plane's shared memory");
+static_assert(2 * kHomoBytes <= kPlaneBytes + kGmmBytes, "the homogeneity maps reuse the plane and table memory");
 static_assert(kPlaneBytes % 16 == 0 && kHomoBytes % 16 == 0, "float4 fills");
+
+// raw / maximum for every mosaic site, in the reference's IEEE division
+// (xraw), once per image: the plane-resident kernel reads each sample in
+// several steps and for each of its four plane pairs.
+__global__ void k_xt_normalize(XtArgs A, float* norm) {
+  const long long n = (long long)A.W * A.H;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    norm[i] = A.cstride == 1 ? A.raw[i] / A.maximum : xraw(A, (int)(i / A.W), (int)(i % A.W));
+}
 
 // (g) YPbPr derivatives of one finished direction plane D (:2346-2405),
 // yuv recomputed at the three taps, and the plane's RGB, into the CTA's
@@ -749,6 +769,14 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xtrans_3pass_planes(XtArgs Ai
   extern __shared__ __align__(16) unsigned char xs_smem[];
   float* pl = reinterpret_cast<float*>(xs_smem);                   // [XTS][XTS][3]
   float2* gmm = reinterpret_cast<float2*>(xs_smem + kPlaneBytes);  // [XTS][XTS/2] (min, max)
+  // the tile's non-green sites and 2x2-block greens, as row * XTS + column
+  unsigned short* lst_ng = reinterpret_cast<unsigned short*>(xs_smem + kPlaneBytes + kGmmBytes);
+  unsigned short* lst_gg = lst_ng + kXsListCap;
+  // per tile row / column: pattern phase (bits 0-2, mod 6), off the
+  // solitary-green class (bit 3), phase mod 3 (bits 4-5)
+  unsigned char* rinfo = reinterpret_cast<unsigned char*>(lst_gg + kXsListCap);
+  unsigned char* cinfo = rinfo + XTS;
+  __shared__ int s_n[2];
   const int tid = threadIdx.x, nth = blockDim.x;
   __shared__ XtArgs sA;
   {
@@ -778,28 +806,60 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xtrans_3pass_planes(XtArgs Ai
     const int mrow_g = min(top + ts, H - 3);  // global row bound of the computations
     const int mcol_g = min(left + ts, W - 3);
     const int nr = mrow_g - top, nc = mcol_g - left;
-    const XDiv fd_nc(nc);
+    const int warp = tid >> 5, lane = tid & 31, nwarps = nth >> 5;
+
+    // site classes of the tile: line info, then the two site lists (their
+    // order is free: every step's sites are independent)
+    for (int i = tid; i < XTS; i += nth) {
+      const int r6 = (top + i) % 6, c6 = (left + i) % 6;
+      rinfo[i] = (unsigned char)(r6 | (((top + i - P.sgrow) % 3 != 0) << 3) | ((r6 % 3) << 4));
+      cinfo[i] = (unsigned char)(c6 | (((left + i - P.sgcol) % 3 != 0) << 3) | ((c6 % 3) << 4));
+    }
+    if (tid == 0) s_n[0] = s_n[1] = 0;
+    __syncthreads();
+    for (int lr = warp; lr < nr; lr += nwarps) {
+      const int ri = rinfo[lr];
+      for (int c0 = 0; c0 < nc; c0 += 32) {
+        const int lc = c0 + lane;
+        const int ci = lc < nc ? cinfo[lc] : 0;
+        const bool ng = lc < nc && !(P.xt[ri >> 4][ci >> 4] & 1);
+        const bool gg = lc < nc && (ri & 8) && (ci & 8);
+        const unsigned mng = __ballot_sync(0xffffffffu, ng), mgg = __ballot_sync(0xffffffffu, gg);
+        int bng = 0, bgg = 0;
+        if (lane == 0) {
+          bng = atomicAdd(&s_n[0], __popc(mng));
+          bgg = atomicAdd(&s_n[1], __popc(mgg));
+        }
+        bng = __shfl_sync(0xffffffffu, bng, 0);
+        bgg = __shfl_sync(0xffffffffu, bgg, 0);
+        const unsigned lt = (1u << lane) - 1u;
+        if (ng) lst_ng[bng + __popc(mng & lt)] = (unsigned short)(lr * XTS + lc);
+        if (gg) lst_gg[bgg + __popc(mgg & lt)] = (unsigned short)(lr * XTS + lc);
+      }
+    }
+    __syncthreads();
+    const int n_ng = s_n[0], n_gg = s_n[1];
 
     // (a) green min / max (:1968-2053).  The scan stores a site's hexagon
     // min/max at its half-column slot; on rows with adjacent non-green pairs
     // it stores the first site's values at both sites' slots and computes
     // none for the second.
-    for (int i = tid; i < nr * nc; i += nth) {
-      const int lr = fd_nc.div(i), lc = i - lr * nc;
+    for (int j = tid; j < n_ng; j += nth) {
+      const int e = lst_ng[j], lr = e / XTS, lc = e - lr * XTS;
+      const int r3 = rinfo[lr] >> 4;
+      if (lc > 0 && !(P.xt[r3][cinfo[lc - 1] >> 4] & 1)) continue;  // second of a pair
       const int row = top + lr, col = left + lc;
-      if (xisgreen(P, row, col)) continue;
-      if (lc > 0 && !xisgreen(P, row, col - 1)) continue;  // second of a pair
-      const short* hex = P.allhex0[row % 3][col % 3];
+      const short* hex = P.allhex0[r3][cinfo[lc] >> 4];
       float minval = FLT_MAX, maxval = 0.f;
       for (int c = 0; c < 6; c++) {
-        const float val = xraw_hex(A, row, col, hex[c]);
+        const float val = xn_hex(A, row, col, hex[c]);
         minval = minval < val ? minval : val;
         maxval = maxval > val ? maxval : val;
       }
       const float2 v = make_float2(minval, maxval);
       float2* g = gmm + (size_t)lr * (ts / 2);
       g[lc >> 1] = v;
-      if (lc + 1 < nc && !xisgreen(P, row, col + 1)) g[(lc + 1) >> 1] = v;
+      if (lc + 1 < nc && !(P.xt[r3][cinfo[lc + 1] >> 4] & 1)) g[(lc + 1) >> 1] = v;
     }
 
     for (int k = 0; k < 4; k++) {
@@ -811,30 +871,36 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xtrans_3pass_planes(XtArgs Ai
         for (int i = tid; i < (int)(kPlaneBytes / 16); i += nth) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
       __syncthreads();
-      for (int i = tid; i < nr * nc; i += nth) {
-        const int lr = fd_nc.div(i), lc = i - lr * nc;
+      for (int lr = warp; lr < nr; lr += nwarps) {
+        const int r6 = rinfo[lr] & 7;
+        const float* src = A.norm + (size_t)(top + lr) * W + left;
+        float* prow = pl + lr * ts * 3;
+        for (int lc = lane; lc < nc; lc += 32) {
+          const int fcv = P.xt[r6][cinfo[lc] & 7];
+          if (k == 0 || lr * ts + lc != ts * ts - 1 || fcv != 2) prow[lc * 3 + fcv] = src[lc];
+        }
+      }
+      for (int j = tid; j < n_ng; j += nth) {
+        const int e = lst_ng[j], lr = e / XTS, lc = e - lr * XTS;
         const int row = top + lr, col = left + lc;
-        float* rix = pl + (lr * ts + lc) * 3;
-        const int fcv = xfc(P, row, col);
-        if (k == 0 || (lr * ts + lc) * 3 + fcv != (int)kPlaneFloats - 1) rix[fcv] = xraw(A, row, col);
-        if (fcv == 1) continue;
-        const short* hex = P.allhex0[row % 3][col % 3];
-        const int cdir = k ^ (P.right_shift[row % 3] == 1 ? 0 : 1);
+        const int r3 = rinfo[lr] >> 4;
+        const short* hex = P.allhex0[r3][cinfo[lc] >> 4];
+        const int cdir = k ^ (P.right_shift[r3] == 1 ? 0 : 1);
         float color;
         if (cdir == 0) {
-          color = 0.6796875f * (xraw_hex(A, row, col, hex[1]) + xraw_hex(A, row, col, hex[0])) -
-                  0.1796875f * (xraw_hex(A, row, col, 2 * hex[1]) + xraw_hex(A, row, col, 2 * hex[0]));
+          color = 0.6796875f * (xn_hex(A, row, col, hex[1]) + xn_hex(A, row, col, hex[0])) -
+                  0.1796875f * (xn_hex(A, row, col, 2 * hex[1]) + xn_hex(A, row, col, 2 * hex[0]));
         } else if (cdir == 1) {
-          color = 0.87109375f * xraw_hex(A, row, col, hex[3]) + xraw_hex(A, row, col, hex[2]) * 0.12890625f +
-                  0.359375f * (xraw_hex(A, row, col, 0) - xraw_hex(A, row, col, -hex[2]));
+          color = 0.87109375f * xn_hex(A, row, col, hex[3]) + xn_hex(A, row, col, hex[2]) * 0.12890625f +
+                  0.359375f * (xn_hex(A, row, col, 0) - xn_hex(A, row, col, -hex[2]));
         } else {
           const int h4 = hex[cdir + 2];
-          color = 0.640625f * xraw_hex(A, row, col, h4) + 0.359375f * xraw_hex(A, row, col, -2 * h4) +
-                  0.12890625f * (2.f * xraw_hex(A, row, col, 0) - xraw_hex(A, row, col, 3 * h4) -
-                                 xraw_hex(A, row, col, -3 * h4));
+          color = 0.640625f * xn_hex(A, row, col, h4) + 0.359375f * xn_hex(A, row, col, -2 * h4) +
+                  0.12890625f * (2.f * xn_hex(A, row, col, 0) - xn_hex(A, row, col, 3 * h4) -
+                                 xn_hex(A, row, col, -3 * h4));
         }
         const float2 mmv = gmm[(size_t)lr * (ts / 2) + (lc >> 1)];
-        rix[1] = LIMf(color, mmv.x, mmv.y);
+        pl[e * 3 + 1] = LIMf(color, mmv.x, mmv.y);
       }
       __syncthreads();
 
@@ -848,23 +914,19 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xtrans_3pass_planes(XtArgs Ai
         // (c) recalculate green from closer pixels (:2138-2183): direction
         // d = 3..5 updates plane (d - 2) ^ flip, reading green sites only
         if (pass) {
-          const int rows = nr - 4, ncols = nc - 4;
-          if (rows > 0 && ncols > 0) {
-            const XDiv fd(ncols);
-            for (int i = tid; i < rows * ncols; i += nth) {
-              const int q = fd.div(i), lr = 2 + q, lc = 2 + i - q * ncols;
-              const int row = top + lr, col = left + lc;
-              if (xisgreen(P, row, col)) continue;
-              const int dd = k ^ (P.right_shift[row % 3] == 1 ? 0 : 1);
-              if (dd == 0) continue;
-              const int f = xfc(P, row, col);
-              const int hx = P.allhex1[row % 3][col % 3][dd + 2];
-              float* rix = pl + (lr * ts + lc) * 3;
-              const int o1 = hx * 3, o2 = -2 * hx * 3;
-              const float val = 0.33333333f * (rix[o2 + 1] + 2 * (rix[o1 + 1] - rix[o1 + f]) - rix[o2 + f]) + rix[f];
-              const float2 mmv = gmm[(size_t)lr * (ts / 2) + (lc >> 1)];
-              rix[1] = LIMf(val, mmv.x, mmv.y);
-            }
+          for (int j = tid; j < n_ng; j += nth) {
+            const int e = lst_ng[j], lr = e / XTS, lc = e - lr * XTS;
+            if (lr < 2 || lr >= nr - 2 || lc < 2 || lc >= nc - 2) continue;
+            const int ri = rinfo[lr], ci = cinfo[lc];
+            const int dd = k ^ (P.right_shift[ri >> 4] == 1 ? 0 : 1);
+            if (dd == 0) continue;
+            const int f = P.xt[ri & 7][ci & 7];
+            const int hx = P.allhex1[ri >> 4][ci >> 4][dd + 2];
+            float* rix = pl + e * 3;
+            const int o1 = hx * 3, o2 = -2 * hx * 3;
+            const float val = 0.33333333f * (rix[o2 + 1] + 2 * (rix[o1 + 1] - rix[o1 + f]) - rix[o2 + f]) + rix[f];
+            const float2 mmv = gmm[(size_t)lr * (ts / 2) + (lc >> 1)];
+            rix[1] = LIMf(val, mmv.x, mmv.y);
           }
           __syncthreads();
         }
@@ -921,56 +983,42 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xtrans_3pass_planes(XtArgs Ai
         // (e) red for blue pixels and vice versa (:2224-2264): every non-green
         // site writes its other colour f = 2 - own
         {
-          const int rows = nr - 6, ncols = nc - 6;
-          if (rows > 0 && ncols > 0) {
-            const XDiv fd(ncols);
-            for (int i = tid; i < rows * ncols; i += nth) {
-              const int q = fd.div(i), lr = 3 + q, lc = 3 + i - q * ncols;
-              const int row = top + lr, col = left + lc;
-              if (xisgreen(P, row, col)) continue;
-              const int c = ((row - P.sgrow) % 3) ? ts : 1;
-              const int h = 3 * (c ^ ts ^ 1);
-              const int f = 2 - xfc(P, row, col);
-              float* rix = pl + (lr * ts + lc) * 3;
-              const float g0 = rix[1];
-              const bool use_c = k > 1 || ((k ^ c) & 1) ||
-                                 ((fabsf(g0 - rix[c * 3 + 1]) + fabsf(g0 - rix[-c * 3 + 1])) <
-                                  2.f * (fabsf(g0 - rix[h * 3 + 1]) + fabsf(g0 - rix[-h * 3 + 1])));
-              const int s = use_c ? c : h;
-              rix[f] = g0 + 0.5f * (rix[s * 3 + f] + rix[-s * 3 + f] - rix[s * 3 + 1] - rix[-s * 3 + 1]);
-            }
+          for (int j = tid; j < n_ng; j += nth) {
+            const int e = lst_ng[j], lr = e / XTS, lc = e - lr * XTS;
+            if (lr < 3 || lr >= nr - 3 || lc < 3 || lc >= nc - 3) continue;
+            const int ri = rinfo[lr];
+            const int c = (ri & 8) ? ts : 1;  // (row - sgrow) % 3 != 0
+            const int h = 3 * (c ^ ts ^ 1);
+            const int f = 2 - P.xt[ri & 7][cinfo[lc] & 7];
+            float* rix = pl + e * 3;
+            const float g0 = rix[1];
+            const bool use_c = k > 1 || ((k ^ c) & 1) ||
+                               ((fabsf(g0 - rix[c * 3 + 1]) + fabsf(g0 - rix[-c * 3 + 1])) <
+                                2.f * (fabsf(g0 - rix[h * 3 + 1]) + fabsf(g0 - rix[-h * 3 + 1])));
+            const int s = use_c ? c : h;
+            rix[f] = g0 + 0.5f * (rix[s * 3 + f] + rix[-s * 3 + f] - rix[s * 3 + 1] - rix[-s * 3 + 1]);
           }
         }
         __syncthreads();
         // (f) R and B for 2x2 green blocks (:2266-2310): greens off the
         // solitary-green row and column classes, hexagon allhex1
         {
-          int topstart = top + 2;
-          for (; topstart < mrow_g - 2; topstart++)
-            if ((topstart - P.sgrow) % 3) break;
-          int leftstart = left + 2;
-          for (; leftstart < mcol_g - 2; leftstart++)
-            if ((leftstart - P.sgcol) % 3) break;
-          const int ncols = mcol_g - 2 - leftstart, nrows = mrow_g - 2 - topstart;
-          if (nrows > 0 && ncols > 0) {
-            const XDiv fd(ncols);
-            for (int i = tid; i < nrows * ncols; i += nth) {
-              const int q = fd.div(i), row = topstart + q, col = leftstart + i - q * ncols;
-              if (!((row - P.sgrow) % 3) || !((col - P.sgcol) % 3)) continue;
-              float* rix = pl + ((row - top) * ts + (col - left)) * 3;
-              const short* hex = P.allhex1[row % 3][col % 3];
-              const int o0 = hex[2 * k] * 3, o1 = hex[2 * k + 1] * 3;
-              const float v1 = rix[1], a1 = rix[o0 + 1], b1 = rix[o1 + 1];
-              const float a0 = rix[o0], b0 = rix[o1], a2 = rix[o0 + 2], b2 = rix[o1 + 2];
-              if (hex[2 * k] + hex[2 * k + 1]) {
-                const float g = 3 * v1 - 2 * a1 - b1;
-                rix[0] = (g + 2 * a0 + b0) * 0.33333333f;
-                rix[2] = (g + 2 * a2 + b2) * 0.33333333f;
-              } else {
-                const float g = 2 * v1 - a1 - b1;
-                rix[0] = (g + a0 + b0) * 0.5f;
-                rix[2] = (g + a2 + b2) * 0.5f;
-              }
+          for (int j = tid; j < n_gg; j += nth) {
+            const int e = lst_gg[j], lr = e / XTS, lc = e - lr * XTS;
+            if (lr < 2 || lr >= nr - 2 || lc < 2 || lc >= nc - 2) continue;
+            float* rix = pl + e * 3;
+            const short* hex = P.allhex1[rinfo[lr] >> 4][cinfo[lc] >> 4];
+            const int o0 = hex[2 * k] * 3, o1 = hex[2 * k + 1] * 3;
+            const float v1 = rix[1], a1 = rix[o0 + 1], b1 = rix[o1 + 1];
+            const float a0 = rix[o0], b0 = rix[o1], a2 = rix[o0 + 2], b2 = rix[o1 + 2];
+            if (hex[2 * k] + hex[2 * k + 1]) {
+              const float g = 3 * v1 - 2 * a1 - b1;
+              rix[0] = (g + 2 * a0 + b0) * 0.33333333f;
+              rix[2] = (g + 2 * a2 + b2) * 0.33333333f;
+            } else {
+              const float g = 2 * v1 - a1 - b1;
+              rix[0] = (g + a0 + b0) * 0.5f;
+              rix[2] = (g + a2 + b2) * 0.5f;
             }
           }
         }
@@ -1119,6 +1167,11 @@ XtParams make_xt_params(const char* xtrans, int width) {
 bool xt_sites_ok(const XtParams& P) {
   auto isg = [&](int r, int c) { return P.xt[((r % 3) + 3) % 3][((c % 3) + 3) % 3] & 1; };
   auto fc = [&](int r, int c) { return (int)P.xt[(r + 6) % 6][(c + 6) % 6]; };
+  // the plane kernel's site lists hold at most 4 non-green sites per 3x3
+  int greens = 0;
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) greens += isg(r, c);
+  if (9 - greens > 4) return false;
   for (int t0 = 0; t0 < 6; t0++)
     for (int l0 = 0; l0 < 6; l0++) {
       const int top = 6 + t0, left = 6 + l0, mrow = top + 30, mcol = left + 30;
@@ -1226,16 +1279,19 @@ bool xt_sites_ok(const XtParams& P) {
 
 }  // namespace
 
-size_t ws_bytes_xtrans(size_t w, size_t h, int passes) {
-  (void)w;
-  (void)h;
-  return passes == 1 ? 0 : std::max((size_t)kXtMaxCtas * kXtSlabBytes, (size_t)kXsMaxCtas * kXsSpillBytes) + 4096;
+size_t ws_bytes_xtrans(size_t w, size_t h, int passes, const char* xtrans) {
+  if (passes == 1) return 0;
+  const size_t planes = (size_t)kXsMaxCtas * kXsSpillBytes + ((w * h * sizeof(float) + 255) / 256) * 256;
+  const size_t rowscan = (size_t)kXtMaxCtas * kXtSlabBytes;
+  if (xtrans) return (xt_sites_ok(make_xt_params(xtrans, (int)w)) ? planes : rowscan) + 4096;
+  return std::max(rowscan, planes) + 4096;
 }
 
 lre_status launch_xtrans(Context* c, const float* raw, int cstride, float* rgb, size_t w, size_t h, const char* xtrans,
                          float maximum_value, int passes) {
   XtArgs A;
   A.raw = raw;
+  A.norm = nullptr;
   A.cstride = cstride;
   A.rgb_out = rgb;
   A.W = (int)w;
@@ -1265,6 +1321,13 @@ lre_status launch_xtrans(Context* c, const float* raw, int cstride, float* rgb, 
     // one 1024-thread CTA per SM.  Others run the row-scan kernel, two
     // 512-thread CTAs per SM, each with its whole tile in a global slab.
     const bool sites = xt_sites_ok(A.P);
+    if (sites) {
+      float* norm = reinterpret_cast<float*>(c->ws.take(w * h * sizeof(float)));
+      if (!norm) return fail(c, LRE_ERR_OUT_OF_MEMORY, "demosaic_xtrans_3pass: workspace too small");
+      k_xt_normalize<<<grid_for(w * h, 256, c->sm_count * 8), 256, 0, c->stream>>>(A, norm);
+      count_launch(c);
+      A.norm = norm;
+    }
     const int nblk = sites ? std::min(std::min(tiles, c->sm_count), kXsMaxCtas)
                            : std::min(std::min(tiles, c->sm_count * kXtCtasPerSm), kXtMaxCtas);
     A.scratch = reinterpret_cast<unsigned char*>(c->ws.take((size_t)nblk * (sites ? kXsSpillBytes : kXtSlabBytes)));

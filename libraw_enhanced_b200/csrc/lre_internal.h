@@ -190,7 +190,9 @@ size_t ws_bytes_detail_tonemap(size_t w, size_t h);
 size_t ws_bytes_micro_contrast(size_t w, size_t h);
 size_t ws_bytes_lateral(size_t w, size_t h, int cell, int levels, bool in_place);
 size_t ws_bytes_amaze(size_t w, size_t h);
-size_t ws_bytes_xtrans(size_t w, size_t h, int passes);
+// xtrans (nullable): the 6x6 pattern; with it the size is that of the kernel
+// the pattern selects, without it the larger of the two.
+size_t ws_bytes_xtrans(size_t w, size_t h, int passes, const char* xtrans = nullptr);
 
 }  // namespace lre
 

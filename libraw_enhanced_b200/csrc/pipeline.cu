@@ -40,7 +40,7 @@ size_t stage_ws(const lre_develop_params& p, size_t w, size_t h) {
   size_t m = 0;
   switch (route(p)) {
     case Demosaic::Xtrans1: m = std::max(m, lre::ws_bytes_xtrans(w, h, 1)); break;
-    case Demosaic::Xtrans3: m = std::max(m, lre::ws_bytes_xtrans(w, h, 3)); break;
+    case Demosaic::Xtrans3: m = std::max(m, lre::ws_bytes_xtrans(w, h, 3, p.xtrans)); break;
     case Demosaic::Dcb: m = std::max(m, lre::ws_bytes_dcb(w, h)); break;
     case Demosaic::Aahd: m = std::max(m, lre::ws_bytes_aahd(w, h)); break;
     case Demosaic::Linear: break;
