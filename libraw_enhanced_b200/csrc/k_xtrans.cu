@@ -19,6 +19,7 @@
 //   row per thread in its column order, with the whole tile (8 directions x
 //   114^2 RGB, derivatives, homogeneity maps) in a per-CTA global slab.
 #include <cfloat>
+#include <cstdlib>
 #include <cstring>
 
 #include "common.cuh"
@@ -1277,13 +1278,22 @@ bool xt_sites_ok(const XtParams& P) {
   return true;
 }
 
+// The plane-resident kernel runs where the replay accepts the pattern,
+// unless LRE_XTRANS_ROWSCAN=1 asks for the row-scan kernel (a test hook:
+// it keeps the fallback path covered on the X-Trans layouts).
+bool xt_use_planes(const XtParams& P) {
+  const char* force = std::getenv("LRE_XTRANS_ROWSCAN");
+  if (force && force[0] == '1') return false;
+  return xt_sites_ok(P);
+}
+
 }  // namespace
 
 size_t ws_bytes_xtrans(size_t w, size_t h, int passes, const char* xtrans) {
   if (passes == 1) return 0;
   const size_t planes = (size_t)kXsMaxCtas * kXsSpillBytes + ((w * h * sizeof(float) + 255) / 256) * 256;
   const size_t rowscan = (size_t)kXtMaxCtas * kXtSlabBytes;
-  if (xtrans) return (xt_sites_ok(make_xt_params(xtrans, (int)w)) ? planes : rowscan) + 4096;
+  if (xtrans) return (xt_use_planes(make_xt_params(xtrans, (int)w)) ? planes : rowscan) + 4096;
   return std::max(rowscan, planes) + 4096;
 }
 
@@ -1320,7 +1330,7 @@ lre_status launch_xtrans(Context* c, const float* raw, int cstride, float* rgb, 
     // Patterns whose scans the replay confirms run the plane-resident kernel:
     // one 1024-thread CTA per SM.  Others run the row-scan kernel, two
     // 512-thread CTAs per SM, each with its whole tile in a global slab.
-    const bool sites = xt_sites_ok(A.P);
+    const bool sites = xt_use_planes(A.P);
     if (sites) {
       float* norm = reinterpret_cast<float*>(c->ws.take(w * h * sizeof(float)));
       if (!norm) return fail(c, LRE_ERR_OUT_OF_MEMORY, "demosaic_xtrans_3pass: workspace too small");

@@ -115,6 +115,22 @@ def test_xtrans_3pass_parity(acc, h, w):
 
 
 @pytest.mark.parametrize("h,w", [(1024, 1536), (131, 211)])
+def test_xtrans_3pass_rowscan_kernel(acc, monkeypatch, h, w):
+    """The row-scan kernel (the fallback for 6x6 patterns whose scans are
+    not site-parallel), forced on the X-Trans layout, against the same
+    reference run and bit for bit against the plane-resident kernel."""
+    rgb = scenes.scene_rgb(h, w, 23)
+    mos = scenes.mosaic(rgb, scenes.XTRANS_STD, (1.8, 1.0, 1.6, 1.0), 23)
+    sp = scenes.sparse_rgb(mos, scenes.XTRANS_STD)
+    ref = oracle.xtrans(sp, scenes.XTRANS_STD, 3, fresh_tiles=True)
+    planes = acc.demosaic_xtrans_3pass(sp, scenes.XTRANS_STD)
+    monkeypatch.setenv("LRE_XTRANS_ROWSCAN", "1")
+    rowscan = acc.demosaic_xtrans_3pass(sp, scenes.XTRANS_STD)
+    assert_parity(rowscan, ref, what=f"xtrans3 row-scan {w}x{h}")
+    assert np.array_equal(rowscan, planes)
+
+
+@pytest.mark.parametrize("h,w", [(1024, 1536), (131, 211)])
 def test_xtrans_1pass_parity(acc, h, w):
     rgb = scenes.scene_rgb(h, w, 22)
     mos = scenes.mosaic(rgb, scenes.XTRANS_STD, (1.8, 1.0, 1.6, 1.0), 22)
