@@ -558,15 +558,17 @@ typedef struct lre_server_config {
   int device;
   int lanes;                  /* concurrent requests on the device (0: 4)     */
   size_t device_budget_bytes; /* admission limit on resident buffers (0: 150 GB) */
+  int decode_threads;         /* host threads running decode callbacks (0: 2) */
 } lre_server_config;
 
 typedef struct lre_request_stats {
   lre_status status;
   int lane;
-  double queue_ms;  /* submit -> admitted                                     */
+  double queue_ms;  /* ready (submitted, or decoded) -> admitted              */
   double run_ms;    /* admitted -> result in host memory                      */
   double total_ms;  /* submit -> result in host memory                        */
   size_t device_bytes;
+  double decode_ms; /* submit -> decode callback returned (0 without one)     */
 } lre_request_stats;
 
 typedef struct lre_server lre_server;
@@ -577,6 +579,20 @@ const char* lre_server_last_error(const lre_server* s);
 /* Queue a request; the image's buffers must stay valid until it completes.
  * Returns LRE_ERR_BUSY when the request alone exceeds the budget. */
 lre_status lre_server_submit(lre_server* s, const lre_image* img, uint64_t* ticket);
+/* Host-side decode overlapped with device work.  The reference decodes a
+ * file with LibRaw on the CPU (load_file and unpack,
+ * core/libraw_wrapper.cpp:2489-2503) before any develop stage runs; it has no
+ * server, so nothing overlaps that decode.  This queues a request whose
+ * mosaic is not decoded yet: one of the server's decode threads calls
+ * decode(user, mosaic, width, height) to fill img->mosaic (caller-owned,
+ * width * height floats, written through the callback), and the request
+ * then joins the device queue.  While a decode thread works on one file,
+ * the lanes develop earlier ones.  A non-LRE_OK return from decode
+ * completes the request with that status.  The callback may run on any
+ * decode thread, concurrently with itself for other requests. */
+typedef lre_status (*lre_decode_fn)(void* user, float* mosaic, size_t width, size_t height);
+lre_status lre_server_submit_decode(lre_server* s, const lre_image* img, lre_decode_fn decode, void* user,
+                                    uint64_t* ticket);
 /* Block until the request completes (timeout_ms < 0: no limit); LRE_ERR_TIMEOUT
  * if it has not completed in time.  The ticket is released on completion. */
 lre_status lre_server_wait(lre_server* s, uint64_t ticket, double timeout_ms, lre_request_stats* stats);

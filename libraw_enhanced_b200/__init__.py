@@ -575,9 +575,9 @@ class Server:
     device-memory budget.  ``submit`` queues a request and returns a ticket;
     ``wait`` returns the result and its latency record."""
 
-    def __init__(self, device: int = 0, lanes: int = 4, budget_bytes: int = 150 * 10**9):
+    def __init__(self, device: int = 0, lanes: int = 4, budget_bytes: int = 150 * 10**9, decode_threads: int = 2):
         self._lib = _lib.load()
-        cfg = _lib.ServerConfig(int(device), int(lanes), int(budget_bytes))
+        cfg = _lib.ServerConfig(int(device), int(lanes), int(budget_bytes), int(decode_threads))
         h = C.c_void_p()
         st = self._lib.lre_server_create(C.byref(cfg), C.byref(h))
         if st != _lib.LRE_OK:
@@ -615,15 +615,46 @@ class Server:
         self._live[t.value] = (m, out)
         return t.value
 
+    def submit_decode(self, shape, params: DevelopParams, decode, out=None) -> int:
+        """Queue a request whose mosaic is produced on the host first, the way
+        the reference runs LibRaw's ``unpack`` before developing.
+        ``decode(mosaic)`` receives a writable (H, W) float32 array and fills
+        it; it runs on one of the server's decode threads while the device
+        develops earlier requests.  An exception in ``decode`` fails the
+        request and is raised again by ``wait``."""
+        h, w = (int(shape[0]), int(shape[1]))
+        m = np.empty((h, w), dtype=np.float32)
+        if out is None:
+            out = _out_for(h, w, params)
+        errors = []
+
+        def _run(user, ptr, width, height):
+            try:
+                decode(np.ctypeslib.as_array(ptr, shape=(int(height), int(width))))
+                return _lib.LRE_OK
+            except Exception as e:  # reported by wait()
+                errors.append(e)
+                return 1  # LRE_ERR_INVALID_ARGUMENT
+
+        cb = _lib.DECODE_FN(_run)
+        img = _lib.Image(m.ctypes.data, out.ctypes.data, w, h, params)
+        t = C.c_uint64()
+        self._check(self._lib.lre_server_submit_decode(self._h, C.byref(img), cb, None, C.byref(t)))
+        self._live[t.value] = (m, out, cb, errors)
+        return t.value
+
     def wait(self, ticket: int, timeout_ms: float = -1.0):
         st = _lib.RequestStats()
         r = self._lib.lre_server_wait(self._h, int(ticket), float(timeout_ms), C.byref(st))
         if r == 5:  # LRE_ERR_TIMEOUT: still running
             raise TimeoutError(f"request {ticket} not complete after {timeout_ms} ms")
-        m, out = self._live.pop(int(ticket), (None, None))
+        live = self._live.pop(int(ticket), (None, None))
+        out = live[1]
+        if len(live) > 2 and live[3]:
+            raise live[3][0]
         self._check(r)
         return out, {"queue_ms": st.queue_ms, "run_ms": st.run_ms, "total_ms": st.total_ms, "lane": st.lane,
-                     "device_bytes": st.device_bytes}
+                     "device_bytes": st.device_bytes, "decode_ms": st.decode_ms}
 
     def memory(self):
         a, b = C.c_size_t(), C.c_size_t()

@@ -151,7 +151,8 @@ class BatchStats(C.Structure):
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("device", C.c_int), ("lanes", C.c_int), ("device_budget_bytes", C.c_size_t)]
+    _fields_ = [("device", C.c_int), ("lanes", C.c_int), ("device_budget_bytes", C.c_size_t),
+                ("decode_threads", C.c_int)]
 
 
 class RequestStats(C.Structure):
@@ -162,7 +163,12 @@ class RequestStats(C.Structure):
         ("run_ms", C.c_double),
         ("total_ms", C.c_double),
         ("device_bytes", C.c_size_t),
+        ("decode_ms", C.c_double),
     ]
+
+
+# lre_decode_fn: status (void* user, float* mosaic, size_t width, size_t height)
+DECODE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_float), C.c_size_t, C.c_size_t)
 
 
 _p = C.c_void_p
@@ -255,6 +261,7 @@ SIGNATURES = {
     "lre_server_destroy": (None, [_p]),
     "lre_server_last_error": (C.c_char_p, [_p]),
     "lre_server_submit": (_st, [_p, C.POINTER(Image), C.POINTER(C.c_uint64)]),
+    "lre_server_submit_decode": (_st, [_p, C.POINTER(Image), DECODE_FN, _p, C.POINTER(C.c_uint64)]),
     "lre_server_wait": (_st, [_p, C.c_uint64, C.c_double, C.POINTER(RequestStats)]),
     "lre_server_memory": (_st, [_p, C.POINTER(_sz), C.POINTER(_sz)]),
 }

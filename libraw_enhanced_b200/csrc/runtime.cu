@@ -492,7 +492,9 @@ struct Request {
   uint64_t ticket = 0;
   lre_image img{};
   size_t bytes = 0;
-  Clock::time_point t_submit, t_admit, t_done;
+  lre_decode_fn decode = nullptr;  // fills img.mosaic on a decode thread first
+  void* user = nullptr;
+  Clock::time_point t_submit, t_ready, t_admit, t_done;  // t_ready: joined the device queue
   lre_status status = LRE_OK;
   int lane = -1;
   bool done = false;
@@ -506,7 +508,11 @@ struct Server {
   std::vector<char> finished;     // per lane: completion callback fired
   std::mutex mu;
   std::condition_variable cv_sched, cv_done;
-  std::deque<Request*> queue;
+  std::deque<Request*> queue;     // ready for a lane
+  std::deque<Request*> decode_q;  // waiting for a decode thread
+  int decoding = 0;               // decode callbacks running
+  std::condition_variable cv_decode;
+  std::vector<std::thread> decoders;
   std::unordered_map<uint64_t, Request*> reqs;
   uint64_t next_ticket = 1;
   size_t resident = 0, peak = 0;
@@ -560,7 +566,7 @@ void scheduler(Server* s) {
   for (;;) {
     reap(s);
     bool any_running = std::any_of(s->running.begin(), s->running.end(), [](Request* r) { return r != nullptr; });
-    if (s->stop && s->queue.empty() && !any_running) break;
+    if (s->stop && s->queue.empty() && !any_running && s->decode_q.empty() && s->decoding == 0) break;
     // admit FIFO while a lane is idle and the budget holds
     bool admitted = false;
     while (!s->queue.empty()) {
@@ -616,6 +622,91 @@ void scheduler(Server* s) {
     }
     if (!admitted) s->cv_sched.wait(lk);
   }
+}
+
+// Decode thread: runs queued decode callbacks (FIFO) outside the lock and
+// moves each decoded request to the device queue.  Drains its queue before
+// it stops, so destroying the server finishes every submitted request.
+void decoder(Server* s) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    s->cv_decode.wait(lk, [&] { return s->stop || !s->decode_q.empty(); });
+    if (s->decode_q.empty()) break;  // stopping, nothing left
+    Request* r = s->decode_q.front();
+    s->decode_q.pop_front();
+    s->decoding++;
+    lk.unlock();
+    const lre_status st = r->decode(r->user, const_cast<float*>(r->img.mosaic), r->img.width, r->img.height);
+    lk.lock();
+    s->decoding--;
+    r->t_ready = Clock::now();
+    if (st != LRE_OK) {
+      r->status = st;
+      r->t_admit = r->t_done = r->t_ready;
+      r->done = true;
+      s->err = "server: the decode callback returned an error";
+      s->cv_done.notify_all();
+    } else {
+      s->queue.push_back(r);
+    }
+    s->cv_sched.notify_one();
+  }
+}
+
+// Validation, budget check and page-locking shared by both submit forms.
+lre_status prepare_request(Server* s, const lre_image* img, Request** out) {
+  if (!img->mosaic || !img->out) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->err = "server: null buffer";
+    return LRE_ERR_INVALID_ARGUMENT;
+  }
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    lre_status st = develop_validate(&s->vctx, &img->params, img->width, img->height);
+    if (st != LRE_OK) {
+      s->err = "server: " + s->vctx.last_error;
+      return st;
+    }
+  }
+  Request* r = new Request();
+  r->img = *img;
+  r->bytes = image_device_bytes(*img);
+  if (r->bytes > s->cfg.device_budget_bytes) {
+    delete r;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->err = "server: request needs more device memory than the budget";
+    return LRE_ERR_BUSY;
+  }
+  cudaSetDevice(s->cfg.device);
+  if (r->pins.pin(img->mosaic, mosaic_bytes_of(*img)) != cudaSuccess ||
+      r->pins.pin(img->out, out_bytes_of(*img)) != cudaSuccess) {
+    delete r;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->err = "server: cannot page-lock the request's host buffers";
+    return LRE_ERR_OUT_OF_MEMORY;
+  }
+  r->t_submit = r->t_ready = Clock::now();
+  *out = r;
+  return LRE_OK;
+}
+
+// Tickets the request and queues it (device queue, or the decode queue when
+// it has a decode callback).
+lre_status enqueue_request(Server* s, Request* r, uint64_t* ticket) {
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) {
+      delete r;
+      return LRE_ERR_BUSY;
+    }
+    r->ticket = s->next_ticket++;
+    s->reqs[r->ticket] = r;
+    (r->decode ? s->decode_q : s->queue).push_back(r);
+    *ticket = r->ticket;
+  }
+  if (r->decode) s->cv_decode.notify_one();
+  else s->cv_sched.notify_one();
+  return LRE_OK;
 }
 
 }  // namespace
@@ -755,7 +846,10 @@ lre_status lre_server_create(const lre_server_config* cfg, lre_server** out) {
   }
   s->running.assign(s->cfg.lanes, nullptr);
   s->finished.assign(s->cfg.lanes, 0);
+  if (s->cfg.decode_threads <= 0) s->cfg.decode_threads = 2;
+  s->cfg.decode_threads = std::min(s->cfg.decode_threads, 16);
   s->sched = std::thread(lre::scheduler, s);
+  for (int i = 0; i < s->cfg.decode_threads; i++) s->decoders.emplace_back(lre::decoder, s);
   *out = reinterpret_cast<lre_server*>(s);
   return LRE_OK;
 }
@@ -768,6 +862,8 @@ void lre_server_destroy(lre_server* sp) {
     s->stop = true;
   }
   s->cv_sched.notify_all();
+  s->cv_decode.notify_all();
+  for (auto& t : s->decoders) t.join();  // the decode queue is drained first
   if (s->sched.joinable()) s->sched.join();
   cudaSetDevice(s->cfg.device);
   for (auto& l : s->L) lre::lane_close(l);
@@ -783,50 +879,20 @@ const char* lre_server_last_error(const lre_server* sp) {
 lre_status lre_server_submit(lre_server* sp, const lre_image* img, uint64_t* ticket) {
   Server* s = reinterpret_cast<Server*>(sp);
   if (!s || !img || !ticket) return LRE_ERR_INVALID_ARGUMENT;
-  if (!img->mosaic || !img->out) {
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->err = "server: null buffer";
-    return LRE_ERR_INVALID_ARGUMENT;
-  }
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    lre_status st = lre::develop_validate(&s->vctx, &img->params, img->width, img->height);
-    if (st != LRE_OK) {
-      s->err = "server: " + s->vctx.last_error;
-      return st;
-    }
-  }
-  lre::Request* r = new lre::Request();
-  r->img = *img;
-  r->bytes = lre::image_device_bytes(*img);
-  if (r->bytes > s->cfg.device_budget_bytes) {
-    delete r;
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->err = "server: request needs more device memory than the budget";
-    return LRE_ERR_BUSY;
-  }
-  cudaSetDevice(s->cfg.device);
-  if (r->pins.pin(img->mosaic, lre::mosaic_bytes_of(*img)) != cudaSuccess ||
-      r->pins.pin(img->out, lre::out_bytes_of(*img)) != cudaSuccess) {
-    delete r;
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->err = "server: cannot page-lock the request's host buffers";
-    return LRE_ERR_OUT_OF_MEMORY;
-  }
-  r->t_submit = lre::Clock::now();
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    if (s->stop) {
-      delete r;
-      return LRE_ERR_BUSY;
-    }
-    r->ticket = s->next_ticket++;
-    s->reqs[r->ticket] = r;
-    s->queue.push_back(r);
-    *ticket = r->ticket;
-  }
-  s->cv_sched.notify_one();
-  return LRE_OK;
+  lre::Request* r = nullptr;
+  LRE_TRY(lre::prepare_request(s, img, &r));
+  return lre::enqueue_request(s, r, ticket);
+}
+
+lre_status lre_server_submit_decode(lre_server* sp, const lre_image* img, lre_decode_fn decode, void* user,
+                                    uint64_t* ticket) {
+  Server* s = reinterpret_cast<Server*>(sp);
+  if (!s || !img || !ticket || !decode) return LRE_ERR_INVALID_ARGUMENT;
+  lre::Request* r = nullptr;
+  LRE_TRY(lre::prepare_request(s, img, &r));
+  r->decode = decode;
+  r->user = user;
+  return lre::enqueue_request(s, r, ticket);
 }
 
 lre_status lre_server_wait(lre_server* sp, uint64_t ticket, double timeout_ms, lre_request_stats* stats) {
@@ -845,10 +911,11 @@ lre_status lre_server_wait(lre_server* sp, uint64_t ticket, double timeout_ms, l
   if (stats) {
     stats->status = r->status;
     stats->lane = r->lane;
-    stats->queue_ms = lre::ms_since(r->t_submit, r->t_admit);
+    stats->queue_ms = lre::ms_since(r->t_ready, r->t_admit);
     stats->run_ms = lre::ms_since(r->t_admit, r->t_done);
     stats->total_ms = lre::ms_since(r->t_submit, r->t_done);
     stats->device_bytes = r->bytes;
+    stats->decode_ms = r->decode ? lre::ms_since(r->t_submit, r->t_ready) : 0.0;
   }
   lre_status st = r->status;
   s->reqs.erase(it);

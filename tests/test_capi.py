@@ -13,6 +13,7 @@ HEADER = os.path.join(ROOT, "include", "lre_cuda.h")
 def declared_functions():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"^typedef[^;]*;", "", src, flags=re.M | re.S)  # callback types are not entry points
     names = re.findall(r"^[A-Za-z_][\w\s\*]*?\b(lre_\w+)\s*\(", src, flags=re.M)
     return sorted(set(names))
 

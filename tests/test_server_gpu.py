@@ -125,3 +125,52 @@ def test_wait_timeout_and_invalid(lre):
         assert out.shape == (512, 768, 3)
     finally:
         srv.close()
+
+
+def test_decode_callbacks_overlap_device_work(lre, acc):
+    """lre_server_submit_decode: a host decode step (here a stand-in for
+    LibRaw's unpack: a 14-bit integer raw plane scaled to float, with a
+    50 ms delay) runs on the server's decode threads while the lanes develop
+    earlier requests.  Results equal the plain path's bit for bit; two
+    decode threads finish six requests in well under the serial time; an
+    error in one decode fails that request only."""
+    import time
+
+    srv = lre.Server(0, lanes=2, decode_threads=2)
+    try:
+        raws, params, expect = [], [], []
+        for i in range(6):
+            m, p = _request(lre, 20 + i, 256, 384)
+            raw = np.clip(np.rint(m * 16383.0), 0, 16383).astype(np.uint16)
+            raws.append(raw)
+            params.append(p)
+            expect.append(acc.develop(raw.astype(np.float32) / np.float32(16383.0), p))
+
+        def decoder(raw):
+            def fill(mosaic):
+                time.sleep(0.05)
+                np.divide(raw.astype(np.float32), np.float32(16383.0), out=mosaic)
+            return fill
+
+        t0 = time.perf_counter()
+        tickets = [srv.submit_decode(r.shape, p, decoder(r)) for r, p in zip(raws, params)]
+        results = [srv.wait(t) for t in tickets]
+        wall_ms = (time.perf_counter() - t0) * 1e3
+        serial_ms = 0.0
+        for (out, st), e in zip(results, expect):
+            assert np.array_equal(out, e)
+            assert st["decode_ms"] >= 45.0
+            serial_ms += st["decode_ms"] + st["run_ms"]
+        assert wall_ms < 0.75 * serial_ms, (wall_ms, serial_ms)
+
+        def broken(mosaic):
+            raise RuntimeError("corrupt raw file")
+
+        bad = srv.submit_decode((64, 96), params[0], broken)
+        good = srv.submit_decode(raws[0].shape, params[0], decoder(raws[0]))
+        with pytest.raises(RuntimeError, match="corrupt raw file"):
+            srv.wait(bad)
+        out, _ = srv.wait(good)
+        assert np.array_equal(out, expect[0])
+    finally:
+        srv.close()
