@@ -228,20 +228,23 @@ __device__ __forceinline__ void f2_unpack(unsigned long long v, float& a, float&
   asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
 }
 // acc + w * x per lane, the product and the sum each rounded to nearest
-// (the reference's order, no contraction), as two IEEE scalar operations per
-// lane.  The packed f32x2 forms cannot stand in: a probe of mul.rn.f32x2
-// followed by add.rn.f32x2 on B200 (as separate instructions, as one asm
-// block, or with the add written as fma.rn.f32x2(1, p, acc)) returned the
-// fused result, w * x + acc rounded once, on 12.6% of random pairs, and on
-// the 51 MP workload that single rounding flipped one pixel's
-// classification by 1.6e-3.
+// (the reference's order, no contraction): the two products as IEEE scalar
+// multiplies, the two sums as one packed add.rn.f32x2.  A packed multiply
+// feeding a packed add is not safe: ptxas contracts that pair into a fused
+// multiply-add (one rounding), which on the 51 MP workload flipped one
+// pixel's classification by 1.6e-3.  With scalar products between them
+// there is nothing to contract: a B200 probe of the 21-tap chain gave 0
+// differences from scalar multiply-then-add over 4.2 M outputs, and the
+// blurs need a quarter fewer FP instructions than in all-scalar form.
 __device__ __forceinline__ unsigned long long f2_madd(unsigned long long acc, unsigned long long w,
                                                       unsigned long long x) {
-  float a0, a1, w0, w1, x0, x1;
-  f2_unpack(acc, a0, a1);
+  float w0, w1, x0, x1;
   f2_unpack(w, w0, w1);
   f2_unpack(x, x0, x1);
-  return f2_pack(__fadd_rn(a0, __fmul_rn(w0, x0)), __fadd_rn(a1, __fmul_rn(w1, x1)));
+  const unsigned long long p = f2_pack(__fmul_rn(w0, x0), __fmul_rn(w1, x1));
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(acc), "l"(p));
+  return r;
 }
 
 // The two separable passes of one plane on the tile in shared memory.
